@@ -1,0 +1,109 @@
+"""The CPU restatement (oracle/rd_oracle.c) against the reference's own outputs.
+
+Fixtures in tests/golden/ were produced by the reference's CPU code compiled from
+its sources (tests/golden/make_golden.py); every comparison here is bit for bit.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+BF = sorted(glob.glob(os.path.join(GOLD, "bf_*.npz")))
+TILED = sorted(glob.glob(os.path.join(GOLD, "tiled_*.npz")))
+
+
+def bits_equal(a, b):
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    return a.shape == b.shape and np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+@pytest.mark.parametrize("path", BF, ids=[os.path.basename(p) for p in BF])
+def test_bf_steps_match_reference(path):
+    g = np.load(path)
+    P, r1, r2 = g["P"], float(g["r1"]), float(g["r2"])
+    S0 = O.choose(P, r1)
+    assert bits_equal(S0, g["S_choose"])
+    S1, sums, cnt, _key, cont = O.evolve_pass(P, S0, r1)
+    assert bits_equal(S1, g["S_pass1"])
+    assert bits_equal(sums, g["sums_pass1"])
+    assert np.array_equal(cnt, g["cnt_pass1"])
+    assert cont == int(g["cont_pass1"])
+    Se, passes = O.evolve(P, S0, r1)
+    assert passes >= 1
+    assert bits_equal(Se, g["S_evolved"])
+    assert bits_equal(O.decimate(Se, r2), g["S_decimated"])
+    Sd, seg = O.decimate_seg(Se, g["seg_in"], r2)
+    assert bits_equal(Sd, g["S_decimated_nocopy"])
+    assert np.array_equal(seg, g["seg_out"])
+
+
+@pytest.mark.parametrize("path", BF, ids=[os.path.basename(p) for p in BF])
+def test_bf_pipeline_matches_reference(path):
+    g = np.load(path)
+    S, st = O.ridge_bf(g["P"], float(g["r1"]), float(g["r2"]))
+    assert bits_equal(S, g["S_final"])
+    assert st.ns_choose == g["S_choose"].shape[0]
+
+
+@pytest.mark.parametrize("path", TILED, ids=[os.path.basename(p) for p in TILED])
+def test_tiled_pipeline_matches_reference(path):
+    g = np.load(path)
+    S, _st, nl = O.ridge_tiled(g["P"], float(g["r1"]), float(g["r2"]),
+                               int(g["max_tile_capacity"]), g["tiles_per_dim"])
+    assert nl >= 1
+    assert bits_equal(S, g["S_final"])
+
+
+def test_hausdorff_basic():
+    A = np.array([[0, 0], [1, 0]], np.float32)
+    B = np.array([[0, 0], [1, 0], [1, 2]], np.float32)
+    assert O.hausdorff(A, A) == 0.0
+    assert abs(O.hausdorff(A, B) - 2.0) < 1e-12
+
+
+def test_adjoint_oracle_matches_finite_differences():
+    """FP64 reverse pass vs central differences of the same forward with the
+    assignment frozen (the forward is then affine in P, so FD is exact)."""
+    from ridgedetection_b200 import generators as G
+    P = G.helix3d(3000, seed=21)
+    r1 = 0.2
+    S0 = O.choose(P, r1)
+    rng = np.random.default_rng(5)
+    W = rng.normal(size=S0.shape)
+    iters = 6
+    gP, gS0, Sf = O.evolve_adjoint(P, S0, r1, iters, W)
+    # frozen-assignment FP64 forward
+    keys = []
+    S = S0.astype(np.float32).copy()
+    for _ in range(iters):
+        k = O.assign(P, S, r1)
+        keys.append(k)
+        _, sums, cnt, _, _ = O.evolve_pass(P, S, r1)
+        nz = cnt > 0
+        S = S.copy()
+        S[nz] = (sums[nz] / cnt[nz, None].astype(np.float32)).astype(np.float32)
+    assert np.array_equal(S, Sf)
+
+    def fwd64(Pd, S0d):
+        Sd = S0d.copy()
+        for k in keys:
+            out = Sd.copy()
+            for c in np.unique(k[k >= 0]):
+                out[c] = Pd[k == c].mean(axis=0)
+            Sd = out
+        return float((W * Sd).sum())
+    P64, S064 = P.astype(np.float64), S0.astype(np.float64)
+    h = 1e-3
+    idx = rng.choice(P.shape[0] * 3, 12, replace=False)
+    for f in idx:
+        i, d = divmod(int(f), 3)
+        Pp, Pm = P64.copy(), P64.copy()
+        Pp[i, d] += h
+        Pm[i, d] -= h
+        fd = (fwd64(Pp, S064) - fwd64(Pm, S064)) / (2 * h)
+        assert abs(fd - gP[i, d]) <= 1e-8 + 1e-6 * abs(fd)
