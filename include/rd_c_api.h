@@ -1,0 +1,122 @@
+/*
+ * rd_c_api.h -- C ABI of the B200 ridge-detection library (librd_b200.so).
+ *
+ * Plain pointers and sizes only.  Every call returns an rd_status; nothing
+ * exits or traps.  rd_last_error() gives the calling thread's last message.
+ * Streams are passed as void* (a cudaStream_t; NULL = legacy default stream).
+ * Handles are not thread-safe; distinct handles may be used concurrently.
+ *
+ * The entry points replace the reference's device-facing interfaces (paths are
+ * inside ridge_detection/ of aosewski/RidgeDetection):
+ *   rd_bf_*     rd::gpu::bruteForce::RidgeDetection<T,DIM,IN,OUT>
+ *               rd/gpu/device/brute_force/simulation.cuh:35-112, .inl:40-434
+ *   rd_tiled_*  rd::gpu::tiled::RidgeDetection<DIM,IN,OUT,RD_BRUTE_FORCE,RD_MIXED,
+ *               RD_EXTENDED_TILE,T>   rd/gpu/device/tiled/simulation.cuh:41-241
+ *   rd_batch_*  no reference counterpart (the reference solves one cloud per call)
+ *   rd_evolve_adjoint  no reference counterpart
+ *
+ * Point layouts follow rd::DataMemoryLayout (rd/utils/memory.h:21-26):
+ *   RD_ROW_MAJOR  point i, coordinate d at  p[i * pitch + d]   (pitch >= dim)
+ *   RD_COL_MAJOR  point i, coordinate d at  p[d * pitch + i]   (pitch >= n)
+ * A pitch of 0 means "packed" (dim for ROW_MAJOR, n for COL_MAJOR).
+ * All coordinates are float32.
+ */
+#ifndef RD_C_API_H
+#define RD_C_API_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define RD_API __attribute__((visibility("default")))
+#else
+#define RD_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum rd_status {
+    RD_OK = 0,
+    RD_ERR_ARG = 1,             /* invalid argument                                   */
+    RD_ERR_CUDA = 2,            /* a CUDA runtime call failed                          */
+    RD_ERR_CAPACITY = 3,        /* a device buffer would overflow                      */
+    RD_ERR_NOT_CONVERGED = 4,   /* an iteration limit was reached (results partial)    */
+    RD_ERR_ALLOC = 5,           /* device or host allocation failed                    */
+    RD_ERR_UNSUPPORTED = 6      /* dimension / option not built into this library      */
+} rd_status;
+
+typedef enum rd_layout { RD_ROW_MAJOR = 0, RD_COL_MAJOR = 1 } rd_layout;
+
+/* how the evolve -> decimate -> convergence loop is driven */
+typedef enum rd_loop_mode {
+    RD_LOOP_GRAPH = 0,  /* CUDA graph with a device-side WHILE node; no host sync per iteration */
+    RD_LOOP_HOST = 1    /* host reads a device flag after every iteration (reference style)    */
+} rd_loop_mode;
+
+typedef struct rd_run_stats {
+    int64_t loop_iters;     /* loop iterations (evolve passes of the slowest cloud)  */
+    int64_t evolve_passes;  /* evolve passes summed over clouds                      */
+    int64_t max_passes;     /* evolve passes of the cloud that needed most           */
+    double  pairs;          /* sum over passes of (cloud points x chosen points)     */
+    int32_t err_bits;       /* device error bits (0 when clean)                      */
+    int32_t pad;
+} rd_run_stats;
+
+RD_API const char* rd_last_error(void);
+RD_API int rd_abi_version(void);
+/* dimensions compiled into the kernels, as a bit mask (bit d set = dim d) */
+RD_API int rd_supported_dims(void);
+
+/* ---------------------------------------------------------------------------
+ * Brute force, one cloud.  Mirrors rd::gpu::bruteForce::RidgeDetection:
+ *   ctor(np, r1, r2)            -> rd_bf_create       (simulation.inl:40-90)
+ *   caller fills dP_            -> rd_bf_set_points   (tests/test_rd_gpu_simulation/
+ *                                                       brute_force/simulation.cu:188-190)
+ *   ridgeDetection()            -> rd_bf_run          (simulation.inl:183-384)
+ *   getChosenSamplesCount()     -> rd_bf_get_count    (simulation.inl:172-176)
+ *   dS_ (ns_ points)            -> rd_bf_get_points
+ * ------------------------------------------------------------------------- */
+typedef struct rd_bf rd_bf;
+RD_API rd_status rd_bf_create(rd_bf** out, int dim, int in_layout, int out_layout, int64_t np,
+                       float r1, float r2);
+RD_API rd_status rd_bf_set_points(rd_bf* h, const float* pts, int64_t pitch, int src_on_device,
+                           void* stream);
+RD_API rd_status rd_bf_set_loop_mode(rd_bf* h, int mode);
+RD_API rd_status rd_bf_run(rd_bf* h, void* stream);
+RD_API rd_status rd_bf_get_count(rd_bf* h, int64_t* ns);
+/* out receives ns points in the handle's out_layout (pitch as above, for n = ns) */
+RD_API rd_status rd_bf_get_points(rd_bf* h, float* out, int64_t pitch, int dst_on_device, void* stream);
+RD_API rd_status rd_bf_get_stats(rd_bf* h, rd_run_stats* st);
+RD_API rd_status rd_bf_destroy(rd_bf* h);
+
+/* ---------------------------------------------------------------------------
+ * Batched: many independent clouds solved together (brute force per cloud).
+ * Cloud c has n points at pts + offset (ROW_MAJOR, packed, offset counted in
+ * floats so clouds of different dims can share one array) and its own dim,
+ * r1, r2.  Clouds of different dims are solved in separate sub-batches.
+ * ------------------------------------------------------------------------- */
+typedef struct rd_cloud_desc {
+    int64_t offset;   /* first float of the cloud in pts                          */
+    int64_t n;        /* number of points                                         */
+    int32_t dim;
+    float r1, r2;
+    int32_t pad;
+} rd_cloud_desc;
+
+typedef struct rd_batch rd_batch;
+RD_API rd_status rd_batch_create(rd_batch** out);
+RD_API rd_status rd_batch_set_loop_mode(rd_batch* h, int mode);
+/* pts: packed ROW_MAJOR floats; total_floats = length of pts in floats */
+RD_API rd_status rd_batch_run(rd_batch* h, const rd_cloud_desc* clouds, int32_t n_clouds,
+                       const float* pts, int64_t total_floats, int src_on_device, void* stream);
+RD_API rd_status rd_batch_get_counts(rd_batch* h, int64_t* ns);  /* n_clouds entries */
+RD_API rd_status rd_batch_get_points(rd_batch* h, int32_t cloud, float* out, int dst_on_device,
+                              void* stream);                 /* ns[cloud]*dim floats */
+RD_API rd_status rd_batch_get_stats(rd_batch* h, rd_run_stats* st);
+RD_API rd_status rd_batch_destroy(rd_batch* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RD_C_API_H */

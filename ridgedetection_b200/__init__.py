@@ -1,0 +1,15 @@
+"""B200-native ridge detection (choose / evolve / decimate) over a C ABI.
+
+The compute path is librd_b200.so: hand-written sm_100a CUDA kernels driven by
+a C++ host engine (ridgedetection_b200/csrc).  This package is the Python-side
+mirror of the reference's interface; it never falls back to a CPU path.
+"""
+from . import generators  # noqa: F401
+from ._lib import RDError, RunStats, lib  # noqa: F401
+from .api import (COL_MAJOR, LOOP_GRAPH, LOOP_HOST, ROW_MAJOR,  # noqa: F401
+                  BatchedRidgeDetection, BruteForceRidgeDetection, pack_clouds,
+                  ridge_detection)
+
+__all__ = ["BruteForceRidgeDetection", "BatchedRidgeDetection", "ridge_detection",
+           "pack_clouds", "ROW_MAJOR", "COL_MAJOR", "LOOP_GRAPH", "LOOP_HOST", "RDError",
+           "RunStats", "lib", "generators"]

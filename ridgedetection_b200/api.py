@@ -1,0 +1,204 @@
+"""Python mirror of the reference's device-facing classes, over the C ABI.
+
+``BruteForceRidgeDetection`` follows rd::gpu::bruteForce::RidgeDetection
+(rd/gpu/device/brute_force/simulation.cuh:35-112): construct with
+(np, r1, r2), fill the points, call ``ridge_detection()``, then
+``get_chosen_samples_count()`` and read the chosen points.
+
+``BatchedRidgeDetection`` solves many independent clouds in one engine run (no
+reference counterpart; the reference solves one cloud per call).
+
+Inputs may be numpy arrays (host memory) or CUDA torch tensors (device memory,
+enqueued on the current torch stream).  There is no CPU path: everything runs
+through librd_b200.so.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib as L
+
+ROW_MAJOR = L.RD_ROW_MAJOR
+COL_MAJOR = L.RD_COL_MAJOR
+LOOP_GRAPH = L.RD_LOOP_GRAPH
+LOOP_HOST = L.RD_LOOP_HOST
+
+
+def _is_torch_cuda(x) -> bool:
+    return hasattr(x, "is_cuda") and bool(x.is_cuda)
+
+
+def _ptr_of(x, want_writable=False):
+    """(pointer, on_device, stream) of a float32 numpy array or CUDA tensor."""
+    if _is_torch_cuda(x):
+        import torch
+        if x.dtype != torch.float32:
+            raise TypeError("points must be float32")
+        if not x.is_contiguous():
+            raise ValueError("CUDA tensors must be contiguous")
+        return ctypes.c_void_p(x.data_ptr()), 1, ctypes.c_void_p(
+            torch.cuda.current_stream(x.device).cuda_stream)
+    if not isinstance(x, np.ndarray):
+        raise TypeError("points must be a numpy array or a CUDA torch tensor")
+    if x.dtype != np.float32 or not x.flags["C_CONTIGUOUS"]:
+        raise TypeError("numpy points must be C-contiguous float32")
+    if want_writable and not x.flags["WRITEABLE"]:
+        raise ValueError("output array is read-only")
+    return ctypes.c_void_p(x.ctypes.data), 0, ctypes.c_void_p(0)
+
+
+class BruteForceRidgeDetection:
+    """rd::gpu::bruteForce::RidgeDetection<float, DIM, IN_MEM_LAYOUT, OUT_MEM_LAYOUT>."""
+
+    def __init__(self, np_: int, r1: float, r2: float, dim: int,
+                 in_layout: int = ROW_MAJOR, out_layout: int = ROW_MAJOR,
+                 loop_mode: int = LOOP_GRAPH):
+        self._lib = L.lib()
+        self._h = ctypes.c_void_p()
+        L.check(self._lib.rd_bf_create(ctypes.byref(self._h), dim, in_layout, out_layout,
+                                       int(np_), float(r1), float(r2)))
+        self.np_ = int(np_)
+        self.r1_ = float(r1)
+        self.r2_ = float(r2)
+        self.dim = int(dim)
+        self.in_layout = in_layout
+        self.out_layout = out_layout
+        self.ns_ = 0
+        self.set_loop_mode(loop_mode)
+
+    def set_loop_mode(self, mode: int):
+        L.check(self._lib.rd_bf_set_loop_mode(self._h, mode))
+
+    def set_points(self, pts, pitch: int = 0):
+        """Copy the cloud into the device (the reference's dP_)."""
+        p, dev, st = _ptr_of(pts)
+        L.check(self._lib.rd_bf_set_points(self._h, p, int(pitch), dev, st))
+
+    def ridge_detection(self, stream=None):
+        st = ctypes.c_void_p(stream) if stream is not None else self._current_stream()
+        L.check(self._lib.rd_bf_run(self._h, st))
+        self.get_chosen_samples_count()
+
+    def get_chosen_samples_count(self) -> int:
+        n = ctypes.c_int64(0)
+        L.check(self._lib.rd_bf_get_count(self._h, ctypes.byref(n)))
+        self.ns_ = int(n.value)
+        return self.ns_
+
+    def chosen_points(self, out=None, pitch: int = 0):
+        """Chosen points in the handle's output layout (numpy unless `out` is given)."""
+        if out is None:
+            if self.out_layout == ROW_MAJOR:
+                out = np.empty((self.ns_, self.dim), np.float32)
+            else:
+                out = np.empty((self.dim, self.ns_), np.float32)
+        p, dev, st = _ptr_of(out, want_writable=True)
+        L.check(self._lib.rd_bf_get_points(self._h, p, int(pitch), dev, st))
+        return out
+
+    def stats(self) -> L.RunStats:
+        s = L.RunStats()
+        L.check(self._lib.rd_bf_get_stats(self._h, ctypes.byref(s)))
+        return s
+
+    @staticmethod
+    def _current_stream():
+        try:
+            import torch
+            if torch.cuda.is_available():
+                return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        except Exception:
+            pass
+        return ctypes.c_void_p(0)
+
+    def close(self):
+        if self._h:
+            self._lib.rd_bf_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def ridge_detection(P: np.ndarray, r1: float, r2: float, loop_mode: int = LOOP_GRAPH):
+    """Brute-force ridge of one ROW_MAJOR float32 cloud; returns (S, stats)."""
+    P = np.ascontiguousarray(P, dtype=np.float32)
+    rd = BruteForceRidgeDetection(P.shape[0], r1, r2, P.shape[1], loop_mode=loop_mode)
+    try:
+        rd.set_points(P)
+        rd.ridge_detection()
+        return rd.chosen_points(), rd.stats()
+    finally:
+        rd.close()
+
+
+class BatchedRidgeDetection:
+    """Many independent clouds, one engine run per point dimension."""
+
+    def __init__(self, loop_mode: int = LOOP_GRAPH):
+        self._lib = L.lib()
+        self._h = ctypes.c_void_p()
+        L.check(self._lib.rd_batch_create(ctypes.byref(self._h)))
+        L.check(self._lib.rd_batch_set_loop_mode(self._h, loop_mode))
+        self._dims: List[int] = []
+        self._counts = np.zeros(0, np.int64)
+
+    def run(self, packed, descs: Sequence[Tuple[int, int, int, float, float]], stream=None):
+        """packed: all clouds' ROW_MAJOR floats back to back (numpy or CUDA
+        tensor); descs: per cloud (offset_in_floats, n, dim, r1, r2)."""
+        arr = (L.CloudDesc * len(descs))()
+        for k, (off, n, dim, r1, r2) in enumerate(descs):
+            arr[k].offset, arr[k].n, arr[k].dim = int(off), int(n), int(dim)
+            arr[k].r1, arr[k].r2 = float(r1), float(r2)
+        p, dev, st = _ptr_of(packed)
+        if stream is not None:
+            st = ctypes.c_void_p(stream)
+        total = int(packed.numel() if dev else packed.size)
+        L.check(self._lib.rd_batch_run(self._h, arr, len(descs), p, total, dev, st))
+        self._dims = [int(d[2]) for d in descs]
+        self._counts = np.zeros(len(descs), np.int64)
+        L.check(self._lib.rd_batch_get_counts(
+            self._h, self._counts.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
+        return self._counts.copy()
+
+    def chosen_points(self, cloud: int) -> np.ndarray:
+        out = np.empty((int(self._counts[cloud]), self._dims[cloud]), np.float32)
+        if out.size:
+            L.check(self._lib.rd_batch_get_points(self._h, int(cloud),
+                                                  ctypes.c_void_p(out.ctypes.data), 0,
+                                                  ctypes.c_void_p(0)))
+        return out
+
+    def stats(self) -> L.RunStats:
+        s = L.RunStats()
+        L.check(self._lib.rd_batch_get_stats(self._h, ctypes.byref(s)))
+        return s
+
+    def close(self):
+        if self._h:
+            self._lib.rd_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def pack_clouds(clouds: Sequence[Tuple[np.ndarray, float, float]]):
+    """[(P, r1, r2), ...] -> (packed float32 array, descs)."""
+    descs, parts, off = [], [], 0
+    for P, r1, r2 in clouds:
+        P = np.ascontiguousarray(P, dtype=np.float32)
+        descs.append((off, P.shape[0], P.shape[1], r1, r2))
+        parts.append(P.reshape(-1))
+        off += P.size
+    packed = np.concatenate(parts) if parts else np.zeros(0, np.float32)
+    return np.ascontiguousarray(packed, dtype=np.float32), descs

@@ -1,0 +1,441 @@
+// rd_capi.cu -- extern "C" entry points declared in include/rd_c_api.h.
+#include "../../include/rd_c_api.h"
+#include "rd_engine_host.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+using namespace rdb;
+
+namespace {
+
+thread_local std::string g_err;
+
+rd_status set_err(rd_status s, const std::string& msg)
+{
+    g_err = msg;
+    return s;
+}
+
+rd_status from_engine(int rc, const Engine& e)
+{
+    if (rc == 0) return RD_OK;
+    g_err = e.last_error;
+    return (rd_status)rc;
+}
+
+#define CK_CUDA(call)                                                                  \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess)                                                         \
+            return set_err(RD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+__global__ void k_in_to_row(const float* __restrict__ src, int layout, int64_t pitch, int64_t n,
+                            int dim, float* __restrict__ dst)
+{
+    const int64_t total = n * dim;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = e / dim;
+        const int d = (int)(e - i * dim);
+        dst[e] = (layout == RD_ROW_MAJOR) ? src[i * pitch + d] : src[(int64_t)d * pitch + i];
+    }
+}
+
+__global__ void k_row_to_out(const float* __restrict__ src, int64_t n, int dim, int layout,
+                             int64_t pitch, float* __restrict__ dst)
+{
+    const int64_t total = n * dim;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = e / dim;
+        const int d = (int)(e - i * dim);
+        if (layout == RD_ROW_MAJOR) dst[i * pitch + d] = src[e];
+        else dst[(int64_t)d * pitch + i] = src[e];
+    }
+}
+
+int grid_for(int64_t n)
+{
+    int64_t g = (n + 255) / 256;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 16));
+}
+
+// Copies n points (layout/pitch) from host or device into the packed ROW_MAJOR
+// buffer dst on the device.
+rd_status load_points(const float* src, int layout, int64_t pitch, int64_t n, int dim,
+                      int src_on_device, float* dst, DevBuf& staging, cudaStream_t st)
+{
+    if (n == 0) return RD_OK;
+    if (!src) return set_err(RD_ERR_ARG, "null point pointer");
+    if (layout == RD_ROW_MAJOR) {
+        if (pitch == 0) pitch = dim;
+        if (pitch < dim) return set_err(RD_ERR_ARG, "ROW_MAJOR pitch < dim");
+        if (pitch == dim) {
+            CK_CUDA(cudaMemcpyAsync(dst, src, sizeof(float) * n * dim,
+                                    src_on_device ? cudaMemcpyDeviceToDevice
+                                                  : cudaMemcpyHostToDevice, st));
+        } else {
+            CK_CUDA(cudaMemcpy2DAsync(dst, sizeof(float) * dim, src, sizeof(float) * pitch,
+                                      sizeof(float) * dim, n,
+                                      src_on_device ? cudaMemcpyDeviceToDevice
+                                                    : cudaMemcpyHostToDevice, st));
+        }
+        return RD_OK;
+    }
+    if (layout != RD_COL_MAJOR) return set_err(RD_ERR_ARG, "unknown layout");
+    if (pitch == 0) pitch = n;
+    if (pitch < n) return set_err(RD_ERR_ARG, "COL_MAJOR pitch < n");
+    const float* dsrc = src;
+    if (!src_on_device) {
+        CK_CUDA(staging.ensure(sizeof(float) * n * dim));
+        CK_CUDA(cudaMemcpy2DAsync(staging.p, sizeof(float) * n, src, sizeof(float) * pitch,
+                                  sizeof(float) * n, dim, cudaMemcpyHostToDevice, st));
+        dsrc = staging.as<float>();
+        pitch = n;
+    }
+    k_in_to_row<<<grid_for(n * dim), 256, 0, st>>>(dsrc, RD_COL_MAJOR, pitch, n, dim, dst);
+    CK_CUDA(cudaGetLastError());
+    return RD_OK;
+}
+
+// Copies n packed ROW_MAJOR points from the device to dst (layout/pitch).
+rd_status store_points(const float* src, int64_t n, int dim, int layout, int64_t pitch,
+                       float* dst, int dst_on_device, DevBuf& staging, cudaStream_t st)
+{
+    if (n == 0) return RD_OK;
+    if (!dst) return set_err(RD_ERR_ARG, "null output pointer");
+    if (layout == RD_ROW_MAJOR) {
+        if (pitch == 0) pitch = dim;
+        if (pitch < dim) return set_err(RD_ERR_ARG, "ROW_MAJOR pitch < dim");
+        CK_CUDA(cudaMemcpy2DAsync(dst, sizeof(float) * pitch, src, sizeof(float) * dim,
+                                  sizeof(float) * dim, n,
+                                  dst_on_device ? cudaMemcpyDeviceToDevice
+                                                : cudaMemcpyDeviceToHost, st));
+        return RD_OK;
+    }
+    if (layout != RD_COL_MAJOR) return set_err(RD_ERR_ARG, "unknown layout");
+    if (pitch == 0) pitch = n;
+    if (pitch < n) return set_err(RD_ERR_ARG, "COL_MAJOR pitch < n");
+    if (dst_on_device) {
+        k_row_to_out<<<grid_for(n * dim), 256, 0, st>>>(src, n, dim, RD_COL_MAJOR, pitch, dst);
+        CK_CUDA(cudaGetLastError());
+        return RD_OK;
+    }
+    CK_CUDA(staging.ensure(sizeof(float) * n * dim));
+    k_row_to_out<<<grid_for(n * dim), 256, 0, st>>>(src, n, dim, RD_COL_MAJOR, n,
+                                                    staging.as<float>());
+    CK_CUDA(cudaGetLastError());
+    CK_CUDA(cudaMemcpy2DAsync(dst, sizeof(float) * pitch, staging.p, sizeof(float) * n,
+                              sizeof(float) * n, dim, cudaMemcpyDeviceToHost, st));
+    return RD_OK;
+}
+
+void fill_stats(const RunStats& s, rd_run_stats* o)
+{
+    std::memset(o, 0, sizeof(*o));
+    o->loop_iters = s.loop_iters;
+    o->evolve_passes = s.total_passes;
+    o->max_passes = s.max_passes;
+    o->pairs = s.pairs;
+    o->err_bits = s.err_bits;
+}
+
+bool dim_ok(int dim) { return dim == 2 || dim == 3; }
+
+}  // namespace
+
+struct rd_bf {
+    int dim, in_layout, out_layout;
+    int64_t np;
+    float r1, r2;
+    int mode = RD_LOOP_GRAPH;
+    Engine eng;
+    DevBuf staging;
+    int64_t ns = 0;
+    bool have_result = false;
+};
+
+struct rd_batch {
+    int mode = RD_LOOP_GRAPH;
+    std::map<int, std::unique_ptr<Engine>> eng;   // one engine per dim
+    std::vector<int> cloud_dim;                   // per user cloud
+    std::vector<int> cloud_slot;                  // per user cloud: index in its engine
+    std::vector<int64_t> ns;                      // per user cloud
+    DevBuf staging;
+    DevBuf gather_tab;
+    RunStats stats;
+};
+
+extern "C" {
+
+const char* rd_last_error(void) { return g_err.c_str(); }
+
+int rd_abi_version(void) { return 1; }
+
+int rd_supported_dims(void) { return (1 << 2) | (1 << 3); }
+
+// ------------------------------------------------------------------------
+// brute force
+// ------------------------------------------------------------------------
+rd_status rd_bf_create(rd_bf** out, int dim, int in_layout, int out_layout, int64_t np,
+                       float r1, float r2)
+{
+    if (!out) return set_err(RD_ERR_ARG, "null handle pointer");
+    *out = nullptr;
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if ((in_layout != RD_ROW_MAJOR && in_layout != RD_COL_MAJOR) ||
+        (out_layout != RD_ROW_MAJOR && out_layout != RD_COL_MAJOR))
+        return set_err(RD_ERR_ARG, "unknown layout");
+    if (np < 0 || np > INT32_MAX - 1024) return set_err(RD_ERR_ARG, "np out of range");
+    if (!(r1 > 0.0f) || !(r2 > 0.0f)) return set_err(RD_ERR_ARG, "r1 and r2 must be > 0");
+    rd_bf* h = new (std::nothrow) rd_bf();
+    if (!h) return set_err(RD_ERR_ALLOC, "host allocation failed");
+    h->dim = dim;
+    h->in_layout = in_layout;
+    h->out_layout = out_layout;
+    h->np = np;
+    h->r1 = r1;
+    h->r2 = r2;
+    CloudDesc cd;
+    std::memset(&cd, 0, sizeof(cd));
+    cd.p_off = 0;
+    cd.n_all = (int32_t)np;
+    cd.n_own = (int32_t)np;
+    cd.r1 = r1;
+    cd.r2 = r2;
+    cd.group = 0;
+    GroupDesc gd;
+    std::memset(&gd, 0, sizeof(gd));
+    gd.cloud_begin = 0;
+    gd.n_clouds = 1;
+    gd.nocopy = 0;
+    int rc = h->eng.setup(dim, {cd}, {gd}, np);
+    if (rc) {
+        rd_status s = from_engine(rc, h->eng);
+        delete h;
+        return s;
+    }
+    *out = h;
+    return RD_OK;
+}
+
+rd_status rd_bf_set_points(rd_bf* h, const float* pts, int64_t pitch, int src_on_device,
+                           void* stream)
+{
+    if (!h) return set_err(RD_ERR_ARG, "null handle");
+    h->have_result = false;
+    return load_points(pts, h->in_layout, pitch, h->np, h->dim, src_on_device, h->eng.points(),
+                       h->staging, (cudaStream_t)stream);
+}
+
+rd_status rd_bf_set_loop_mode(rd_bf* h, int mode)
+{
+    if (!h) return set_err(RD_ERR_ARG, "null handle");
+    if (mode != RD_LOOP_GRAPH && mode != RD_LOOP_HOST) return set_err(RD_ERR_ARG, "bad mode");
+    h->mode = mode;
+    return RD_OK;
+}
+
+rd_status rd_bf_run(rd_bf* h, void* stream)
+{
+    if (!h) return set_err(RD_ERR_ARG, "null handle");
+    int rc = h->eng.run((cudaStream_t)stream, h->mode == RD_LOOP_GRAPH);
+    h->have_result = (rc == 0 || rc == RD_ERR_NOT_CONVERGED);
+    h->ns = h->have_result && !h->eng.ns().empty() ? h->eng.ns()[0] : 0;
+    return from_engine(rc, h->eng);
+}
+
+rd_status rd_bf_get_count(rd_bf* h, int64_t* ns)
+{
+    if (!h || !ns) return set_err(RD_ERR_ARG, "null argument");
+    *ns = h->have_result ? h->ns : 0;
+    return RD_OK;
+}
+
+rd_status rd_bf_get_points(rd_bf* h, float* out, int64_t pitch, int dst_on_device, void* stream)
+{
+    if (!h) return set_err(RD_ERR_ARG, "null handle");
+    if (!h->have_result) return set_err(RD_ERR_ARG, "no result: call rd_bf_run first");
+    rd_status s = store_points(h->eng.chosen(), h->ns, h->dim, h->out_layout, pitch, out,
+                               dst_on_device, h->staging, (cudaStream_t)stream);
+    if (s != RD_OK) return s;
+    CK_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    return RD_OK;
+}
+
+rd_status rd_bf_get_stats(rd_bf* h, rd_run_stats* st)
+{
+    if (!h || !st) return set_err(RD_ERR_ARG, "null argument");
+    fill_stats(h->eng.stats(), st);
+    return RD_OK;
+}
+
+rd_status rd_bf_destroy(rd_bf* h)
+{
+    delete h;
+    return RD_OK;
+}
+
+// ------------------------------------------------------------------------
+// batched
+// ------------------------------------------------------------------------
+__global__ void k_gather_clouds(const float* __restrict__ src, const int64_t* __restrict__ tab,
+                                int n_clouds, int dim, float* __restrict__ dst)
+{
+    // tab: per cloud (src_off_floats, dst_off_floats, n_floats)
+    for (int c = blockIdx.y; c < n_clouds; c += gridDim.y) {
+        const int64_t so = tab[3 * c], dof = tab[3 * c + 1], nf = tab[3 * c + 2];
+        for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nf;
+             e += (int64_t)gridDim.x * blockDim.x)
+            dst[dof + e] = src[so + e];
+    }
+    (void)dim;
+}
+
+rd_status rd_batch_create(rd_batch** out)
+{
+    if (!out) return set_err(RD_ERR_ARG, "null handle pointer");
+    *out = new (std::nothrow) rd_batch();
+    return *out ? RD_OK : set_err(RD_ERR_ALLOC, "host allocation failed");
+}
+
+rd_status rd_batch_set_loop_mode(rd_batch* h, int mode)
+{
+    if (!h) return set_err(RD_ERR_ARG, "null handle");
+    if (mode != RD_LOOP_GRAPH && mode != RD_LOOP_HOST) return set_err(RD_ERR_ARG, "bad mode");
+    h->mode = mode;
+    return RD_OK;
+}
+
+rd_status rd_batch_run(rd_batch* h, const rd_cloud_desc* clouds, int32_t n_clouds,
+                       const float* pts, int64_t total_floats, int src_on_device, void* stream)
+{
+    if (!h) return set_err(RD_ERR_ARG, "null handle");
+    if (n_clouds < 0 || (n_clouds > 0 && (!clouds || !pts)))
+        return set_err(RD_ERR_ARG, "bad cloud list");
+    cudaStream_t st = (cudaStream_t)stream;
+    h->cloud_dim.assign(n_clouds, 0);
+    h->cloud_slot.assign(n_clouds, 0);
+    h->ns.assign(n_clouds, 0);
+    h->stats = RunStats();
+    // validate and bucket by dim (largest clouds first inside each bucket)
+    std::map<int, std::vector<int>> by_dim;
+    for (int c = 0; c < n_clouds; ++c) {
+        const rd_cloud_desc& d = clouds[c];
+        if (!dim_ok(d.dim)) return set_err(RD_ERR_UNSUPPORTED, "cloud dim must be 2 or 3");
+        if (d.n < 0 || d.n > INT32_MAX - 1024 || d.offset < 0 ||
+            d.offset + d.n * d.dim > total_floats)
+            return set_err(RD_ERR_ARG, "cloud out of range");
+        if (!(d.r1 > 0.0f) || !(d.r2 > 0.0f)) return set_err(RD_ERR_ARG, "r1, r2 must be > 0");
+        by_dim[d.dim].push_back(c);
+    }
+    const float* dsrc = pts;
+    if (!src_on_device && total_floats > 0) {
+        CK_CUDA(h->staging.ensure(sizeof(float) * total_floats));
+        CK_CUDA(cudaMemcpyAsync(h->staging.p, pts, sizeof(float) * total_floats,
+                                cudaMemcpyHostToDevice, st));
+        dsrc = h->staging.as<float>();
+    }
+    for (auto& kv : by_dim) {
+        const int dim = kv.first;
+        std::vector<int>& ids = kv.second;
+        std::stable_sort(ids.begin(), ids.end(),
+                         [&](int a, int b) { return clouds[a].n > clouds[b].n; });
+        std::vector<CloudDesc> cl(ids.size());
+        std::vector<GroupDesc> gr(ids.size());
+        std::vector<int64_t> tab(3 * ids.size());
+        int64_t off = 0;
+        for (size_t k = 0; k < ids.size(); ++k) {
+            const rd_cloud_desc& d = clouds[ids[k]];
+            CloudDesc& cd = cl[k];
+            std::memset(&cd, 0, sizeof(cd));
+            cd.p_off = off;
+            cd.n_all = (int32_t)d.n;
+            cd.n_own = (int32_t)d.n;
+            cd.r1 = d.r1;
+            cd.r2 = d.r2;
+            cd.group = (int32_t)k;
+            GroupDesc& gd = gr[k];
+            std::memset(&gd, 0, sizeof(gd));
+            gd.cloud_begin = (int32_t)k;
+            gd.n_clouds = 1;
+            tab[3 * k] = d.offset;
+            tab[3 * k + 1] = off * dim;
+            tab[3 * k + 2] = d.n * dim;
+            off += d.n;
+            h->cloud_dim[ids[k]] = dim;
+            h->cloud_slot[ids[k]] = (int)k;
+        }
+        auto& e = h->eng[dim];
+        if (!e) e.reset(new (std::nothrow) Engine());
+        if (!e) return set_err(RD_ERR_ALLOC, "host allocation failed");
+        int rc = e->setup(dim, cl, gr, off);
+        if (rc) return from_engine(rc, *e);
+        CK_CUDA(h->gather_tab.ensure(sizeof(int64_t) * tab.size()));
+        CK_CUDA(cudaMemcpyAsync(h->gather_tab.p, tab.data(), sizeof(int64_t) * tab.size(),
+                                cudaMemcpyHostToDevice, st));
+        dim3 grid(64, (unsigned)std::min<size_t>(ids.size(), 65535));
+        k_gather_clouds<<<grid, 256, 0, st>>>(dsrc, h->gather_tab.as<int64_t>(), (int)ids.size(),
+                                              dim, e->points());
+        CK_CUDA(cudaGetLastError());
+        rc = e->run(st, h->mode == RD_LOOP_GRAPH);
+        if (rc && rc != RD_ERR_NOT_CONVERGED) return from_engine(rc, *e);
+        const RunStats& s = e->stats();
+        h->stats.loop_iters += s.loop_iters;
+        h->stats.total_passes += s.total_passes;
+        h->stats.max_passes = std::max(h->stats.max_passes, s.max_passes);
+        h->stats.pairs += s.pairs;
+        h->stats.err_bits |= s.err_bits;
+        for (size_t k = 0; k < ids.size(); ++k) h->ns[ids[k]] = e->ns()[k];
+        if (rc) return from_engine(rc, *e);
+    }
+    return RD_OK;
+}
+
+rd_status rd_batch_get_counts(rd_batch* h, int64_t* ns)
+{
+    if (!h || !ns) return set_err(RD_ERR_ARG, "null argument");
+    for (size_t c = 0; c < h->ns.size(); ++c) ns[c] = h->ns[c];
+    return RD_OK;
+}
+
+rd_status rd_batch_get_points(rd_batch* h, int32_t cloud, float* out, int dst_on_device,
+                              void* stream)
+{
+    if (!h || !out) return set_err(RD_ERR_ARG, "null argument");
+    if (cloud < 0 || cloud >= (int32_t)h->ns.size()) return set_err(RD_ERR_ARG, "bad cloud index");
+    const int dim = h->cloud_dim[cloud];
+    auto it = h->eng.find(dim);
+    if (it == h->eng.end()) return set_err(RD_ERR_ARG, "no result");
+    const Engine& e = *it->second;
+    const CloudDesc& cd = e.clouds()[h->cloud_slot[cloud]];
+    const int64_t n = h->ns[cloud];
+    if (n == 0) return RD_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    CK_CUDA(cudaMemcpyAsync(out, e.chosen() + cd.s_off * dim, sizeof(float) * n * dim,
+                            dst_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+    CK_CUDA(cudaStreamSynchronize(st));
+    return RD_OK;
+}
+
+rd_status rd_batch_get_stats(rd_batch* h, rd_run_stats* st)
+{
+    if (!h || !st) return set_err(RD_ERR_ARG, "null argument");
+    fill_stats(h->stats, st);
+    return RD_OK;
+}
+
+rd_status rd_batch_destroy(rd_batch* h)
+{
+    delete h;
+    return RD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,333 @@
+// rd_engine.cu -- host side of the batch engine (see rd_engine_host.hpp).
+#include "rd_engine_host.hpp"
+
+#include <algorithm>
+#include <cstring>
+
+namespace rdb {
+
+cudaError_t DevBuf::ensure(size_t want)
+{
+    if (want == 0) want = 16;
+    if (want <= bytes) return cudaSuccess;
+    release();
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        bytes = 0;
+        return e;
+    }
+    bytes = want;
+    return cudaSuccess;
+}
+
+void DevBuf::release()
+{
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+Engine::Engine() {}
+
+Engine::~Engine()
+{
+    if (exec_) cudaGraphExecDestroy(exec_);
+    if (graph_) cudaGraphDestroy(graph_);
+    if (cap_stream_) cudaStreamDestroy(cap_stream_);
+}
+
+int Engine::fail(const char* what, cudaError_t e)
+{
+    last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return 2;  // RD_ERR_CUDA
+}
+
+#define RD_CK(call)                                   \
+    do {                                              \
+        cudaError_t e_ = (call);                      \
+        if (e_ != cudaSuccess) return fail(#call, e_); \
+    } while (0)
+
+template <class T>
+static cudaError_t upload(DevBuf& b, const std::vector<T>& h, cudaStream_t st)
+{
+    cudaError_t e = b.ensure(sizeof(T) * (h.size() + 1));
+    if (e != cudaSuccess || h.empty()) return e;
+    return cudaMemcpyAsync(b.p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, st);
+}
+
+int Engine::setup(int dim, const std::vector<CloudDesc>& clouds,
+                  const std::vector<GroupDesc>& groups, int64_t total_points)
+{
+    if (dim != 2 && dim != 3) {
+        last_error = "dim must be 2 or 3";
+        return 6;  // RD_ERR_UNSUPPORTED
+    }
+    if (!tune_supported(dim, tune)) {
+        last_error = "unsupported tuning parameters";
+        return 1;
+    }
+    dim_ = dim;
+    total_points_ = total_points;
+    h_cl_ = clouds;
+    h_gr_ = groups;
+    chunk_pts_ = tune.block * tune.items;
+    // chunks and chosen capacity
+    int64_t chunk = 0, s_off = 0;
+    h_chunk_cloud_.clear();
+    for (size_t c = 0; c < h_cl_.size(); ++c) {
+        CloudDesc& cd = h_cl_[c];
+        cd.s_off = s_off;
+        s_off += cd.n_own;
+        cd.chunk_begin = chunk;
+        cd.n_chunks = (cd.n_all + chunk_pts_ - 1) / chunk_pts_;
+        for (int k = 0; k < cd.n_chunks; ++k) h_chunk_cloud_.push_back((int32_t)c);
+        chunk += cd.n_chunks;
+        cd.n_seg = (cd.n_chunks + SEG - 1) / SEG;
+    }
+    n_chunks_ = (int32_t)chunk;
+    const size_t nc = h_cl_.size();
+    RD_CK(bP_.ensure(sizeof(float) * (size_t)(total_points * dim + 4)));
+    RD_CK(bS_.ensure(sizeof(float) * (size_t)(s_off * dim + 4)));
+    RD_CK(bNext_.ensure(sizeof(int32_t) * (size_t)(s_off + 1)));
+    RD_CK(bKeys_.ensure(sizeof(int32_t) * (size_t)(total_points + 1)));
+    RD_CK(bGrouped_.ensure(sizeof(float) * (size_t)(total_points * dim + 4)));
+    RD_CK(bNs_.ensure(4 * (nc + 1)));
+    RD_CK(bPhase_.ensure(4 * (nc + 1)));
+    RD_CK(bCont_.ensure(4 * (nc + 1)));
+    RD_CK(bPasses_.ensure(4 * (nc + 1)));
+    RD_CK(bTotPasses_.ensure(4 * (nc + 1)));
+    RD_CK(bOuter_.ensure(4 * (nc + 1)));
+    RD_CK(bErr_.ensure(4 * (nc + 1)));
+    RD_CK(bPairs_.ensure(8 * (nc + 1)));
+    RD_CK(bCtr_.ensure(4 * CTR_COUNT));
+    return 0;
+}
+
+EngineView Engine::view() const
+{
+    EngineView v;
+    std::memset(&v, 0, sizeof(v));
+    v.cl = bCl_.as<CloudDesc>();
+    v.gr = bGr_.as<GroupDesc>();
+    v.chunk_cloud = bChunkCloud_.as<int32_t>();
+    v.slot_cloud = bSlotCloud_.as<int32_t>();
+    v.seg_list = bSegList_.as<int2>();
+    v.P = bP_.as<float>();
+    v.S = bS_.as<float>();
+    v.keys = bKeys_.as<int32_t>();
+    v.grouped = bGrouped_.as<float>();
+    v.hist = bHist_.as<int32_t>();
+    v.segsum = bSegsum_.as<int32_t>();
+    v.cnt = bCnt_.as<int32_t>();
+    v.base = bBase_.as<int32_t>();
+    v.next = bNext_.as<int32_t>();
+    v.ns = bNs_.as<int32_t>();
+    v.phase = bPhase_.as<int32_t>();
+    v.cont = bCont_.as<int32_t>();
+    v.passes = bPasses_.as<int32_t>();
+    v.total_passes = bTotPasses_.as<int32_t>();
+    v.outer = bOuter_.as<int32_t>();
+    v.err = bErr_.as<int32_t>();
+    v.pairs = bPairs_.as<unsigned long long>();
+    v.ctr = bCtr_.as<int32_t>();
+    v.dx = bDx_.as<float>();
+    v.dcell = bDcell_.as<int32_t>();
+    v.dalive = bDalive_.as<int32_t>();
+    v.dc1 = bDc1_.as<int32_t>();
+    v.dc2 = bDc2_.as<int32_t>();
+    v.dbstart = bDbstart_.as<int32_t>();
+    v.ditems = bDitems_.as<int32_t>();
+    v.dec_hoff = bDecHoff_.as<int64_t>();
+    v.dec_hbits = bDecHbits_.as<int32_t>();
+    v.n_clouds = (int32_t)h_cl_.size();
+    v.n_groups = (int32_t)h_gr_.size();
+    v.n_chunks = n_chunks_;
+    v.n_slots = n_slots_;
+    v.n_segs = n_segs_;
+    v.chunk_pts = chunk_pts_;
+    v.hist_smem = hist_smem_;
+    v.scat_smem = scat_smem_;
+    v.max_passes = max_passes;
+    v.max_outer = max_outer;
+    v.max_iters = max_iters;
+    return v;
+}
+
+static int ceil_log2(int64_t x)
+{
+    int b = 0;
+    while ((int64_t(1) << b) < x) ++b;
+    return b;
+}
+
+int Engine::finish_setup_after_choose(cudaStream_t st)
+{
+    const size_t nc = h_cl_.size();
+    h_ns_.resize(nc);
+    RD_CK(cudaMemcpyAsync(h_ns_.data(), bNs_.p, 4 * nc, cudaMemcpyDeviceToHost, st));
+    RD_CK(cudaStreamSynchronize(st));
+    int64_t hist = 0, seg = 0, key = 0;
+    int max_ns = 0;
+    h_slot_cloud_.clear();
+    h_seg_list_.clear();
+    for (size_t c = 0; c < nc; ++c) {
+        CloudDesc& cd = h_cl_[c];
+        cd.ns_cap = h_ns_[c];
+        max_ns = std::max(max_ns, cd.ns_cap);
+        cd.hist_off = hist;
+        hist += (int64_t)cd.n_chunks * cd.ns_cap;
+        cd.seg_off = seg;
+        seg += (int64_t)cd.n_seg * cd.ns_cap;
+        cd.key_off = key;
+        key += cd.ns_cap;
+        for (int k = 0; k < cd.ns_cap; ++k) h_slot_cloud_.push_back((int32_t)c);
+        if (cd.ns_cap > 0)
+            for (int s = 0; s < cd.n_seg; ++s) h_seg_list_.push_back(make_int2((int)c, s));
+    }
+    n_slots_ = (int32_t)key;
+    n_segs_ = (int32_t)h_seg_list_.size();
+    // group decimation scratch
+    h_dec_hoff_.resize(h_gr_.size());
+    h_dec_hbits_.resize(h_gr_.size());
+    int64_t sscr = 0, hoff = 0;
+    for (size_t g = 0; g < h_gr_.size(); ++g) {
+        GroupDesc& gd = h_gr_[g];
+        int64_t tot = 0;
+        for (int i = 0; i < gd.n_clouds; ++i) tot += h_cl_[gd.cloud_begin + i].ns_cap;
+        gd.s_scratch = sscr;
+        sscr += tot;
+        const int hb = std::min(20, std::max(6, ceil_log2(std::max<int64_t>(tot, 1))));
+        h_dec_hbits_[g] = hb;
+        h_dec_hoff_[g] = hoff;
+        hoff += (int64_t(1) << hb) + 1;
+    }
+    // shared-memory budgets (ints)
+    hist_smem_ = std::min(max_ns, 24 * 1024);
+    scat_smem_ = std::min(max_ns, 12 * 1024);
+    RD_CK(upload(bCl_, h_cl_, st));
+    RD_CK(upload(bGr_, h_gr_, st));
+    RD_CK(upload(bSlotCloud_, h_slot_cloud_, st));
+    RD_CK(upload(bSegList_, h_seg_list_, st));
+    RD_CK(upload(bDecHoff_, h_dec_hoff_, st));
+    RD_CK(upload(bDecHbits_, h_dec_hbits_, st));
+    RD_CK(bHist_.ensure(4 * (size_t)(hist + 1)));
+    RD_CK(bSegsum_.ensure(4 * (size_t)(seg + 1)));
+    RD_CK(bCnt_.ensure(4 * (size_t)(key + 1)));
+    RD_CK(bBase_.ensure(4 * (size_t)(key + 1)));
+    RD_CK(bDx_.ensure(4 * (size_t)(sscr * dim_ + 1)));
+    RD_CK(bDcell_.ensure(4 * (size_t)(sscr * dim_ + 1)));
+    RD_CK(bDalive_.ensure(4 * (size_t)(sscr + 1)));
+    RD_CK(bDc1_.ensure(4 * (size_t)(sscr + 1)));
+    RD_CK(bDc2_.ensure(4 * (size_t)(sscr + 1)));
+    RD_CK(bDitems_.ensure(4 * (size_t)(sscr + 1)));
+    RD_CK(bDbstart_.ensure(4 * (size_t)(hoff + 1)));
+    // persistent assignment grid: every resident CTA slot, at most one per chunk
+    int dev = 0, sms = 0;
+    RD_CK(cudaGetDevice(&dev));
+    RD_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int per_sm = std::max(1, max_assign_blocks_per_sm(dim_, tune, hist_smem_));
+    assign_grid_ = std::max(1, std::min(n_chunks_, sms * per_sm));
+    return 0;
+}
+
+int Engine::build_graph(cudaStream_t st)
+{
+    (void)st;
+    const EngineView v = view();
+    std::vector<unsigned char> key(sizeof(v) + sizeof(TuneParams) + sizeof(int));
+    std::memcpy(key.data(), &v, sizeof(v));
+    std::memcpy(key.data() + sizeof(v), &tune, sizeof(TuneParams));
+    std::memcpy(key.data() + sizeof(v) + sizeof(TuneParams), &assign_grid_, sizeof(int));
+    if (exec_ && key == graph_key_) return 0;
+    if (exec_) { cudaGraphExecDestroy(exec_); exec_ = nullptr; }
+    if (graph_) { cudaGraphDestroy(graph_); graph_ = nullptr; }
+    if (!cap_stream_) RD_CK(cudaStreamCreateWithFlags(&cap_stream_, cudaStreamNonBlocking));
+    RD_CK(cudaGraphCreate(&graph_, 0));
+    cudaGraphConditionalHandle h;
+    RD_CK(cudaGraphConditionalHandleCreate(&h, graph_, 1, cudaGraphCondAssignDefault));
+    alignas(cudaGraphNodeParams) unsigned char cp_raw[sizeof(cudaGraphNodeParams)];
+    std::memset(cp_raw, 0, sizeof(cp_raw));
+    cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cp_raw);
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    RD_CK(cudaGraphAddNode(&node, graph_, nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    RD_CK(cudaStreamBeginCaptureToGraph(cap_stream_, body, nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeThreadLocal));
+    cudaError_t e1 = launch_pass(dim_, v, tune, assign_grid_, cap_stream_);
+    cudaError_t e2 = launch_loopcond(v, h, 1, cap_stream_);
+    cudaGraph_t out = nullptr;
+    cudaError_t e3 = cudaStreamEndCapture(cap_stream_, &out);
+    if (e1 != cudaSuccess) return fail("capture pass", e1);
+    if (e2 != cudaSuccess) return fail("capture loopcond", e2);
+    if (e3 != cudaSuccess) return fail("end capture", e3);
+    RD_CK(cudaGraphInstantiate(&exec_, graph_, 0));
+    graph_key_ = key;
+    return 0;
+}
+
+int Engine::run(cudaStream_t st, bool use_graph)
+{
+    if (h_cl_.empty()) return 0;
+    stats_ = RunStats();
+    RD_CK(upload(bCl_, h_cl_, st));
+    RD_CK(upload(bGr_, h_gr_, st));
+    RD_CK(upload(bChunkCloud_, h_chunk_cloud_, st));
+    {
+        EngineView v0 = view();
+        RD_CK(launch_reset(v0, st));
+        RD_CK(launch_choose(dim_, v0, st));
+    }
+    if (int rc = finish_setup_after_choose(st)) return rc;
+    const EngineView v = view();
+    RD_CK(prepare_pass(dim_, v, tune));
+    if (use_graph) {
+        if (int rc = build_graph(st)) return rc;
+        RD_CK(cudaGraphLaunch(exec_, st));
+    } else {
+        for (;;) {
+            RD_CK(launch_pass(dim_, v, tune, assign_grid_, st));
+            RD_CK(launch_loopcond(v, cudaGraphConditionalHandle(), 0, st));
+            int32_t act = 0;
+            RD_CK(cudaMemcpyAsync(&act, v.ctr + CTR_ACTIVE, 4, cudaMemcpyDeviceToHost, st));
+            RD_CK(cudaStreamSynchronize(st));
+            if (act == 0) break;
+        }
+    }
+    // results
+    const size_t nc = h_cl_.size();
+    std::vector<int32_t> tp(nc);
+    std::vector<unsigned long long> pr(nc);
+    int32_t ctr[CTR_COUNT];
+    h_err_.resize(nc);
+    RD_CK(cudaMemcpyAsync(h_ns_.data(), bNs_.p, 4 * nc, cudaMemcpyDeviceToHost, st));
+    RD_CK(cudaMemcpyAsync(h_err_.data(), bErr_.p, 4 * nc, cudaMemcpyDeviceToHost, st));
+    RD_CK(cudaMemcpyAsync(tp.data(), bTotPasses_.p, 4 * nc, cudaMemcpyDeviceToHost, st));
+    RD_CK(cudaMemcpyAsync(pr.data(), bPairs_.p, 8 * nc, cudaMemcpyDeviceToHost, st));
+    RD_CK(cudaMemcpyAsync(ctr, bCtr_.p, sizeof(ctr), cudaMemcpyDeviceToHost, st));
+    RD_CK(cudaStreamSynchronize(st));
+    stats_.loop_iters = ctr[CTR_ITERS];
+    stats_.err_bits = ctr[CTR_ERR];
+    for (size_t c = 0; c < nc; ++c) {
+        stats_.total_passes += tp[c];
+        stats_.max_passes = std::max<int64_t>(stats_.max_passes, tp[c]);
+        stats_.pairs += (double)pr[c];
+        stats_.err_bits |= h_err_[c];
+    }
+    if (stats_.err_bits & (ERRB_EVOLVE_CAP | ERRB_OUTER_CAP | ERRB_DEC_CAP)) {
+        last_error = "iteration limit reached before convergence";
+        return 4;  // RD_ERR_NOT_CONVERGED
+    }
+    if (stats_.err_bits & ERRB_CAPACITY) {
+        last_error = "device capacity exceeded";
+        return 3;
+    }
+    return 0;
+}
+
+}  // namespace rdb

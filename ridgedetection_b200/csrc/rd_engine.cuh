@@ -1,0 +1,99 @@
+// rd_engine.cuh -- the device-side batch engine shared by every entry point.
+//
+// One engine run solves a batch of independent "clouds" (see CloudDesc) that
+// share the point dimension DIM:
+//   choose      one CTA per cloud, greedy r1-separated subset in input order
+//               over a hashed uniform grid (exact test, grid only prunes);
+//   evolve      passes of  assign -> column scan -> segment scan -> stable
+//               scatter -> ordered sum + shift -> control, over all clouds still
+//               evolving; the per-chosen coordinate sums are formed in cloud-point
+//               index order, exactly as the reference's serial loop forms them;
+//   decimate    one CTA per group with the reference's in-order semantics;
+//   loop        a device flag says whether any cloud is unfinished; it drives a
+//               CUDA-graph WHILE node (graph mode) or is read by the host (plain).
+#pragma once
+
+#include "rd_internal.cuh"
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace rdb {
+
+enum : int {
+    CTR_WORK = 0,      // assignment work ticket
+    CTR_ACTIVE = 1,    // unfinished clouds after the last control step
+    CTR_ITERS = 2,     // loop iterations run
+    CTR_ERR = 3,       // OR of global error bits
+    CTR_COUNT = 8,
+};
+
+struct EngineView {
+    const CloudDesc* cl;
+    const GroupDesc* gr;
+    const int32_t* chunk_cloud;  // chunk -> cloud
+    const int32_t* slot_cloud;   // chosen slot -> cloud
+    const int2* seg_list;        // (cloud, segment) pairs
+    float* P;                    // packed evolve points, ROW_MAJOR
+    float* S;                    // chosen points, ROW_MAJOR, capacity n_own per cloud
+    int32_t* keys;               // per point slot: assigned chosen index or -1
+    float* grouped;              // per point slot: points regrouped by key
+    int32_t* hist;               // per cloud: n_chunks x ns_cap key histogram
+    int32_t* segsum;             // per cloud: n_seg x ns_cap segment sums
+    int32_t* cnt;                // per chosen slot: members in the last pass
+    int32_t* base;               // per chosen slot: first grouped slot
+    int32_t* hash;               // choose hash heads
+    int32_t* next;               // per chosen slot: choose hash chain
+    int32_t* ns;                 // per cloud: current chosen count
+    int32_t* phase;              // per cloud: PH_*
+    int32_t* cont;               // per cloud: a coordinate moved in this pass
+    int32_t* passes;             // per cloud: passes of the current evolve run
+    int32_t* total_passes;       // per cloud: all passes
+    int32_t* outer;              // per cloud: evolve/decimate rounds
+    int32_t* err;                // per cloud: ERRB_* bits
+    unsigned long long* pairs;   // per cloud: sum over passes of n_all * ns
+    int32_t* ctr;                // CTR_* counters
+    // decimation scratch, per group (offsets in GroupDesc / dec_hoff)
+    float* dx;                   // coordinates of the group's chosen points
+    int32_t* dcell;              // their grid cells
+    int32_t* dalive;
+    int32_t* dc1;                // alive neighbours within r2 (self included)
+    int32_t* dc2;                // alive neighbours within 2*r2 (self included)
+    int32_t* dbstart;            // bucket starts (HB+1 per group)
+    int32_t* ditems;             // bucket members
+    const int64_t* dec_hoff;     // per group: start of its bucket arrays
+    const int32_t* dec_hbits;    // per group: log2 buckets
+    int32_t n_clouds;
+    int32_t n_groups;
+    int32_t n_chunks;
+    int32_t n_slots;
+    int32_t n_segs;
+    int32_t chunk_pts;           // points per assignment chunk
+    int32_t hist_smem;           // ints of dynamic smem for the assign histogram
+    int32_t scat_smem;           // ints of dynamic smem per scatter warp
+    int32_t max_passes;
+    int32_t max_outer;
+    int32_t max_iters;
+};
+
+// launch configuration picked by the tuner per (dim, cloud size) bucket
+struct TuneParams {
+    int block;     // assign CTA size
+    int items;     // points per assign thread
+};
+
+// host-side launchers (rd_kernels.cu); all enqueue on `st`
+cudaError_t launch_choose(int dim, const EngineView& v, cudaStream_t st);
+cudaError_t prepare_pass(int dim, const EngineView& v, const TuneParams& tp);
+cudaError_t launch_pass(int dim, const EngineView& v, const TuneParams& tp, int assign_grid,
+                        cudaStream_t st);
+cudaError_t launch_loopcond(const EngineView& v, cudaGraphConditionalHandle h, int use_handle,
+                            cudaStream_t st);
+cudaError_t launch_reset(const EngineView& v, cudaStream_t st);
+int assign_smem_bytes(int dim, const TuneParams& tp, int hist_ints);
+int max_assign_blocks_per_sm(int dim, const TuneParams& tp, int hist_ints);
+bool tune_supported(int dim, const TuneParams& tp);
+
+}  // namespace rdb

@@ -1,0 +1,99 @@
+// rd_engine_host.hpp -- host side of the batch engine: device buffers, work
+// decomposition, the CUDA-graph WHILE loop and the host-synchronised loop.
+#pragma once
+
+#include "rd_engine.cuh"
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace rdb {
+
+// A device buffer that only grows; reused across runs of one engine.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t want);
+    void release();
+    ~DevBuf() { release(); }
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+struct RunStats {
+    int64_t loop_iters = 0;       // graph/host loop iterations
+    int64_t total_passes = 0;     // sum over clouds of evolve passes
+    int64_t max_passes = 0;       // max over clouds
+    double pairs = 0;             // sum over clouds of sum over passes of n_all*ns
+    int err_bits = 0;
+};
+
+class Engine {
+public:
+    Engine();
+    ~Engine();
+    Engine(const Engine&) = delete;
+    Engine& operator=(const Engine&) = delete;
+
+    // Describe the batch.  Clouds must be given with p_off, n_all, n_own, r1,
+    // r2 and group filled in; groups with cloud_begin/n_clouds/nocopy.  The
+    // clouds of a group must be contiguous and share r2.
+    int setup(int dim, const std::vector<CloudDesc>& clouds, const std::vector<GroupDesc>& groups,
+              int64_t total_points);
+
+    float* points() { return bP_.as<float>(); }     // packed ROW_MAJOR evolve points
+    int64_t total_points() const { return total_points_; }
+    int dim() const { return dim_; }
+
+    // choose -> (evolve -> decimate)* on `st`.  use_graph selects the CUDA
+    // graph WHILE loop; otherwise the host reads the loop flag after each
+    // iteration (the reference's style).  Blocks until the run is complete.
+    int run(cudaStream_t st, bool use_graph);
+
+    // results, valid after run(): per-cloud chosen count and device pointer
+    const std::vector<int32_t>& ns() const { return h_ns_; }
+    const std::vector<CloudDesc>& clouds() const { return h_cl_; }
+    const float* chosen() const { return bS_.as<float>(); }
+    const RunStats& stats() const { return stats_; }
+    const std::vector<int32_t>& cloud_err() const { return h_err_; }
+
+    // limits (the reference has none; these keep every loop bounded)
+    int max_passes = 1 << 16;
+    int max_outer = 4096;
+    int max_iters = 1 << 18;
+    TuneParams tune{128, 8};
+    std::string last_error;
+
+private:
+    int finish_setup_after_choose(cudaStream_t st);
+    int build_graph(cudaStream_t st);
+    EngineView view() const;
+    int fail(const char* what, cudaError_t e);
+
+    int dim_ = 0;
+    int64_t total_points_ = 0;
+    std::vector<CloudDesc> h_cl_;
+    std::vector<GroupDesc> h_gr_;
+    std::vector<int32_t> h_chunk_cloud_, h_slot_cloud_, h_ns_, h_err_;
+    std::vector<int2> h_seg_list_;
+    std::vector<int64_t> h_dec_hoff_;
+    std::vector<int32_t> h_dec_hbits_;
+    int32_t n_chunks_ = 0, n_slots_ = 0, n_segs_ = 0;
+    int chunk_pts_ = 1024;
+    int hist_smem_ = 0, scat_smem_ = 0;
+    int assign_grid_ = 0;
+    RunStats stats_;
+
+    DevBuf bCl_, bGr_, bChunkCloud_, bSlotCloud_, bSegList_;
+    DevBuf bP_, bS_, bKeys_, bGrouped_, bHist_, bSegsum_, bCnt_, bBase_, bNext_;
+    DevBuf bNs_, bPhase_, bCont_, bPasses_, bTotPasses_, bOuter_, bErr_, bPairs_, bCtr_;
+    DevBuf bDx_, bDcell_, bDalive_, bDc1_, bDc2_, bDbstart_, bDitems_, bDecHoff_, bDecHbits_;
+
+    cudaStream_t cap_stream_ = nullptr;
+    cudaGraphExec_t exec_ = nullptr;
+    cudaGraph_t graph_ = nullptr;
+    std::vector<unsigned char> graph_key_;
+};
+
+}  // namespace rdb

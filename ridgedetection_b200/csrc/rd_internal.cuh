@@ -1,0 +1,117 @@
+// rd_internal.cuh -- shared device-side definitions of the B200 ridge-detection
+// engine: per-cloud descriptors, exact FP32 arithmetic helpers and error bits.
+//
+// Exactness contract.  Every floating-point result that decides a discrete
+// outcome (a choose, an assignment, a movement test, a decimation count) or that
+// is written back as a chosen coordinate is computed with explicitly rounded
+// intrinsics (__fsub_rn/__fmul_rn/__fadd_rn/__fdiv_rn), in the operation order of
+// the reference CPU code, so nvcc cannot contract a multiply and an add into an
+// FMA.  With that, the GPU path reproduces the reference's serial CPU output bit
+// for bit:
+//   squared distance   t = a - b; acc += t*t, d = 0..DIM-1    rd/cpu/brute_force/rd_inner.hpp:42-49
+//   argmin             strict '<', lowest index wins ties     rd/cpu/brute_force/evolve.hpp:54-65
+//   membership         min <= r1*r1                            rd/cpu/brute_force/evolve.hpp:66
+//   centroid sums      FP32, in cloud-point index order        rd/cpu/brute_force/evolve.hpp:66-75
+//   shift test         |mc - c| > 2.f*|mc|*cnt*FLT_EPSILON     rd/cpu/brute_force/evolve.hpp:151-153
+#pragma once
+
+#include <cfloat>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace rdb {
+
+// ---------------------------------------------------------------------------
+// error bits recorded on the device (per cloud and globally); the host turns
+// them into rd_status codes.  No kernel ever traps.
+// ---------------------------------------------------------------------------
+enum : int {
+    ERRB_EVOLVE_CAP = 1 << 0,   // evolve pass limit reached before convergence
+    ERRB_OUTER_CAP = 1 << 1,    // outer (evolve/decimate) iteration limit reached
+    ERRB_CAPACITY = 1 << 2,     // a device buffer would have overflowed
+    ERRB_DEC_CAP = 1 << 3,      // decimation pass limit reached
+};
+
+// phases of one cloud's state machine
+enum : int {
+    PH_EVOLVE = 0,      // evolve passes running
+    PH_CONVERGED = 1,   // evolve converged, waiting for its group's decimation
+    PH_DONE = 2,        // chosen count stable: finished
+};
+
+// Per-cloud descriptor.  A "cloud" is a set of evolve points with its own chosen
+// set: a whole input cloud for the brute-force and batched paths, or one leaf
+// tile (own points first, then its r1 halo) for the tiled path.  Clouds of one
+// group are decimated together (a tiled run is a single group; every
+// brute-force cloud is its own group).
+struct CloudDesc {
+    int64_t p_off;       // first point slot of this cloud in the packed point array
+    int32_t n_all;       // evolve points (own + halo)
+    int32_t n_own;       // choose points (own points; == n_all for brute force)
+    float r1, r2;
+    int64_t s_off;       // first chosen slot (capacity n_own)
+    int64_t chunk_begin; // first assignment chunk of this cloud
+    int32_t n_chunks;
+    int32_t group;
+    int64_t hist_off;    // start of this cloud's chunk x key histogram (set after choose)
+    int32_t n_seg;       // ceil(n_chunks / SEG)
+    int32_t ns_cap;      // chosen count right after choose (hist row length)
+    int64_t seg_off;     // start of this cloud's segment x key sums
+    int64_t key_off;     // start of this cloud's per-chosen arrays (cnt/base)
+    int64_t hash_off;    // start of this cloud's choose hash heads
+    int32_t hash_bits;   // log2 of the number of hash buckets
+    int32_t pad;
+};
+
+struct GroupDesc {
+    int32_t cloud_begin;
+    int32_t n_clouds;
+    int32_t nocopy;      // decimateNoCopy semantics (tiled) instead of decimate
+    int32_t pad;
+    int64_t s_scratch;   // scratch slots for the group's decimation
+};
+
+constexpr int SEG = 16;  // histogram rows per segment in the column scan
+
+// ---------------------------------------------------------------------------
+// exact FP32 helpers
+// ---------------------------------------------------------------------------
+template <int DIM>
+__device__ __forceinline__ float sqdist_exact(const float* a, const float* b)
+{
+    float t = __fsub_rn(a[0], b[0]);
+    float acc = __fmul_rn(t, t);  // 0 + t*t == t*t exactly
+#pragma unroll
+    for (int d = 1; d < DIM; ++d) {
+        t = __fsub_rn(a[d], b[d]);
+        acc = __fadd_rn(acc, __fmul_rn(t, t));
+    }
+    return acc;
+}
+
+__device__ __forceinline__ float sqr_rn(float r) { return __fmul_rn(r, r); }
+
+// shift of one coordinate (rd/cpu/brute_force/evolve.hpp:143-177); returns 1
+// when the coordinate moved.
+__device__ __forceinline__ int shift_coord(float sum, int cnt, float& c)
+{
+    const float fc = (float)cnt;
+    const float mc = __fdiv_rn(sum, fc);
+    float thr = __fmul_rn(2.0f, fabsf(mc));
+    thr = __fmul_rn(thr, fc);
+    thr = __fmul_rn(thr, FLT_EPSILON);
+    if (fabsf(__fsub_rn(mc, c)) > thr) {
+        c = mc;
+        return 1;
+    }
+    return 0;
+}
+
+__device__ __forceinline__ unsigned lanemask_lt()
+{
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+}  // namespace rdb

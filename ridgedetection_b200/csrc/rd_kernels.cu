@@ -1,0 +1,915 @@
+// rd_kernels.cu -- sm_100a kernels of the batch engine (see rd_engine.cuh).
+//
+// All arithmetic is FP32 on the CUDA cores.  The point/chosen contraction has
+// K = DIM <= 3, far too thin for tcgen05 tiles, and the reference's rounding
+// (sub, mul, add, each rounded) rules out the |p|^2 - 2 p.c + |c|^2 expansion a
+// tensor-core formulation would need, so the hot loop is a register-blocked
+// SIMT kernel instead: each thread holds ITEMS cloud points, the chosen set
+// streams through shared memory, and every pair costs DIM sub + DIM mul +
+// (DIM-1) add + compare + 2 selects, all explicitly rounded.
+#include "rd_engine.cuh"
+
+#include <cuda_runtime.h>
+
+namespace rdb {
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+template <int DIM>
+struct Pow3 { static constexpr int v = 3 * Pow3<DIM - 1>::v; };
+template <>
+struct Pow3<0> { static constexpr int v = 1; };
+
+__device__ __forceinline__ int cell_of(float x, double inv)
+{
+    double c = floor((double)x * inv);
+    c = fmin(fmax(c, -1073741824.0), 1073741823.0);
+    return (int)c;
+}
+
+template <int DIM>
+__device__ __forceinline__ uint32_t cell_hash(const int* c)
+{
+    uint32_t h = 2166136261u;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) h = (h ^ (uint32_t)c[d]) * 16777619u;
+    return h ^ (h >> 15);
+}
+
+// offset o in [0, 3^DIM) -> neighbour cell; o == (3^DIM-1)/2 is the home cell
+template <int DIM>
+__device__ __forceinline__ void neighbour_cell(const int* cc, int o, int* out)
+{
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        out[d] = cc[d] + (o % 3) - 1;
+        o /= 3;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// choose: rd/cpu/brute_force/choose.hpp:37-70, one CTA per cloud.
+// Blocks of BLOCK points are visited in order.  Phase 1 (all threads) drops
+// every point that has a chosen point within r1 among those chosen by earlier
+// blocks, looked up through a hashed grid of cell edge > r1 (the grid only
+// prunes; the test itself is the exact FP32 one).  Phase 2 (warp 0) walks the
+// survivors in order and re-tests each against the grid, which by then also
+// holds the points chosen earlier in the same block, so the outcome is the
+// sequential greedy one.  Chosen coordinates and hash chains are mirrored in
+// shared memory for the first SCAP chosen points.
+// ---------------------------------------------------------------------------
+template <int DIM>
+struct ChooseSmem {
+    static constexpr int HBITS = 13;
+    static constexpr int HB = 1 << HBITS;
+    static constexpr int SCAP = (DIM <= 2) ? 6144 : 4096;
+};
+
+template <int DIM, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_choose(EngineView v)
+{
+    using CS = ChooseSmem<DIM>;
+    constexpr int NB = Pow3<DIM>::v;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    int32_t* s_heads = reinterpret_cast<int32_t*>(smem_raw);          // HB
+    int32_t* s_next = s_heads + CS::HB;                                // SCAP
+    float* s_S = reinterpret_cast<float*>(s_next + CS::SCAP);          // SCAP*DIM
+    float* s_sp = s_S + CS::SCAP * DIM;                                // BLOCK*DIM
+    int32_t* s_scell = reinterpret_cast<int32_t*>(s_sp + BLOCK * DIM); // BLOCK*DIM
+    __shared__ int s_ns, s_nsurv;
+    __shared__ int s_wsum[BLOCK / 32];
+
+    const int c = blockIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const CloudDesc cd = v.cl[c];
+    const int n = cd.n_own;
+    const float rsq = sqr_rn(cd.r1);
+    const double inv = 1.0 / ((double)cd.r1 * (1.0 + 1.0 / 1024.0));
+    const uint32_t hmask = CS::HB - 1;
+    float* gS = v.S + cd.s_off * DIM;
+    int32_t* gnext = v.next + cd.s_off;
+    const float* P = v.P + cd.p_off * DIM;
+
+    for (int h = tid; h < CS::HB; h += BLOCK) s_heads[h] = -1;
+    if (tid == 0) s_ns = 0;
+    __syncthreads();
+
+    auto coord = [&](int q, int d) -> float {
+        return (q < CS::SCAP) ? s_S[q * DIM + d] : gS[(int64_t)q * DIM + d];
+    };
+    auto nxt = [&](int q) -> int { return (q < CS::SCAP) ? s_next[q] : gnext[q]; };
+    // any chosen point within r1 of p, over the given neighbour cells
+    auto query = [&](const float* p, const int* cc, int o) -> bool {
+        int nc[DIM];
+        neighbour_cell<DIM>(cc, o, nc);
+        int q = s_heads[cell_hash<DIM>(nc) & hmask];
+        while (q >= 0) {
+            float s[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) s[d] = coord(q, d);
+            if (sqdist_exact<DIM>(p, s) <= rsq) return true;
+            q = nxt(q);
+        }
+        return false;
+    };
+
+    for (int base = 0; base < n; base += BLOCK) {
+        const int i = base + tid;
+        const bool valid = i < n;
+        float p[DIM];
+        int cc[DIM];
+        bool surv = false;
+        if (valid) {
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                p[d] = P[(int64_t)i * DIM + d];
+                cc[d] = cell_of(p[d], inv);
+            }
+            bool hit = false;
+            for (int t = 0; t < NB && !hit; ++t) hit = query(p, cc, (t + NB / 2) % NB);
+            surv = !hit;
+        }
+        // compact survivors in visiting order
+        const unsigned bal = __ballot_sync(FULL, surv);
+        if (lane == 0) s_wsum[warp] = __popc(bal);
+        __syncthreads();
+        int wbase = 0, tot = 0;
+        for (int w = 0; w < BLOCK / 32; ++w) {
+            const int x = s_wsum[w];
+            wbase += (w < warp) ? x : 0;
+            tot += x;
+        }
+        if (surv) {
+            const int pos = wbase + __popc(bal & lanemask_lt());
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                s_sp[pos * DIM + d] = p[d];
+                s_scell[pos * DIM + d] = cc[d];
+            }
+        }
+        __syncthreads();
+        if (warp == 0) {
+            int ns = s_ns;
+            for (int sidx = 0; sidx < tot; ++sidx) {
+                float ps[DIM];
+                int cs[DIM];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) {
+                    ps[d] = s_sp[sidx * DIM + d];
+                    cs[d] = s_scell[sidx * DIM + d];
+                }
+                bool hit = false;
+                for (int o = lane; o < NB; o += 32) hit = hit || query(ps, cs, o);
+                hit = __any_sync(FULL, hit);
+                if (!hit) {
+                    if (lane == 0) {
+                        const uint32_t b = cell_hash<DIM>(cs) & hmask;
+                        const int head = s_heads[b];
+#pragma unroll
+                        for (int d = 0; d < DIM; ++d) gS[(int64_t)ns * DIM + d] = ps[d];
+                        if (ns < CS::SCAP) {
+#pragma unroll
+                            for (int d = 0; d < DIM; ++d) s_S[ns * DIM + d] = ps[d];
+                            s_next[ns] = head;
+                        } else {
+                            gnext[ns] = head;
+                        }
+                        s_heads[b] = ns;
+                    }
+                    ++ns;
+                }
+                __syncwarp();
+            }
+            if (lane == 0) s_ns = ns;
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        v.ns[c] = s_ns;
+        v.phase[c] = (s_ns > 0) ? PH_EVOLVE : PH_DONE;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// assign: rd/cpu/brute_force/evolve.hpp:43-66 over one chunk of CHUNK cloud
+// points per work item; writes the key of every point and the chunk's key
+// histogram row.  This is the hot kernel.
+// ---------------------------------------------------------------------------
+template <int DIM>
+struct PadDim { static constexpr int v = (DIM == 3) ? 4 : DIM; };
+
+template <int DIM>
+__device__ __forceinline__ void load_chosen(const float* sS, int kk, float* s)
+{
+    constexpr int DP = PadDim<DIM>::v;
+    if constexpr (DP == 4) {
+        const float4 t = reinterpret_cast<const float4*>(sS)[kk];
+        s[0] = t.x; s[1] = t.y; s[2] = t.z;
+        if constexpr (DIM == 4) s[3] = t.w;
+    } else if constexpr (DP == 2) {
+        const float2 t = reinterpret_cast<const float2*>(sS)[kk];
+        s[0] = t.x; s[1] = t.y;
+    } else {
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) s[d] = sS[kk * DP + d];
+    }
+}
+
+constexpr int ASSIGN_TS = 1024;  // chosen points per shared-memory tile
+
+template <int DIM, int BLOCK, int ITEMS>
+__global__ void __launch_bounds__(BLOCK) k_assign(EngineView v)
+{
+    constexpr int DP = PadDim<DIM>::v;
+    constexpr int TS = ASSIGN_TS;
+    __shared__ __align__(16) float sS[TS * DP];
+    __shared__ int s_item;
+    extern __shared__ int s_hist[];
+    const int tid = threadIdx.x;
+
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(&v.ctr[CTR_WORK], 1);
+        __syncthreads();
+        const int item = s_item;
+        __syncthreads();
+        if (item >= v.n_chunks) break;
+        const int c = v.chunk_cloud[item];
+        if (v.phase[c] != PH_EVOLVE) continue;
+        const CloudDesc cd = v.cl[c];
+        const int lc = item - (int)cd.chunk_begin;
+        const int start = lc * (BLOCK * ITEMS);
+        const int n = cd.n_all;
+        const int ns = v.ns[c];
+        const float* P = v.P + cd.p_off * DIM;
+        const float* gS = v.S + cd.s_off * DIM;
+
+        float p[ITEMS][DIM];
+        float best[ITEMS];
+        int bi[ITEMS];
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            const int i = start + j * BLOCK + tid;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) p[j][d] = (i < n) ? P[(int64_t)i * DIM + d] : 0.0f;
+            best[j] = FLT_MAX;
+            bi[j] = -1;
+        }
+        for (int t0 = 0; t0 < ns; t0 += TS) {
+            const int tl = min(TS, ns - t0);
+            __syncthreads();
+            for (int e = tid; e < tl; e += BLOCK) {
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) sS[e * DP + d] = gS[(int64_t)(t0 + e) * DIM + d];
+            }
+            __syncthreads();
+#pragma unroll 4
+            for (int kk = 0; kk < tl; ++kk) {
+                float s[DIM];
+                load_chosen<DIM>(sS, kk, s);
+                const int k = t0 + kk;
+#pragma unroll
+                for (int j = 0; j < ITEMS; ++j) {
+                    const float sq = sqdist_exact<DIM>(s, p[j]);
+                    const bool lt = sq < best[j];
+                    best[j] = lt ? sq : best[j];
+                    bi[j] = lt ? k : bi[j];
+                }
+            }
+        }
+        const float rsq = sqr_rn(cd.r1);
+        int key[ITEMS];
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            const int i = start + j * BLOCK + tid;
+            key[j] = (i < n && best[j] <= rsq) ? bi[j] : -1;
+            if (i < n) v.keys[cd.p_off + i] = key[j];
+        }
+        // chunk histogram row (row length ns_cap, first ns entries used)
+        int32_t* row = v.hist + cd.hist_off + (int64_t)lc * cd.ns_cap;
+        if (ns <= v.hist_smem) {
+            for (int k = tid; k < ns; k += BLOCK) s_hist[k] = 0;
+            __syncthreads();
+#pragma unroll
+            for (int j = 0; j < ITEMS; ++j)
+                if (key[j] >= 0) atomicAdd(&s_hist[key[j]], 1);
+            __syncthreads();
+            for (int k = tid; k < ns; k += BLOCK) row[k] = s_hist[k];
+        } else {
+            for (int k = tid; k < ns; k += BLOCK) row[k] = 0;
+            __syncthreads();
+#pragma unroll
+            for (int j = 0; j < ITEMS; ++j)
+                if (key[j] >= 0) atomicAdd(&row[key[j]], 1);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// column scan: per (cloud, segment of SEG chunk rows) and key, in-place
+// exclusive prefix down the rows and the segment total.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_colscan(EngineView v)
+{
+    const int item = blockIdx.x;
+    if (item >= v.n_segs) return;
+    const int2 cs = v.seg_list[item];
+    const int c = cs.x, seg = cs.y;
+    if (v.phase[c] != PH_EVOLVE) return;
+    const CloudDesc cd = v.cl[c];
+    const int ns = v.ns[c];
+    const int r0 = seg * SEG;
+    const int rows = min(SEG, cd.n_chunks - r0);
+    int32_t* h = v.hist + cd.hist_off + (int64_t)r0 * cd.ns_cap;
+    int32_t* out = v.segsum + cd.seg_off + (int64_t)seg * cd.ns_cap;
+    for (int k = threadIdx.x; k < ns; k += blockDim.x) {
+        int run = 0;
+        for (int r = 0; r < rows; ++r) {
+            const int x = h[(int64_t)r * cd.ns_cap + k];
+            h[(int64_t)r * cd.ns_cap + k] = run;
+            run += x;
+        }
+        out[k] = run;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// segment scan + key bases: one CTA per cloud.  Exclusive prefix of the
+// segment totals per key (in place), member count per key, and the exclusive
+// prefix of the counts over keys (first grouped slot of each key).
+// ---------------------------------------------------------------------------
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_segscan(EngineView v)
+{
+    const int c = blockIdx.x;
+    if (v.phase[c] != PH_EVOLVE) return;
+    const CloudDesc cd = v.cl[c];
+    const int ns = v.ns[c];
+    int32_t* sg = v.segsum + cd.seg_off;
+    int32_t* cnt = v.cnt + cd.key_off;
+    int32_t* base = v.base + cd.key_off;
+    for (int k = threadIdx.x; k < ns; k += BLOCK) {
+        int run = 0;
+        for (int s = 0; s < cd.n_seg; ++s) {
+            const int x = sg[(int64_t)s * cd.ns_cap + k];
+            sg[(int64_t)s * cd.ns_cap + k] = run;
+            run += x;
+        }
+        cnt[k] = run;
+    }
+    __syncthreads();
+    __shared__ int s_w[BLOCK / 32];
+    __shared__ int s_carry;
+    if (threadIdx.x == 0) s_carry = 0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k0 = 0; k0 < ns; k0 += BLOCK) {
+        __syncthreads();
+        const int k = k0 + threadIdx.x;
+        const int x = (k < ns) ? cnt[k] : 0;
+        int incl = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) s_w[warp] = incl;
+        __syncthreads();
+        int wpre = 0, tot = 0;
+        for (int w = 0; w < BLOCK / 32; ++w) {
+            wpre += (w < warp) ? s_w[w] : 0;
+            tot += s_w[w];
+        }
+        const int carry = s_carry;
+        if (k < ns) base[k] = carry + wpre + incl - x;
+        __syncthreads();
+        if (threadIdx.x == 0) s_carry = carry + tot;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// stable scatter: one warp per chunk walks its points in index order and
+// writes each assigned point to the next free slot of its key's segment, so
+// every segment lists its members in cloud-point index order.
+// ---------------------------------------------------------------------------
+template <int DIM>
+__global__ void __launch_bounds__(128) k_scatter(EngineView v)
+{
+    extern __shared__ int s_ctr_all[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int item = blockIdx.x * 4 + warp;
+    if (item >= v.n_chunks) return;
+    const int c = v.chunk_cloud[item];
+    if (v.phase[c] != PH_EVOLVE) return;
+    const CloudDesc cd = v.cl[c];
+    const int ns = v.ns[c];
+    const int lc = item - (int)cd.chunk_begin;
+    const int seg = lc / SEG;
+    int32_t* row = v.hist + cd.hist_off + (int64_t)lc * cd.ns_cap;
+    const int32_t* sg = v.segsum + cd.seg_off + (int64_t)seg * cd.ns_cap;
+    const int32_t* bs = v.base + cd.key_off;
+    const bool in_smem = ns <= v.scat_smem;
+    int32_t* ctr = in_smem ? (s_ctr_all + warp * v.scat_smem) : row;
+    for (int k = lane; k < ns; k += 32) ctr[k] = bs[k] + sg[k] + row[k];
+    __syncwarp();
+    const int start = lc * v.chunk_pts;
+    const int end = min(cd.n_all, start + v.chunk_pts);
+    const int32_t* keys = v.keys + cd.p_off;
+    const float* P = v.P + cd.p_off * DIM;
+    float* G = v.grouped + cd.p_off * DIM;
+    for (int off = start; off < end; off += 32) {
+        const int i = off + lane;
+        const int key = (i < end) ? keys[i] : -1;
+        const unsigned m = __match_any_sync(FULL, key);
+        const int leader = __ffs(m) - 1;
+        int b = 0;
+        if (key >= 0 && lane == leader) {
+            b = ctr[key];
+            ctr[key] = b + __popc(m);
+        }
+        b = __shfl_sync(FULL, b, leader);
+        if (key >= 0) {
+            const int pos = b + __popc(m & lanemask_lt());
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) G[(int64_t)pos * DIM + d] = P[(int64_t)i * DIM + d];
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// ordered sum + shift: one warp per chosen slot.  Lane d (< DIM) folds
+// coordinate d of the key's members in index order with rounded adds,
+// exactly as rd/cpu/brute_force/evolve.hpp:71-74 accumulates, then applies the
+// movement test of evolve.hpp:143-177.
+// ---------------------------------------------------------------------------
+template <int DIM>
+__global__ void __launch_bounds__(256) k_sum_shift(EngineView v)
+{
+    __shared__ float s_buf[8][32 * DIM];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = blockIdx.x * 8 + warp;
+    if (g >= v.n_slots) return;
+    const int c = v.slot_cloud[g];
+    if (v.phase[c] != PH_EVOLVE) return;
+    const CloudDesc cd = v.cl[c];
+    const int k = g - (int)cd.key_off;
+    if (k >= v.ns[c]) return;
+    const int n = v.cnt[cd.key_off + k];
+    if (n == 0) return;
+    const float* G = v.grouped + (cd.p_off + v.base[cd.key_off + k]) * DIM;
+    float* buf = s_buf[warp];
+    float sum = 0.0f;
+    for (int off = 0; off < n; off += 32) {
+        const int m = min(32, n - off);
+        for (int e = lane; e < m * DIM; e += 32) buf[e] = G[(int64_t)off * DIM + e];
+        __syncwarp();
+        if (lane < DIM)
+            for (int j = 0; j < m; ++j) sum = __fadd_rn(sum, buf[j * DIM + lane]);
+        __syncwarp();
+    }
+    int moved = 0;
+    if (lane < DIM) {
+        float* s = v.S + (cd.s_off + k) * DIM + lane;
+        float cval = *s;
+        moved = shift_coord(sum, n, cval);
+        if (moved) *s = cval;
+    }
+    if (__any_sync(FULL, moved) && lane == 0) v.cont[c] = 1;
+}
+
+// ---------------------------------------------------------------------------
+// control: one thread per cloud after each pass.
+// ---------------------------------------------------------------------------
+__global__ void k_control(EngineView v)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (blockIdx.x == 0 && threadIdx.x == 0) v.ctr[CTR_WORK] = 0;
+    if (c >= v.n_clouds) return;
+    if (v.phase[c] != PH_EVOLVE) return;
+    const CloudDesc cd = v.cl[c];
+    v.pairs[c] += (unsigned long long)cd.n_all * (unsigned long long)v.ns[c];
+    v.passes[c] += 1;
+    v.total_passes[c] += 1;
+    if (v.cont[c] == 0) {
+        v.phase[c] = PH_CONVERGED;
+    } else if (v.passes[c] >= v.max_passes) {
+        v.err[c] |= ERRB_EVOLVE_CAP;
+        v.phase[c] = PH_CONVERGED;
+    }
+    v.cont[c] = 0;
+}
+
+// ---------------------------------------------------------------------------
+// decimate: one CTA per group, rd/cpu/brute_force/decimate.hpp:41-81 (brute
+// force) or :85-127 (decimateNoCopy, tiled), on the group's chosen points in
+// cloud order.  Neighbour counts within r2 and 2*r2 (self included) come from a
+// hashed grid of cell edge > 2*r2; the in-order scan is kept exact by updating
+// the counts of a removed point's neighbours at the moment of its removal, and
+// a warp ballot skips runs of points that cannot be removed.
+// ---------------------------------------------------------------------------
+template <int DIM, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_decimate(EngineView v)
+{
+    constexpr int NB = Pow3<DIM>::v;
+    const int g = blockIdx.x;
+    const GroupDesc gd = v.gr[g];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    __shared__ int s_flag, s_total, s_cnt;
+    __shared__ int s_off[33];
+    if (tid == 0) { s_flag = 0; s_total = 0; }
+    __syncthreads();
+    // all members converged?  (any evolving -> wait; all done -> nothing to do)
+    for (int i = tid; i < gd.n_clouds; i += BLOCK) {
+        const int ph = v.phase[gd.cloud_begin + i];
+        if (ph == PH_EVOLVE) atomicOr(&s_flag, 1);
+        if (ph == PH_CONVERGED) atomicOr(&s_flag, 2);
+    }
+    __syncthreads();
+    if ((s_flag & 1) || !(s_flag & 2)) return;
+
+    const CloudDesc c0 = v.cl[gd.cloud_begin];
+    const float rsq = sqr_rn(c0.r2);
+    const float rsq4 = __fmul_rn(4.0f, rsq);
+    const double inv = 1.0 / (2.0 * (double)c0.r2 * (1.0 + 1.0 / 1024.0));
+    float* X = v.dx + gd.s_scratch * DIM;
+    int32_t* cell = v.dcell + gd.s_scratch * DIM;
+    int32_t* alive = v.dalive + gd.s_scratch;
+    int32_t* c1 = v.dc1 + gd.s_scratch;
+    int32_t* c2 = v.dc2 + gd.s_scratch;
+    int32_t* items = v.ditems + gd.s_scratch;
+    const int hbits = v.dec_hbits[g];
+    const uint32_t hmask = (1u << hbits) - 1;
+    int32_t* bstart = v.dbstart + v.dec_hoff[g];
+
+    // gather the group's chosen points (cloud order) into X
+    int total = 0;
+    for (int i = 0; i < gd.n_clouds; ++i) {
+        const int c = gd.cloud_begin + i;
+        const CloudDesc cd = v.cl[c];
+        const int ns = v.ns[c];
+        for (int e = tid; e < ns * DIM; e += BLOCK) X[(int64_t)total * DIM + e] = v.S[cd.s_off * DIM + e];
+        total += ns;
+    }
+    for (int h = tid; h <= (int)hmask + 1; h += BLOCK) bstart[h] = 0;
+    __syncthreads();
+    // cells and bucket counts
+    for (int i = tid; i < total; i += BLOCK) {
+        int cc[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            cc[d] = cell_of(X[(int64_t)i * DIM + d], inv);
+            cell[(int64_t)i * DIM + d] = cc[d];
+        }
+        atomicAdd(&bstart[(cell_hash<DIM>(cc) & hmask) + 1], 1);
+        alive[i] = 1;
+    }
+    __syncthreads();
+    // exclusive prefix over buckets (single warp, sequential carry)
+    if (warp == 0) {
+        int carry = 0;
+        for (int h0 = 0; h0 <= (int)hmask + 1; h0 += 32) {
+            const int h = h0 + lane;
+            int x = (h <= (int)hmask + 1) ? bstart[h] : 0;
+            int incl = x;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += y;
+            }
+            if (h <= (int)hmask + 1) bstart[h] = carry + incl;
+            carry += __shfl_sync(FULL, incl, 31);
+        }
+    }
+    __syncthreads();
+    // fill buckets (member order inside a bucket does not matter: counts only)
+    for (int i = tid; i < total; i += BLOCK) {
+        int cc[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) cc[d] = cell[(int64_t)i * DIM + d];
+        const uint32_t b = cell_hash<DIM>(cc) & hmask;
+        const int slot = atomicAdd(&bstart[b], 1);
+        items[slot] = i;
+    }
+    __syncthreads();
+    // bstart[b] now holds the end of bucket b; start of b is bstart[b-1] (0 for b = 0)
+    auto bucket_range = [&](uint32_t b, int& lo, int& hi) {
+        lo = (b == 0) ? 0 : bstart[b - 1];
+        hi = bstart[b];
+    };
+    // initial counts
+    for (int i = tid; i < total; i += BLOCK) {
+        float p[DIM];
+        int cc[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            p[d] = X[(int64_t)i * DIM + d];
+            cc[d] = cell[(int64_t)i * DIM + d];
+        }
+        int n1 = 0, n2 = 0;
+        for (int o = 0; o < NB; ++o) {
+            int nc[DIM];
+            neighbour_cell<DIM>(cc, o, nc);
+            int lo, hi;
+            bucket_range(cell_hash<DIM>(nc) & hmask, lo, hi);
+            for (int t = lo; t < hi; ++t) {
+                const int q = items[t];
+                bool same = true;
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) same = same && (cell[(int64_t)q * DIM + d] == nc[d]);
+                if (!same) continue;
+                float s[DIM];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) s[d] = X[(int64_t)q * DIM + d];
+                const float sq = sqdist_exact<DIM>(p, s);
+                n1 += (sq <= rsq);
+                n2 += (sq <= rsq4);
+            }
+        }
+        c1[i] = n1;
+        c2[i] = n2;
+    }
+    __syncthreads();
+    // sequential in-order scan (warp 0)
+    if (warp == 0) {
+        int cnt = total, left = -1, guard = 0;
+        bool stop = false;
+        while (left != cnt && cnt > 3 && !stop) {
+            if (++guard > total + 2) { if (lane == 0) atomicOr(&v.err[gd.cloud_begin], ERRB_DEC_CAP); break; }
+            left = cnt;
+            int i = 0;
+            while (i < total) {
+                const int w = i + lane;
+                const bool pred = (w < total) && alive[w] && (c1[w] >= 4 || c2[w] < 3);
+                const unsigned bal = __ballot_sync(FULL, pred);
+                if (bal == 0) { i += 32; continue; }
+                const int j = i + __ffs(bal) - 1;
+                if (gd.nocopy && cnt - 1 < 3) { stop = true; break; }
+                if (lane == 0) alive[j] = 0;
+                --cnt;
+                // decrement the counts of j's neighbours
+                float p[DIM];
+                int cc[DIM];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) {
+                    p[d] = X[(int64_t)j * DIM + d];
+                    cc[d] = cell[(int64_t)j * DIM + d];
+                }
+                for (int o = 0; o < NB; ++o) {
+                    int nc[DIM];
+                    neighbour_cell<DIM>(cc, o, nc);
+                    int lo, hi;
+                    bucket_range(cell_hash<DIM>(nc) & hmask, lo, hi);
+                    for (int t = lo + lane; t < hi; t += 32) {
+                        const int q = items[t];
+                        if (q == j) continue;
+                        bool same = true;
+#pragma unroll
+                        for (int d = 0; d < DIM; ++d) same = same && (cell[(int64_t)q * DIM + d] == nc[d]);
+                        if (!same) continue;
+                        float s[DIM];
+#pragma unroll
+                        for (int d = 0; d < DIM; ++d) s[d] = X[(int64_t)q * DIM + d];
+                        const float sq = sqdist_exact<DIM>(p, s);
+                        if (sq <= rsq4) c2[q] -= 1;   // distinct q per lane: no race
+                        if (sq <= rsq) c1[q] -= 1;
+                    }
+                }
+                __syncwarp();
+                if (!gd.nocopy && cnt < 3) break;
+                i = j + 1;
+            }
+            if (!gd.nocopy && cnt < 3) break;
+        }
+        if (lane == 0) s_cnt = cnt;
+    }
+    __syncthreads();
+    // compaction back into each cloud, in order
+    int running = 0, total_after = 0;
+    for (int ci = 0; ci < gd.n_clouds; ++ci) {
+        const int c = gd.cloud_begin + ci;
+        const CloudDesc cd = v.cl[c];
+        const int ns = v.ns[c];
+        int kept = 0;
+        for (int k0 = 0; k0 < ns; k0 += BLOCK) {
+            const int k = k0 + tid;
+            const bool a = (k < ns) && alive[running + k];
+            const unsigned bal = __ballot_sync(FULL, a);
+            if (lane == 0) s_off[warp] = __popc(bal);
+            __syncthreads();
+            int pre = 0, tot = 0;
+            for (int w = 0; w < BLOCK / 32; ++w) {
+                pre += (w < warp) ? s_off[w] : 0;
+                tot += s_off[w];
+            }
+            if (a) {
+                const int pos = kept + pre + __popc(bal & lanemask_lt());
+#pragma unroll
+                for (int d = 0; d < DIM; ++d)
+                    v.S[(cd.s_off + pos) * DIM + d] = X[(int64_t)(running + k) * DIM + d];
+            }
+            kept += tot;
+            __syncthreads();
+        }
+        running += ns;
+        total_after += kept;
+        if (tid == 0) v.ns[c] = kept;
+    }
+    __syncthreads();
+    // outer-loop control: stop when decimation removed nothing
+    const bool stable = (total_after == total);
+    for (int i = tid; i < gd.n_clouds; i += BLOCK) {
+        const int c = gd.cloud_begin + i;
+        v.outer[c] += 1;
+        v.passes[c] = 0;
+        if (stable) {
+            v.phase[c] = PH_DONE;
+        } else if (v.outer[c] >= v.max_outer) {
+            v.err[c] |= ERRB_OUTER_CAP;
+            v.phase[c] = PH_DONE;
+        } else {
+            v.phase[c] = PH_EVOLVE;
+        }
+    }
+    (void)s_total;
+}
+
+// ---------------------------------------------------------------------------
+// loop condition: any unfinished cloud?  Sets the graph WHILE handle (graph
+// mode) and/or leaves the count in ctr[CTR_ACTIVE] for the host (plain mode).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) k_loopcond(EngineView v, cudaGraphConditionalHandle h,
+                                                   int use_handle)
+{
+    __shared__ int s_act;
+    if (threadIdx.x == 0) s_act = 0;
+    __syncthreads();
+    int act = 0;
+    for (int c = threadIdx.x; c < v.n_clouds; c += blockDim.x) act += (v.phase[c] != PH_DONE);
+    if (act) atomicAdd(&s_act, act);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int it = v.ctr[CTR_ITERS] + 1;
+        v.ctr[CTR_ITERS] = it;
+        int a = s_act;
+        if (it >= v.max_iters && a > 0) {
+            v.ctr[CTR_ERR] |= ERRB_EVOLVE_CAP;
+            a = 0;
+        }
+        v.ctr[CTR_ACTIVE] = a;
+        if (use_handle) cudaGraphSetConditional(h, a > 0 ? 1u : 0u);
+    }
+}
+
+__global__ void k_reset(EngineView v)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < CTR_COUNT && blockIdx.x == 0) v.ctr[c] = 0;
+    if (c >= v.n_clouds) return;
+    v.cont[c] = 0;
+    v.passes[c] = 0;
+    v.total_passes[c] = 0;
+    v.outer[c] = 0;
+    v.err[c] = 0;
+    v.pairs[c] = 0;
+}
+
+template <int DIM, int BLOCK, int ITEMS>
+cudaError_t set_assign_attrs(int dyn)
+{
+    return cudaFuncSetAttribute(k_assign<DIM, BLOCK, ITEMS>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+}
+
+template <int DIM>
+cudaError_t prepare_pass_dim(const EngineView& v, const TuneParams& tp)
+{
+    const int hist_bytes = v.hist_smem * 4;
+    cudaError_t e = cudaErrorInvalidValue;
+#define RD_PREP_CASE(B, I) \
+    if (tp.block == B && tp.items == I) e = set_assign_attrs<DIM, B, I>(hist_bytes);
+    RD_PREP_CASE(128, 8) RD_PREP_CASE(128, 4) RD_PREP_CASE(256, 4) RD_PREP_CASE(256, 8)
+    RD_PREP_CASE(128, 16)
+#undef RD_PREP_CASE
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_scatter<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                4 * v.scat_smem * 4);
+}
+
+template <int DIM>
+cudaError_t launch_pass_dim(const EngineView& v, const TuneParams& tp, int assign_grid,
+                            cudaStream_t st)
+{
+    const int hist_bytes = v.hist_smem * 4;
+#define RD_ASSIGN_CASE(B, I)                                                                  \
+    if (tp.block == B && tp.items == I) {                                                     \
+        k_assign<DIM, B, I><<<assign_grid, B, hist_bytes, st>>>(v);                           \
+    } else
+    RD_ASSIGN_CASE(128, 8)
+    RD_ASSIGN_CASE(128, 4)
+    RD_ASSIGN_CASE(256, 4)
+    RD_ASSIGN_CASE(256, 8)
+    RD_ASSIGN_CASE(128, 16)
+    { return cudaErrorInvalidValue; }
+#undef RD_ASSIGN_CASE
+    if (v.n_segs > 0) k_colscan<<<v.n_segs, 256, 0, st>>>(v);
+    k_segscan<1024><<<v.n_clouds, 1024, 0, st>>>(v);
+    if (v.n_chunks > 0) k_scatter<DIM><<<(v.n_chunks + 3) / 4, 128, 4 * v.scat_smem * 4, st>>>(v);
+    if (v.n_slots > 0) k_sum_shift<DIM><<<(v.n_slots + 7) / 8, 256, 0, st>>>(v);
+    k_control<<<(v.n_clouds + 255) / 256, 256, 0, st>>>(v);
+    k_decimate<DIM, 512><<<v.n_groups, 512, 0, st>>>(v);
+    return cudaGetLastError();
+}
+
+template <int DIM>
+cudaError_t launch_choose_dim(const EngineView& v, cudaStream_t st)
+{
+    using CS = ChooseSmem<DIM>;
+    constexpr int B = 512;
+    const int bytes = CS::HB * 4 + CS::SCAP * 4 + CS::SCAP * DIM * 4 + B * DIM * 8;
+    cudaError_t e =
+        cudaFuncSetAttribute(k_choose<DIM, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    k_choose<DIM, B><<<v.n_clouds, B, bytes, st>>>(v);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_choose(int dim, const EngineView& v, cudaStream_t st)
+{
+    switch (dim) {
+        case 2: return launch_choose_dim<2>(v, st);
+        case 3: return launch_choose_dim<3>(v, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t prepare_pass(int dim, const EngineView& v, const TuneParams& tp)
+{
+    switch (dim) {
+        case 2: return prepare_pass_dim<2>(v, tp);
+        case 3: return prepare_pass_dim<3>(v, tp);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_pass(int dim, const EngineView& v, const TuneParams& tp, int assign_grid,
+                        cudaStream_t st)
+{
+    switch (dim) {
+        case 2: return launch_pass_dim<2>(v, tp, assign_grid, st);
+        case 3: return launch_pass_dim<3>(v, tp, assign_grid, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_loopcond(const EngineView& v, cudaGraphConditionalHandle h, int use_handle,
+                            cudaStream_t st)
+{
+    k_loopcond<<<1, 1024, 0, st>>>(v, h, use_handle);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reset(const EngineView& v, cudaStream_t st)
+{
+    const int n = v.n_clouds > CTR_COUNT ? v.n_clouds : CTR_COUNT;
+    k_reset<<<(n + 255) / 256, 256, 0, st>>>(v);
+    return cudaGetLastError();
+}
+
+bool tune_supported(int dim, const TuneParams& tp)
+{
+    (void)dim;
+    return (tp.block == 128 && (tp.items == 4 || tp.items == 8 || tp.items == 16)) ||
+           (tp.block == 256 && (tp.items == 4 || tp.items == 8));
+}
+
+int assign_smem_bytes(int dim, const TuneParams& tp, int hist_ints)
+{
+    (void)tp;
+    const int dp = (dim == 3) ? 4 : dim;
+    return ASSIGN_TS * dp * 4 + 16 + hist_ints * 4;
+}
+
+template <int DIM, int B, int I>
+static int occ_of(int dyn)
+{
+    int nb = 0;
+    if (set_assign_attrs<DIM, B, I>(dyn) != cudaSuccess) return 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_assign<DIM, B, I>, B, dyn);
+    return nb;
+}
+
+int max_assign_blocks_per_sm(int dim, const TuneParams& tp, int hist_ints)
+{
+    const int dyn = hist_ints * 4;
+#define RD_OCC(D, B, I) \
+    if (dim == D && tp.block == B && tp.items == I) return occ_of<D, B, I>(dyn);
+    RD_OCC(2, 128, 8) RD_OCC(2, 128, 4) RD_OCC(2, 256, 4) RD_OCC(2, 256, 8) RD_OCC(2, 128, 16)
+    RD_OCC(3, 128, 8) RD_OCC(3, 128, 4) RD_OCC(3, 256, 4) RD_OCC(3, 256, 8) RD_OCC(3, 128, 16)
+#undef RD_OCC
+    return 0;
+}
+
+}  // namespace rdb
