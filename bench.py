@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 ridge-detection path (one JSON line on rank 0).
+
+Default workload (N=1): brute-force 3D helix, N = 1,000,000 float32 points,
+t~U[0,8pi], p = (cos t, sin t, 0.15 t) + N(0, 0.05^2), r1 = 0.15, r2 = 0.3.
+One step = one full ridge solve (choose, then evolve/decimate to convergence)
+through the library's C ABI.  The metric is evolve pairs/s: the sum over all
+evolve passes of (cloud points x chosen points), divided by the solve time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                  [--workload helix3d_1m|sine2d_20k|batch]
+
+--impl reference times the reference's own OpenMP CPU evolve (compiled from its
+sources into oracle/_ref/librdref_omp.so) on the same cloud, one evolve pass per
+step, on all host cores.  Under torchrun only rank 0 runs it.
+
+For N > 1 every rank solves its own replica of the workload (the single-cloud
+brute-force path does not shard); value = pairs of all ranks / max rank time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "evolve pairs/s"
+UNIT = "pairs/s"
+# DRAM traffic of one k_assign launch on the helix3d_1m workload from ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum); see profiles/.  None = not captured.
+ASSIGN_TRAFFIC_BYTES = None
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="helix3d_1m",
+                    choices=["helix3d_1m", "sine2d_20k", "batch"])
+    ap.add_argument("--clouds", type=int, default=4096, help="batch workload: number of clouds")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(name):
+    from ridgedetection_b200 import generators as G
+    if name == "helix3d_1m":
+        return G.helix3d(1_000_000), 0.15, 0.3
+    if name == "sine2d_20k":
+        return G.sine2d(20_000), 0.3, 0.6
+    raise ValueError(name)
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples every 200 ms while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        busy = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(busy), "sm_max_mhz": max(smax),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline(P, r1, target_s=15.0):
+    """The reference's OpenMP evolve on this host's cores: a bounded sample of
+    whole evolve passes at the chosen set right after choose."""
+    import oracle
+    if oracle.ref(True) is None:
+        return None
+    S0 = oracle.choose(P, r1)
+    threads = os.cpu_count() or 1
+    t = time.perf_counter()
+    oracle.ref_evolve_passes_omp(P, S0, r1, threads=threads, passes=1)
+    t1 = time.perf_counter() - t
+    passes = int(max(1, min(50, target_s / max(t1, 1e-3))))
+    t = time.perf_counter()
+    oracle.ref_evolve_passes_omp(P, S0, r1, threads=threads, passes=passes)
+    dt = time.perf_counter() - t
+    pairs = float(P.shape[0]) * S0.shape[0] * passes
+    return {"value": pairs / dt, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"{passes} OpenMP evolve passes (rd::evolve_omp loop body) of the "
+                      f"{P.shape[0]}-point cloud at the {S0.shape[0]} chosen points after choose, "
+                      f"{dt:.1f} s"}
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    import oracle
+    P, r1, r2 = workload(args.workload)
+    if oracle.ref(True) is None:
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/librdref_omp.so was not built"}))
+        return
+    S0 = oracle.choose(P, r1)
+    threads = os.cpu_count() or 1
+    pairs_step = float(P.shape[0]) * S0.shape[0]
+    for _ in range(args.warmup):
+        oracle.ref_evolve_passes_omp(P, S0, r1, threads=threads, passes=1)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        oracle.ref_evolve_passes_omp(P, S0, r1, threads=threads, passes=1)
+    dt = time.perf_counter() - t
+    val = pairs_step * args.steps / dt
+    sample = (f"one OpenMP evolve pass (rd::evolve_omp loop body) per step over the "
+              f"{P.shape[0]}-point cloud at the {S0.shape[0]} chosen points after choose")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "cores": threads},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def run_b200_bf(args, world, rank, local):
+    import torch
+    import ridgedetection_b200 as rdb
+    from ridgedetection_b200 import _lib as L
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=dev)
+    P, r1, r2 = workload(args.workload)
+    n, dim = P.shape
+    stream = torch.cuda.current_stream()
+    dP = torch.from_numpy(P).to(dev)
+    l2_flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    rd = rdb.BruteForceRidgeDetection(n, r1, r2, dim)
+    rd.set_points(dP)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+            torch.cuda.synchronize()
+
+    for _ in range(max(3, args.warmup)):
+        rd.ridge_detection()
+    torch.cuda.synchronize()
+    st = rd.stats()
+    pairs_step = st.pairs
+    iters_step = st.loop_iters
+
+    # ---- timed region: K device-resident solves, L2 flushed between them ----
+    clock = ClockSampler(local)
+    clock.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    barrier()
+    for k in range(args.steps):
+        l2_flush.zero_()
+        ev[k][0].record(stream)
+        rd.ridge_detection()
+        ev[k][1].record(stream)
+    barrier()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    clocks = clock.stop()
+    ms = sum(step_ms) / len(step_ms)
+    ms_t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(ms_t, op=torch.distributed.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = world * pairs_step / (ms_max * 1e-3)
+
+    # ---- e2e: host (pinned) buffers through the C ABI, copies inside the timing ----
+    hP = torch.from_numpy(P).pin_memory()
+    hout = torch.empty((n, dim), dtype=torch.float32).pin_memory()
+    e2e_ms = []
+    barrier()
+    for k in range(args.steps):
+        l2_flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        rd.set_points(hP.numpy())
+        rd.ridge_detection()
+        out = hout[: rd.ns_]
+        rd.chosen_points(out.numpy())
+        b.record(stream)
+        b.synchronize()
+        e2e_ms.append(a.elapsed_time(b))
+    barrier()
+    e2e_t = torch.tensor([sum(e2e_ms) / len(e2e_ms)], device=dev, dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(e2e_t, op=torch.distributed.ReduceOp.MAX)
+    e2e_val = world * pairs_step / (float(e2e_t.item()) * 1e-3)
+    ns_final = rd.ns_
+
+    # ---- dominant kernel: assign, timed per launch in a host-loop solve ----
+    rd.set_loop_mode(rdb.LOOP_HOST)
+    lib = L.lib()
+    L.check(lib.rd_bf_set_profiling(rd._h, 1))
+    rd.ridge_detection()
+    pst = rd.stats()
+    L.check(lib.rd_bf_set_profiling(rd._h, 0))
+    rd.set_loop_mode(rdb.LOOP_GRAPH)
+    flops_per_pair = 3 * dim
+    assign_ms_avg = pst.assign_ms / max(1, pst.assign_launches)
+    flops_per_launch = pst.pairs * flops_per_pair / max(1, pst.assign_launches)
+    achieved_tflops = flops_per_launch / (assign_ms_avg * 1e-3) / 1e12
+    peak = ctypes.c_double(0)
+    L.check(lib.rd_probe_fp32_peak(ctypes.byref(peak), ctypes.c_void_p(stream.cuda_stream)))
+    nominal = 148 * 128 * 2 * 1.965e9 / 1e12
+
+    if world > 1:
+        torch.distributed.barrier()
+    rd.close()
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline(P, r1)
+        except Exception as e:  # the baseline is reported, never the target
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"failed: {e}"}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms_max,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"{args.workload}: brute-force full solve, N={n}, dim={dim}, "
+                               f"r1={r1}, r2={r2}",
+                   "l2": "flushed (256 MiB write) between timed steps",
+                   "loop": "CUDA graph WHILE node", "parallelism": f"replicas x{world}"},
+        "solves_per_s": world * 1e3 / ms_max,
+        "pairs_per_step": pairs_step, "loop_iters_per_step": iters_step,
+        "ns_final": ns_final,
+        "roofline": {"bound": "fp32", "kernel": "k_assign", "achieved": achieved_tflops,
+                     "peak": peak.value, "unit": "TFLOP/s",
+                     "frac": achieved_tflops / peak.value,
+                     "peak_source": "measured FMA-chain probe (rd_probe_fp32_peak); "
+                                    f"nominal {nominal:.1f} TFLOP/s at 1965 MHz",
+                     "flops_per_pair": flops_per_pair,
+                     "assign_ms_per_launch": assign_ms_avg,
+                     "assign_launches": pst.assign_launches,
+                     "traffic": ASSIGN_TRAFFIC_BYTES},
+        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(P.nbytes),
+                "d2h_bytes_per_step": int(ns_final * dim * 4)},
+        "gpu_launches": args.steps * (2 + 8 * iters_step),
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def run_b200_batch(args, world, rank, local):
+    """Batched workload: graph-driven batched solve vs the plain per-cloud loop."""
+    import torch
+    import ridgedetection_b200 as rdb
+    from ridgedetection_b200 import generators as G
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    spec = G.batch_spec(args.clouds)
+    mine = [s for i, s in enumerate(spec) if i % world == rank]
+    clouds = [(G.batch_cloud(n, dim, seed), r1, r2) for (n, dim, r1, r2, seed) in mine]
+    packed, descs = rdb.pack_clouds(clouds)
+    dpk = torch.from_numpy(packed).to(dev)
+    b = rdb.BatchedRidgeDetection()
+    for _ in range(max(3, args.warmup) if args.warmup else 1):
+        b.run(dpk, descs)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        b.run(dpk, descs)
+    torch.cuda.synchronize()
+    ms_batch = (time.perf_counter() - t0) / args.steps * 1e3
+    stb = b.stats()
+    # plain per-cloud loop (one brute-force handle per cloud, host-synchronised loop)
+    t0 = time.perf_counter()
+    for (P, r1, r2) in clouds:
+        rd = rdb.BruteForceRidgeDetection(P.shape[0], r1, r2, P.shape[1],
+                                          loop_mode=rdb.LOOP_HOST)
+        rd.set_points(torch.from_numpy(P).to(dev))
+        rd.ridge_detection()
+        rd.close()
+    torch.cuda.synchronize()
+    ms_plain = (time.perf_counter() - t0) * 1e3
+    if rank == 0:
+        print(json.dumps({
+            "metric": "ridge solves/s", "value": len(clouds) / (ms_batch * 1e-3),
+            "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_batch, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"batch of {len(clouds)} clouds (log-uniform 1e3..2e5 points, "
+                                   f"half sine2d half helix3d)"},
+            "plain_loop_solves_per_s": len(clouds) / (ms_plain * 1e-3),
+            "batched_over_plain": ms_plain / ms_batch,
+            "pairs_per_step": stb.pairs, "loop_iters": stb.loop_iters,
+        }))
+
+
+def main():
+    args = parse_args()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference_arm(args, world, rank)
+        return
+    if args.workload == "batch":
+        run_b200_batch(args, world, rank, local)
+    else:
+        run_b200_bf(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

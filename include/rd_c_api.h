@@ -61,12 +61,18 @@ typedef struct rd_run_stats {
     double  pairs;          /* sum over passes of (cloud points x chosen points)     */
     int32_t err_bits;       /* device error bits (0 when clean)                      */
     int32_t pad;
+    double  assign_ms;      /* profiling runs only: summed assign-kernel time (ms)   */
+    int64_t assign_launches;/* profiling runs only: assign-kernel launches timed     */
 } rd_run_stats;
 
 RD_API const char* rd_last_error(void);
 RD_API int rd_abi_version(void);
 /* dimensions compiled into the kernels, as a bit mask (bit d set = dim d) */
 RD_API int rd_supported_dims(void);
+/* Measurement helper (no reference counterpart): FP32 FMA throughput of the
+ * current device from an independent-chain FMA kernel timed with CUDA events,
+ * in TFLOP/s (2 flops per FMA).  Used as the FP32 roofline denominator. */
+RD_API rd_status rd_probe_fp32_peak(double* tflops, void* stream);
 
 /* ---------------------------------------------------------------------------
  * Brute force, one cloud.  Mirrors rd::gpu::bruteForce::RidgeDetection:
@@ -88,7 +94,44 @@ RD_API rd_status rd_bf_get_count(rd_bf* h, int64_t* ns);
 /* out receives ns points in the handle's out_layout (pitch as above, for n = ns) */
 RD_API rd_status rd_bf_get_points(rd_bf* h, float* out, int64_t pitch, int dst_on_device, void* stream);
 RD_API rd_status rd_bf_get_stats(rd_bf* h, rd_run_stats* st);
+/* enable = 1: host-loop runs time every assign-kernel launch with CUDA events
+ * (reported in rd_run_stats.assign_ms / assign_launches) */
+RD_API rd_status rd_bf_set_profiling(rd_bf* h, int enable);
 RD_API rd_status rd_bf_destroy(rd_bf* h);
+
+/* ---------------------------------------------------------------------------
+ * Tiled (extended tiles, mixed policy), one cloud.  Mirrors
+ * rd::gpu::tiled::RidgeDetection (rd/gpu/device/tiled/simulation.cuh:41-241):
+ *   ctor(pointsNum, hostPoints)  -> rd_tiled_create + rd_tiled_set_points
+ *   operator()(r1, r2, maxTileCapacity, tilesPerDim[DIM], endPhaseRefinement)
+ *                                -> rd_tiled_run
+ *   getChosenPointsNum()         -> rd_tiled_get_count
+ *   getChosenPoints(T*)          -> rd_tiled_get_points
+ *   getTimers()                  -> rd_tiled_get_timers
+ * The result is that of the reference CPU implementation
+ * rd::tiled::tiledRidgeDetection<EXT_TILE_TREE_MIXED_RD> (rd/cpu/tiled/rd_tiled.hpp:1217-1374):
+ * leaf tiles in pre-order, each tile's chosen points in order.  Only
+ * end_phase_refinement = 0 is supported (RD_ERR_UNSUPPORTED otherwise).
+ * ------------------------------------------------------------------------- */
+typedef struct rd_tiled rd_tiled;
+RD_API rd_status rd_tiled_create(rd_tiled** out, int dim, int in_layout, int out_layout,
+                                 int64_t np);
+RD_API rd_status rd_tiled_set_points(rd_tiled* h, const float* pts, int64_t pitch,
+                                     int src_on_device, void* stream);
+RD_API rd_status rd_tiled_set_loop_mode(rd_tiled* h, int mode);
+RD_API rd_status rd_tiled_run(rd_tiled* h, float r1, float r2, int64_t max_tile_capacity,
+                              const int32_t* tiles_per_dim, int end_phase_refinement,
+                              void* stream);
+RD_API rd_status rd_tiled_get_count(rd_tiled* h, int64_t* ns);
+RD_API rd_status rd_tiled_get_points(rd_tiled* h, float* out, int64_t pitch, int dst_on_device,
+                                     void* stream);
+/* whole, tile build, tile ridge detection, end-phase refinement, in ms
+ * (TiledRidgeDetectionTimers, rd/gpu/agent/agent_tiled_ridge_detection.cuh:96-102) */
+RD_API rd_status rd_tiled_get_timers(rd_tiled* h, float* whole, float* build, float* rd_tiles,
+                                     float* refinement);
+RD_API rd_status rd_tiled_get_stats(rd_tiled* h, rd_run_stats* st);
+RD_API rd_status rd_tiled_get_leaf_count(rd_tiled* h, int64_t* n_leaves);
+RD_API rd_status rd_tiled_destroy(rd_tiled* h);
 
 /* ---------------------------------------------------------------------------
  * Batched: many independent clouds solved together (brute force per cloud).

@@ -107,6 +107,8 @@ def ref(openmp: bool = False):
             L.ref_tiled_ridge.argtypes = [_F, _i64, _int, _flt, _flt, _i64, _I64, _int, _int,
                                           _F, _F]
             L.ref_max_threads.restype = _int
+            L.ref_evolve_passes_omp.restype = _int
+            L.ref_evolve_passes_omp.argtypes = [_F, _i64, _F, _i64, _int, _flt, _int, _int]
             _ref[name] = L
     return _ref[name]
 
@@ -237,6 +239,16 @@ def ref_evolve(P, S, r1, threads=0, openmp=False):
     P, S = _f32(P), _f32(S).copy()
     L.ref_evolve(_fp(P), P.shape[0], _fp(S), S.shape[0], P.shape[1], r1, threads)
     return S
+
+
+def ref_evolve_passes_omp(P, S, r1, threads=0, passes=1):
+    """`passes` passes of the reference's OpenMP evolve loop body (in place on a
+    copy of S); returns (S, cont).  threads=0 uses every core."""
+    L = ref(True)
+    P, S = _f32(P), _f32(S).copy()
+    cont = L.ref_evolve_passes_omp(_fp(P), P.shape[0], _fp(S), S.shape[0], P.shape[1], r1,
+                                   threads, passes)
+    return S, cont
 
 
 def ref_decimate(S, r2):

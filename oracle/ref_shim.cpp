@@ -84,6 +84,49 @@ int ref_evolve_pass(const float* P, int64_t np, float* S, int64_t ns, int dim,
     return contFlag;
 }
 
+/* `passes` evolve passes exactly as the loop body of rd::evolve_omp
+ * (evolve.hpp:258-286) runs them: an OpenMP region that zeroes the sums and
+ * calls calculateClosestSphereCenter_omp, then shiftTowardMassCenter_omp.
+ * Used to time a bounded sample of the reference's OpenMP evolve.  Returns
+ * the continue flag of the last pass. */
+int ref_evolve_passes_omp(const float* P, int64_t np, float* S, int64_t ns, int dim, float r1,
+                          int threads, int passes)
+{
+    float rSqr = r1 * r1;
+    std::vector<float> cordSums((size_t)(ns * dim) + 1);
+    std::vector<int> cnt((size_t)ns + 1);
+    int contFlag = 0;
+#if defined(RD_USE_OPENMP)
+    const int nt = threads > 0 ? threads : omp_get_num_procs();
+    for (int p = 0; p < passes; ++p) {
+        float* cs = cordSums.data();
+        int* sc = cnt.data();
+        #pragma omp parallel num_threads(nt)
+        {
+            rd::fillTable_omp(cs, 0.f, (size_t)(ns * dim));
+            rd::fillTable_omp(sc, 0, (size_t)ns);
+            rd::detail::calculateClosestSphereCenter_omp<float>(P, S, cs, sc, (size_t)np,
+                                                                (size_t)ns, (size_t)dim, rSqr);
+        }
+        contFlag = 0;
+        rd::detail::shiftTowardMassCenter_omp<float>(S, cs, sc, (size_t)ns, (size_t)dim,
+                                                     contFlag, nt);
+    }
+#else
+    (void)threads;
+    for (int p = 0; p < passes; ++p) {
+        std::fill(cordSums.begin(), cordSums.end(), 0.f);
+        std::fill(cnt.begin(), cnt.end(), 0);
+        rd::detail::calculateClosestSphereCenter<float>(P, S, cordSums.data(), cnt.data(),
+                                                        (size_t)np, (size_t)ns, (size_t)dim, rSqr);
+        contFlag = 0;
+        rd::detail::shiftTowardMassCenter<float>(S, cordSums.data(), cnt.data(), (size_t)ns,
+                                                 (size_t)dim, contFlag);
+    }
+#endif
+    return contFlag;
+}
+
 /* rd::evolve (serial) or rd::evolve_omp (threads > 0, OpenMP build only). */
 void ref_evolve(const float* P, int64_t np, float* S, int64_t ns, int dim, float r1,
                 int threads)

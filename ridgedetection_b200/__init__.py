@@ -7,9 +7,10 @@ mirror of the reference's interface; it never falls back to a CPU path.
 from . import generators  # noqa: F401
 from ._lib import RDError, RunStats, lib  # noqa: F401
 from .api import (COL_MAJOR, LOOP_GRAPH, LOOP_HOST, ROW_MAJOR,  # noqa: F401
-                  BatchedRidgeDetection, BruteForceRidgeDetection, pack_clouds,
-                  ridge_detection)
+                  BatchedRidgeDetection, BruteForceRidgeDetection, TiledRidgeDetection,
+                  pack_clouds, ridge_detection, tiled_ridge_detection)
 
-__all__ = ["BruteForceRidgeDetection", "BatchedRidgeDetection", "ridge_detection",
+__all__ = ["BruteForceRidgeDetection", "BatchedRidgeDetection", "TiledRidgeDetection",
+           "ridge_detection", "tiled_ridge_detection",
            "pack_clouds", "ROW_MAJOR", "COL_MAJOR", "LOOP_GRAPH", "LOOP_HOST", "RDError",
            "RunStats", "lib", "generators"]

@@ -38,7 +38,8 @@ class RDError(RuntimeError):
 class RunStats(ctypes.Structure):
     _fields_ = [("loop_iters", ctypes.c_int64), ("evolve_passes", ctypes.c_int64),
                 ("max_passes", ctypes.c_int64), ("pairs", ctypes.c_double),
-                ("err_bits", ctypes.c_int32), ("pad", ctypes.c_int32)]
+                ("err_bits", ctypes.c_int32), ("pad", ctypes.c_int32),
+                ("assign_ms", ctypes.c_double), ("assign_launches", ctypes.c_int64)]
 
 
 class CloudDesc(ctypes.Structure):
@@ -59,6 +60,7 @@ SIGNATURES = {
     "rd_last_error": [],
     "rd_abi_version": [],
     "rd_supported_dims": [],
+    "rd_probe_fp32_peak": [ctypes.POINTER(ctypes.c_double), _vp],
     "rd_bf_create": [ctypes.POINTER(_vp), _i, _i, _i, _i64, _f, _f],
     "rd_bf_set_points": [_vp, _vp, _i64, _i, _vp],
     "rd_bf_set_loop_mode": [_vp, _i],
@@ -66,7 +68,18 @@ SIGNATURES = {
     "rd_bf_get_count": [_vp, _pi64],
     "rd_bf_get_points": [_vp, _vp, _i64, _i, _vp],
     "rd_bf_get_stats": [_vp, ctypes.POINTER(RunStats)],
+    "rd_bf_set_profiling": [_vp, _i],
     "rd_bf_destroy": [_vp],
+    "rd_tiled_create": [ctypes.POINTER(_vp), _i, _i, _i, _i64],
+    "rd_tiled_set_points": [_vp, _vp, _i64, _i, _vp],
+    "rd_tiled_set_loop_mode": [_vp, _i],
+    "rd_tiled_run": [_vp, _f, _f, _i64, ctypes.POINTER(ctypes.c_int32), _i, _vp],
+    "rd_tiled_get_count": [_vp, _pi64],
+    "rd_tiled_get_points": [_vp, _vp, _i64, _i, _vp],
+    "rd_tiled_get_timers": [_vp, _pf, _pf, _pf, _pf],
+    "rd_tiled_get_stats": [_vp, ctypes.POINTER(RunStats)],
+    "rd_tiled_get_leaf_count": [_vp, _pi64],
+    "rd_tiled_destroy": [_vp],
     "rd_batch_create": [ctypes.POINTER(_vp)],
     "rd_batch_set_loop_mode": [_vp, _i],
     "rd_batch_run": [_vp, ctypes.POINTER(CloudDesc), _i32, _vp, _i64, _i, _vp],

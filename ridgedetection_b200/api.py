@@ -138,6 +138,94 @@ def ridge_detection(P: np.ndarray, r1: float, r2: float, loop_mode: int = LOOP_G
         rd.close()
 
 
+class TiledRidgeDetection:
+    """rd::gpu::tiled::RidgeDetection<DIM, IN, OUT, RD_BRUTE_FORCE, RD_MIXED,
+    RD_EXTENDED_TILE, float> (rd/gpu/device/tiled/simulation.cuh:41-241), with the
+    results of the reference CPU EXT_TILE_TREE_MIXED_RD implementation."""
+
+    def __init__(self, points_num: int, dim: int, input_points=None,
+                 in_layout: int = ROW_MAJOR, out_layout: int = ROW_MAJOR,
+                 loop_mode: int = LOOP_GRAPH):
+        self._lib = L.lib()
+        self._h = ctypes.c_void_p()
+        L.check(self._lib.rd_tiled_create(ctypes.byref(self._h), dim, in_layout, out_layout,
+                                          int(points_num)))
+        self.dim = int(dim)
+        self.out_layout = out_layout
+        self.ns_ = 0
+        L.check(self._lib.rd_tiled_set_loop_mode(self._h, loop_mode))
+        if input_points is not None:
+            self.set_points(input_points)
+
+    def set_points(self, pts, pitch: int = 0):
+        p, dev, st = _ptr_of(pts)
+        L.check(self._lib.rd_tiled_set_points(self._h, p, int(pitch), dev, st))
+
+    def __call__(self, r1: float, r2: float, max_tile_capacity: int,
+                 tiles_per_dim: Sequence[int], end_phase_refinement: bool = False,
+                 stream=None):
+        tpd = (ctypes.c_int32 * self.dim)(*[int(t) for t in tiles_per_dim])
+        st = ctypes.c_void_p(stream) if stream is not None \
+            else BruteForceRidgeDetection._current_stream()
+        L.check(self._lib.rd_tiled_run(self._h, float(r1), float(r2), int(max_tile_capacity),
+                                       tpd, int(bool(end_phase_refinement)), st))
+        return self.get_chosen_points_num()
+
+    ridge_detection = __call__
+
+    def get_chosen_points_num(self) -> int:
+        n = ctypes.c_int64(0)
+        L.check(self._lib.rd_tiled_get_count(self._h, ctypes.byref(n)))
+        self.ns_ = int(n.value)
+        return self.ns_
+
+    def get_chosen_points(self, out=None, pitch: int = 0):
+        if out is None:
+            shape = (self.ns_, self.dim) if self.out_layout == ROW_MAJOR else (self.dim, self.ns_)
+            out = np.empty(shape, np.float32)
+        p, dev, st = _ptr_of(out, want_writable=True)
+        L.check(self._lib.rd_tiled_get_points(self._h, p, int(pitch), dev, st))
+        return out
+
+    def get_timers(self):
+        v = [ctypes.c_float(0) for _ in range(4)]
+        L.check(self._lib.rd_tiled_get_timers(self._h, *[ctypes.byref(x) for x in v]))
+        return dict(zip(["whole", "build_tree", "rd_tiles", "refinement"], [x.value for x in v]))
+
+    def leaf_count(self) -> int:
+        n = ctypes.c_int64(0)
+        L.check(self._lib.rd_tiled_get_leaf_count(self._h, ctypes.byref(n)))
+        return int(n.value)
+
+    def stats(self) -> L.RunStats:
+        s = L.RunStats()
+        L.check(self._lib.rd_tiled_get_stats(self._h, ctypes.byref(s)))
+        return s
+
+    def close(self):
+        if self._h:
+            self._lib.rd_tiled_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def tiled_ridge_detection(P: np.ndarray, r1: float, r2: float, max_tile_capacity: int,
+                          tiles_per_dim: Sequence[int], loop_mode: int = LOOP_GRAPH):
+    """Tiled ridge of one ROW_MAJOR float32 cloud; returns (S, stats, n_leaves)."""
+    P = np.ascontiguousarray(P, dtype=np.float32)
+    rd = TiledRidgeDetection(P.shape[0], P.shape[1], P, loop_mode=loop_mode)
+    try:
+        rd(r1, r2, max_tile_capacity, tiles_per_dim)
+        return rd.get_chosen_points(), rd.stats(), rd.leaf_count()
+    finally:
+        rd.close()
+
+
 class BatchedRidgeDetection:
     """Many independent clouds, one engine run per point dimension."""
 

@@ -1,6 +1,7 @@
 // rd_capi.cu -- extern "C" entry points declared in include/rd_c_api.h.
 #include "../../include/rd_c_api.h"
 #include "rd_engine_host.hpp"
+#include "rd_tiled.hpp"
 
 #include <algorithm>
 #include <cstring>
@@ -145,6 +146,24 @@ void fill_stats(const RunStats& s, rd_run_stats* o)
     o->max_passes = s.max_passes;
     o->pairs = s.pairs;
     o->err_bits = s.err_bits;
+    o->assign_ms = s.assign_ms;
+    o->assign_launches = s.assign_launches;
+}
+
+// independent FMA chains: 8 per thread, ITER rounds
+__global__ void __launch_bounds__(256) k_fma_probe(float* out, int iters, float a, float b)
+{
+    float x0 = threadIdx.x * 1e-7f, x1 = x0 + 1e-7f, x2 = x0 + 2e-7f, x3 = x0 + 3e-7f;
+    float x4 = x0 + 4e-7f, x5 = x0 + 5e-7f, x6 = x0 + 6e-7f, x7 = x0 + 7e-7f;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            x0 = fmaf(x0, a, b); x1 = fmaf(x1, a, b); x2 = fmaf(x2, a, b); x3 = fmaf(x3, a, b);
+            x4 = fmaf(x4, a, b); x5 = fmaf(x5, a, b); x6 = fmaf(x6, a, b); x7 = fmaf(x7, a, b);
+        }
+    }
+    const float r = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+    if (r == 1234.5678f) out[threadIdx.x] = r;  // keeps the chains live
 }
 
 bool dim_ok(int dim) { return dim == 2 || dim == 3; }
@@ -159,6 +178,16 @@ struct rd_bf {
     Engine eng;
     DevBuf staging;
     int64_t ns = 0;
+    bool have_result = false;
+};
+
+struct rd_tiled {
+    int dim, in_layout, out_layout;
+    int64_t np;
+    int mode = RD_LOOP_GRAPH;
+    DevBuf pts;      // packed ROW_MAJOR input
+    DevBuf staging;
+    TiledRunner run;
     bool have_result = false;
 };
 
@@ -180,6 +209,33 @@ const char* rd_last_error(void) { return g_err.c_str(); }
 int rd_abi_version(void) { return 1; }
 
 int rd_supported_dims(void) { return (1 << 2) | (1 << 3); }
+
+rd_status rd_probe_fp32_peak(double* tflops, void* stream)
+{
+    if (!tflops) return set_err(RD_ERR_ARG, "null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    int dev = 0, sms = 0;
+    CK_CUDA(cudaGetDevice(&dev));
+    CK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    DevBuf out;
+    CK_CUDA(out.ensure(4096));
+    const int blocks = sms * 8, iters = 4096;
+    cudaEvent_t e0, e1;
+    CK_CUDA(cudaEventCreate(&e0));
+    CK_CUDA(cudaEventCreate(&e1));
+    k_fma_probe<<<blocks, 256, 0, st>>>(out.as<float>(), 64, 0.999f, 1e-6f);  // warm-up
+    CK_CUDA(cudaEventRecord(e0, st));
+    k_fma_probe<<<blocks, 256, 0, st>>>(out.as<float>(), iters, 0.999f, 1e-6f);
+    CK_CUDA(cudaEventRecord(e1, st));
+    CK_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    CK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const double flops = 2.0 * 8 * 16 * (double)iters * blocks * 256.0;
+    *tflops = flops / (ms * 1e-3) / 1e12;
+    return RD_OK;
+}
 
 // ------------------------------------------------------------------------
 // brute force
@@ -277,7 +333,124 @@ rd_status rd_bf_get_stats(rd_bf* h, rd_run_stats* st)
     return RD_OK;
 }
 
+rd_status rd_bf_set_profiling(rd_bf* h, int enable)
+{
+    if (!h) return set_err(RD_ERR_ARG, "null handle");
+    h->eng.profile_assign = enable != 0;
+    return RD_OK;
+}
+
 rd_status rd_bf_destroy(rd_bf* h)
+{
+    delete h;
+    return RD_OK;
+}
+
+// ------------------------------------------------------------------------
+// tiled
+// ------------------------------------------------------------------------
+rd_status rd_tiled_create(rd_tiled** out, int dim, int in_layout, int out_layout, int64_t np)
+{
+    if (!out) return set_err(RD_ERR_ARG, "null handle pointer");
+    *out = nullptr;
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if ((in_layout != RD_ROW_MAJOR && in_layout != RD_COL_MAJOR) ||
+        (out_layout != RD_ROW_MAJOR && out_layout != RD_COL_MAJOR))
+        return set_err(RD_ERR_ARG, "unknown layout");
+    if (np < 0 || np > INT32_MAX / 4) return set_err(RD_ERR_ARG, "np out of range");
+    rd_tiled* h = new (std::nothrow) rd_tiled();
+    if (!h) return set_err(RD_ERR_ALLOC, "host allocation failed");
+    h->dim = dim;
+    h->in_layout = in_layout;
+    h->out_layout = out_layout;
+    h->np = np;
+    if (h->pts.ensure(sizeof(float) * (size_t)(np * dim + 4)) != cudaSuccess) {
+        delete h;
+        return set_err(RD_ERR_ALLOC, "device allocation failed");
+    }
+    *out = h;
+    return RD_OK;
+}
+
+rd_status rd_tiled_set_points(rd_tiled* h, const float* pts, int64_t pitch, int src_on_device,
+                              void* stream)
+{
+    if (!h) return set_err(RD_ERR_ARG, "null handle");
+    h->have_result = false;
+    return load_points(pts, h->in_layout, pitch, h->np, h->dim, src_on_device, h->pts.as<float>(),
+                       h->staging, (cudaStream_t)stream);
+}
+
+rd_status rd_tiled_set_loop_mode(rd_tiled* h, int mode)
+{
+    if (!h) return set_err(RD_ERR_ARG, "null handle");
+    if (mode != RD_LOOP_GRAPH && mode != RD_LOOP_HOST) return set_err(RD_ERR_ARG, "bad mode");
+    h->mode = mode;
+    return RD_OK;
+}
+
+rd_status rd_tiled_run(rd_tiled* h, float r1, float r2, int64_t max_tile_capacity,
+                       const int32_t* tiles_per_dim, int end_phase_refinement, void* stream)
+{
+    if (!h || !tiles_per_dim) return set_err(RD_ERR_ARG, "null argument");
+    if (!(r1 > 0.0f) || !(r2 > 0.0f)) return set_err(RD_ERR_ARG, "r1 and r2 must be > 0");
+    if (max_tile_capacity < 2) return set_err(RD_ERR_ARG, "max_tile_capacity must be >= 2");
+    if (end_phase_refinement)
+        return set_err(RD_ERR_UNSUPPORTED, "end-phase refinement is not built into this library");
+    h->have_result = false;
+    int rc = h->run.run(h->pts.as<float>(), h->np, h->dim, r1, r2, max_tile_capacity,
+                        tiles_per_dim, h->mode == RD_LOOP_GRAPH, (cudaStream_t)stream);
+    h->have_result = (rc == 0 || rc == RD_ERR_NOT_CONVERGED);
+    if (rc) return set_err((rd_status)rc, h->run.last_error);
+    return RD_OK;
+}
+
+rd_status rd_tiled_get_count(rd_tiled* h, int64_t* ns)
+{
+    if (!h || !ns) return set_err(RD_ERR_ARG, "null argument");
+    *ns = h->have_result ? h->run.ns() : 0;
+    return RD_OK;
+}
+
+rd_status rd_tiled_get_points(rd_tiled* h, float* out, int64_t pitch, int dst_on_device,
+                              void* stream)
+{
+    if (!h) return set_err(RD_ERR_ARG, "null handle");
+    if (!h->have_result) return set_err(RD_ERR_ARG, "no result: call rd_tiled_run first");
+    rd_status s = store_points(h->run.result(), h->run.ns(), h->dim, h->out_layout, pitch, out,
+                               dst_on_device, h->staging, (cudaStream_t)stream);
+    if (s != RD_OK) return s;
+    CK_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    return RD_OK;
+}
+
+rd_status rd_tiled_get_timers(rd_tiled* h, float* whole, float* build, float* rd_tiles,
+                              float* refinement)
+{
+    if (!h) return set_err(RD_ERR_ARG, "null handle");
+    const TiledTimers& t = h->run.timers();
+    if (whole) *whole = t.whole_ms;
+    if (build) *build = t.build_ms;
+    if (rd_tiles) *rd_tiles = t.rd_ms;
+    if (refinement) *refinement = t.refine_ms;
+    return RD_OK;
+}
+
+rd_status rd_tiled_get_stats(rd_tiled* h, rd_run_stats* st)
+{
+    if (!h || !st) return set_err(RD_ERR_ARG, "null argument");
+    fill_stats(h->run.stats(), st);
+    return RD_OK;
+}
+
+rd_status rd_tiled_get_leaf_count(rd_tiled* h, int64_t* n_leaves)
+{
+    if (!h || !n_leaves) return set_err(RD_ERR_ARG, "null argument");
+    *n_leaves = h->run.n_leaves();
+    return RD_OK;
+}
+
+rd_status rd_tiled_destroy(rd_tiled* h)
 {
     delete h;
     return RD_OK;

@@ -73,15 +73,25 @@ int Engine::setup(int dim, const std::vector<CloudDesc>& clouds,
     h_cl_ = clouds;
     h_gr_ = groups;
     chunk_pts_ = tune.block * tune.items;
-    // chunks and chosen capacity
+    int dev = 0;
+    RD_CK(cudaGetDevice(&dev));
+    RD_CK(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev));
+    // Chunks split every cloud evenly into at most chunk_pts_ points each.  A
+    // cloud big enough to fill the GPU on its own gets a multiple of the SM
+    // count, so that the single wave of assignment CTAs is balanced.
     int64_t chunk = 0, s_off = 0;
+    chunk_max_ = 0;
     h_chunk_cloud_.clear();
     for (size_t c = 0; c < h_cl_.size(); ++c) {
         CloudDesc& cd = h_cl_[c];
         cd.s_off = s_off;
         s_off += cd.n_own;
         cd.chunk_begin = chunk;
-        cd.n_chunks = (cd.n_all + chunk_pts_ - 1) / chunk_pts_;
+        int64_t nch = (cd.n_all + chunk_pts_ - 1) / chunk_pts_;
+        if (h_cl_.size() == 1 && nch >= 2 * sms_) nch = (nch + sms_ - 1) / sms_ * sms_;
+        cd.n_chunks = (int32_t)nch;
+        if (nch > 0)
+            chunk_max_ = std::max<int>(chunk_max_, (int)((cd.n_all + nch - 1) / nch));
         for (int k = 0; k < cd.n_chunks; ++k) h_chunk_cloud_.push_back((int32_t)c);
         chunk += cd.n_chunks;
         cd.n_seg = (cd.n_chunks + SEG - 1) / SEG;
@@ -92,7 +102,7 @@ int Engine::setup(int dim, const std::vector<CloudDesc>& clouds,
     RD_CK(bS_.ensure(sizeof(float) * (size_t)(s_off * dim + 4)));
     RD_CK(bNext_.ensure(sizeof(int32_t) * (size_t)(s_off + 1)));
     RD_CK(bKeys_.ensure(sizeof(int32_t) * (size_t)(total_points + 1)));
-    RD_CK(bGrouped_.ensure(sizeof(float) * (size_t)(total_points * dim + 4)));
+    RD_CK(bGrouped_.ensure(sizeof(int32_t) * (size_t)(total_points + 4)));
     RD_CK(bNs_.ensure(4 * (nc + 1)));
     RD_CK(bPhase_.ensure(4 * (nc + 1)));
     RD_CK(bCont_.ensure(4 * (nc + 1)));
@@ -117,12 +127,13 @@ EngineView Engine::view() const
     v.P = bP_.as<float>();
     v.S = bS_.as<float>();
     v.keys = bKeys_.as<int32_t>();
-    v.grouped = bGrouped_.as<float>();
+    v.perm = bGrouped_.as<int32_t>();
     v.hist = bHist_.as<int32_t>();
     v.segsum = bSegsum_.as<int32_t>();
     v.cnt = bCnt_.as<int32_t>();
     v.base = bBase_.as<int32_t>();
     v.next = bNext_.as<int32_t>();
+    v.hash = bHash_.as<int32_t>();
     v.ns = bNs_.as<int32_t>();
     v.phase = bPhase_.as<int32_t>();
     v.cont = bCont_.as<int32_t>();
@@ -147,6 +158,7 @@ EngineView Engine::view() const
     v.n_slots = n_slots_;
     v.n_segs = n_segs_;
     v.chunk_pts = chunk_pts_;
+    v.chunk_max = chunk_max_;
     v.hist_smem = hist_smem_;
     v.scat_smem = scat_smem_;
     v.max_passes = max_passes;
@@ -205,7 +217,7 @@ int Engine::finish_setup_after_choose(cudaStream_t st)
     }
     // shared-memory budgets (ints)
     hist_smem_ = std::min(max_ns, 24 * 1024);
-    scat_smem_ = std::min(max_ns, 12 * 1024);
+    scat_smem_ = std::min(max_ns, 4 * 1024);
     RD_CK(upload(bCl_, h_cl_, st));
     RD_CK(upload(bGr_, h_gr_, st));
     RD_CK(upload(bSlotCloud_, h_slot_cloud_, st));
@@ -279,9 +291,18 @@ int Engine::run(cudaStream_t st, bool use_graph)
     RD_CK(upload(bGr_, h_gr_, st));
     RD_CK(upload(bChunkCloud_, h_chunk_cloud_, st));
     {
+        // one large cloud: GPU-wide choose rounds; otherwise one CTA per cloud
+        const bool rounds = h_cl_.size() == 1 && h_cl_[0].n_own >= (1 << 16);
+        if (rounds) {
+            RD_CK(bHash_.ensure(4 * (size_t)choose_hash_buckets()));
+            RD_CK(bSurv_.ensure((size_t)h_cl_[0].n_own + 16));
+        }
         EngineView v0 = view();
         RD_CK(launch_reset(v0, st));
-        RD_CK(launch_choose(dim_, v0, st));
+        if (rounds)
+            RD_CK(launch_choose_rounds(dim_, v0, 0, h_cl_[0].n_own, bSurv_.as<uint8_t>(), st));
+        else
+            RD_CK(launch_choose(dim_, v0, st));
     }
     if (int rc = finish_setup_after_choose(st)) return rc;
     const EngineView v = view();
@@ -290,14 +311,29 @@ int Engine::run(cudaStream_t st, bool use_graph)
         if (int rc = build_graph(st)) return rc;
         RD_CK(cudaGraphLaunch(exec_, st));
     } else {
+        cudaEvent_t a0 = nullptr, a1 = nullptr;
+        if (profile_assign) {
+            RD_CK(cudaEventCreate(&a0));
+            RD_CK(cudaEventCreate(&a1));
+        }
+        stats_.assign_ms = 0;
+        stats_.assign_launches = 0;
         for (;;) {
-            RD_CK(launch_pass(dim_, v, tune, assign_grid_, st));
+            RD_CK(launch_pass(dim_, v, tune, assign_grid_, st, a0, a1));
             RD_CK(launch_loopcond(v, cudaGraphConditionalHandle(), 0, st));
             int32_t act = 0;
             RD_CK(cudaMemcpyAsync(&act, v.ctr + CTR_ACTIVE, 4, cudaMemcpyDeviceToHost, st));
             RD_CK(cudaStreamSynchronize(st));
+            if (a0) {
+                float ms = 0;
+                RD_CK(cudaEventElapsedTime(&ms, a0, a1));
+                stats_.assign_ms += ms;
+                stats_.assign_launches += 1;
+            }
             if (act == 0) break;
         }
+        if (a0) cudaEventDestroy(a0);
+        if (a1) cudaEventDestroy(a1);
     }
     // results
     const size_t nc = h_cl_.size();

@@ -39,11 +39,11 @@ struct EngineView {
     float* P;                    // packed evolve points, ROW_MAJOR
     float* S;                    // chosen points, ROW_MAJOR, capacity n_own per cloud
     int32_t* keys;               // per point slot: assigned chosen index or -1
-    float* grouped;              // per point slot: points regrouped by key
+    int32_t* perm;               // per point slot: point indices grouped by key, index order
     int32_t* hist;               // per cloud: n_chunks x ns_cap key histogram
     int32_t* segsum;             // per cloud: n_seg x ns_cap segment sums
     int32_t* cnt;                // per chosen slot: members in the last pass
-    int32_t* base;               // per chosen slot: first grouped slot
+    int32_t* base;               // per chosen slot: first slot of its segment of perm
     int32_t* hash;               // choose hash heads
     int32_t* next;               // per chosen slot: choose hash chain
     int32_t* ns;                 // per cloud: current chosen count
@@ -70,7 +70,8 @@ struct EngineView {
     int32_t n_chunks;
     int32_t n_slots;
     int32_t n_segs;
-    int32_t chunk_pts;           // points per assignment chunk
+    int32_t chunk_pts;           // max points per assignment chunk (BLOCK*ITEMS)
+    int32_t chunk_max;           // largest chunk actually used (scatter staging)
     int32_t hist_smem;           // ints of dynamic smem for the assign histogram
     int32_t scat_smem;           // ints of dynamic smem per scatter warp
     int32_t max_passes;
@@ -86,9 +87,15 @@ struct TuneParams {
 
 // host-side launchers (rd_kernels.cu); all enqueue on `st`
 cudaError_t launch_choose(int dim, const EngineView& v, cudaStream_t st);
+// choose of one large cloud c (n own points) in GPU-wide rounds; v.hash must
+// hold choose_hash_buckets() ints and surv n bytes
+cudaError_t launch_choose_rounds(int dim, const EngineView& v, int c, int n, uint8_t* surv,
+                                 cudaStream_t st);
+int choose_hash_buckets();
 cudaError_t prepare_pass(int dim, const EngineView& v, const TuneParams& tp);
+// a0/a1 (optional) are recorded on `st` right before and after the assign kernel
 cudaError_t launch_pass(int dim, const EngineView& v, const TuneParams& tp, int assign_grid,
-                        cudaStream_t st);
+                        cudaStream_t st, cudaEvent_t a0 = nullptr, cudaEvent_t a1 = nullptr);
 cudaError_t launch_loopcond(const EngineView& v, cudaGraphConditionalHandle h, int use_handle,
                             cudaStream_t st);
 cudaError_t launch_reset(const EngineView& v, cudaStream_t st);

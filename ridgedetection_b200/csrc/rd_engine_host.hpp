@@ -27,6 +27,8 @@ struct RunStats {
     int64_t max_passes = 0;       // max over clouds
     double pairs = 0;             // sum over clouds of sum over passes of n_all*ns
     int err_bits = 0;
+    double assign_ms = 0;         // host-loop runs with profile_assign: assign kernel time
+    int64_t assign_launches = 0;
 };
 
 class Engine {
@@ -63,6 +65,7 @@ public:
     int max_outer = 4096;
     int max_iters = 1 << 18;
     TuneParams tune{128, 8};
+    bool profile_assign = false;  // host loop only: time every assign launch with events
     std::string last_error;
 
 private:
@@ -81,12 +84,14 @@ private:
     std::vector<int32_t> h_dec_hbits_;
     int32_t n_chunks_ = 0, n_slots_ = 0, n_segs_ = 0;
     int chunk_pts_ = 1024;
+    int chunk_max_ = 0;
+    int sms_ = 148;
     int hist_smem_ = 0, scat_smem_ = 0;
     int assign_grid_ = 0;
     RunStats stats_;
 
     DevBuf bCl_, bGr_, bChunkCloud_, bSlotCloud_, bSegList_;
-    DevBuf bP_, bS_, bKeys_, bGrouped_, bHist_, bSegsum_, bCnt_, bBase_, bNext_;
+    DevBuf bP_, bS_, bKeys_, bGrouped_, bHist_, bSegsum_, bCnt_, bBase_, bNext_, bHash_, bSurv_;
     DevBuf bNs_, bPhase_, bCont_, bPasses_, bTotPasses_, bOuter_, bErr_, bPairs_, bCtr_;
     DevBuf bDx_, bDcell_, bDalive_, bDc1_, bDc2_, bDbstart_, bDitems_, bDecHoff_, bDecHbits_;
 

@@ -193,6 +193,154 @@ __global__ void __launch_bounds__(BLOCK) k_choose(EngineView v)
 }
 
 // ---------------------------------------------------------------------------
+// choose for one large cloud, in rounds over growing ranges [a, b) of its
+// points (same semantics as k_choose).  k_choose_filter, spread over the whole
+// GPU, drops every point of the range that has a point chosen in earlier rounds
+// within r1 (hash grid read from global memory); k_choose_resolve, one CTA,
+// walks the survivors in order and applies the sequential greedy rule with a
+// shared-memory mirror of the grid, then writes the grid back for the next
+// round's filter.
+// ---------------------------------------------------------------------------
+template <int DIM>
+__global__ void __launch_bounds__(256) k_choose_filter(EngineView v, int c, int a, int b,
+                                                       uint8_t* __restrict__ surv)
+{
+    using CS = ChooseSmem<DIM>;
+    constexpr int NB = Pow3<DIM>::v;
+    const CloudDesc cd = v.cl[c];
+    const float rsq = sqr_rn(cd.r1);
+    const double inv = 1.0 / ((double)cd.r1 * (1.0 + 1.0 / 1024.0));
+    const uint32_t hmask = CS::HB - 1;
+    const int32_t* heads = v.hash;
+    const float* gS = v.S + cd.s_off * DIM;
+    const int32_t* gnext = v.next + cd.s_off;
+    const float* P = v.P + cd.p_off * DIM;
+    for (int i = a + blockIdx.x * blockDim.x + threadIdx.x; i < b; i += gridDim.x * blockDim.x) {
+        float p[DIM];
+        int cc[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            p[d] = P[(int64_t)i * DIM + d];
+            cc[d] = cell_of(p[d], inv);
+        }
+        bool hit = false;
+        for (int t = 0; t < NB && !hit; ++t) {
+            int nc[DIM];
+            neighbour_cell<DIM>(cc, (t + NB / 2) % NB, nc);
+            for (int q = heads[cell_hash<DIM>(nc) & hmask]; q >= 0 && !hit; q = gnext[q]) {
+                float s[DIM];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) s[d] = gS[(int64_t)q * DIM + d];
+                hit = sqdist_exact<DIM>(p, s) <= rsq;
+            }
+        }
+        surv[i - a] = hit ? 0 : 1;
+    }
+}
+
+template <int DIM, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_choose_resolve(EngineView v, int c, int a, int b,
+                                                          const uint8_t* __restrict__ surv,
+                                                          int first)
+{
+    using CS = ChooseSmem<DIM>;
+    constexpr int NB = Pow3<DIM>::v;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    int32_t* s_heads = reinterpret_cast<int32_t*>(smem_raw);  // HB
+    int32_t* s_next = s_heads + CS::HB;                        // SCAP
+    float* s_S = reinterpret_cast<float*>(s_next + CS::SCAP);  // SCAP*DIM
+    int32_t* s_list = reinterpret_cast<int32_t*>(s_S + CS::SCAP * DIM);  // BLOCK
+    __shared__ int s_ns;
+    __shared__ int s_wsum[BLOCK / 32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const CloudDesc cd = v.cl[c];
+    const float rsq = sqr_rn(cd.r1);
+    const double inv = 1.0 / ((double)cd.r1 * (1.0 + 1.0 / 1024.0));
+    const uint32_t hmask = CS::HB - 1;
+    float* gS = v.S + cd.s_off * DIM;
+    int32_t* gnext = v.next + cd.s_off;
+    const float* P = v.P + cd.p_off * DIM;
+    const int ns0 = first ? 0 : v.ns[c];
+    for (int h = tid; h < CS::HB; h += BLOCK) s_heads[h] = first ? -1 : v.hash[h];
+    for (int q = tid; q < min(ns0, CS::SCAP); q += BLOCK) {
+        s_next[q] = gnext[q];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) s_S[q * DIM + d] = gS[(int64_t)q * DIM + d];
+    }
+    if (tid == 0) s_ns = ns0;
+    __syncthreads();
+    auto coord = [&](int q, int d) -> float {
+        return (q < CS::SCAP) ? s_S[q * DIM + d] : gS[(int64_t)q * DIM + d];
+    };
+    auto nxt = [&](int q) -> int { return (q < CS::SCAP) ? s_next[q] : gnext[q]; };
+    for (int base = a; base < b; base += BLOCK) {
+        const int i = base + tid;
+        const bool f = (i < b) && surv[i - a];
+        if (!__syncthreads_or(f)) continue;
+        const unsigned bal = __ballot_sync(FULL, f);
+        if (lane == 0) s_wsum[warp] = __popc(bal);
+        __syncthreads();
+        int wbase = 0, tot = 0;
+        for (int w = 0; w < BLOCK / 32; ++w) {
+            const int x = s_wsum[w];
+            wbase += (w < warp) ? x : 0;
+            tot += x;
+        }
+        if (f) s_list[wbase + __popc(bal & lanemask_lt())] = i;
+        __syncthreads();
+        if (warp == 0) {
+            int ns = s_ns;
+            for (int sidx = 0; sidx < tot; ++sidx) {
+                const int pi = s_list[sidx];
+                float ps[DIM];
+                int cs[DIM];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) {
+                    ps[d] = P[(int64_t)pi * DIM + d];
+                    cs[d] = cell_of(ps[d], inv);
+                }
+                bool hit = false;
+                for (int o = lane; o < NB && !hit; o += 32) {
+                    int nc[DIM];
+                    neighbour_cell<DIM>(cs, o, nc);
+                    for (int q = s_heads[cell_hash<DIM>(nc) & hmask]; q >= 0 && !hit; q = nxt(q)) {
+                        float s[DIM];
+#pragma unroll
+                        for (int d = 0; d < DIM; ++d) s[d] = coord(q, d);
+                        hit = sqdist_exact<DIM>(ps, s) <= rsq;
+                    }
+                }
+                hit = __any_sync(FULL, hit);
+                if (!hit) {
+                    if (lane == 0) {
+                        const uint32_t hb = cell_hash<DIM>(cs) & hmask;
+                        const int head = s_heads[hb];
+#pragma unroll
+                        for (int d = 0; d < DIM; ++d) gS[(int64_t)ns * DIM + d] = ps[d];
+                        gnext[ns] = head;
+                        if (ns < CS::SCAP) {
+#pragma unroll
+                            for (int d = 0; d < DIM; ++d) s_S[ns * DIM + d] = ps[d];
+                            s_next[ns] = head;
+                        }
+                        s_heads[hb] = ns;
+                    }
+                    ++ns;
+                }
+                __syncwarp();
+            }
+            if (lane == 0) s_ns = ns;
+        }
+        __syncthreads();
+    }
+    for (int h = tid; h < CS::HB; h += BLOCK) v.hash[h] = s_heads[h];
+    if (tid == 0) {
+        v.ns[c] = s_ns;
+        v.phase[c] = (s_ns > 0) ? PH_EVOLVE : PH_DONE;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // assign: rd/cpu/brute_force/evolve.hpp:43-66 over one chunk of CHUNK cloud
 // points per work item; writes the key of every point and the chunk's key
 // histogram row.  This is the hot kernel.
@@ -239,8 +387,9 @@ __global__ void __launch_bounds__(BLOCK) k_assign(EngineView v)
         if (v.phase[c] != PH_EVOLVE) continue;
         const CloudDesc cd = v.cl[c];
         const int lc = item - (int)cd.chunk_begin;
-        const int start = lc * (BLOCK * ITEMS);
-        const int n = cd.n_all;
+        // chunks split the cloud evenly (at most BLOCK*ITEMS points each)
+        const int start = (int)(((int64_t)lc * cd.n_all) / cd.n_chunks);
+        const int n = (int)(((int64_t)(lc + 1) * cd.n_all) / cd.n_chunks);  // chunk end
         const int ns = v.ns[c];
         const float* P = v.P + cd.p_off * DIM;
         const float* gS = v.S + cd.s_off * DIM;
@@ -324,11 +473,14 @@ __global__ void __launch_bounds__(256) k_colscan(EngineView v)
     int32_t* h = v.hist + cd.hist_off + (int64_t)r0 * cd.ns_cap;
     int32_t* out = v.segsum + cd.seg_off + (int64_t)seg * cd.ns_cap;
     for (int k = threadIdx.x; k < ns; k += blockDim.x) {
+        int x[SEG];  // all loads in flight before the dependent prefix
+#pragma unroll
+        for (int r = 0; r < SEG; ++r) x[r] = (r < rows) ? h[(int64_t)r * cd.ns_cap + k] : 0;
         int run = 0;
-        for (int r = 0; r < rows; ++r) {
-            const int x = h[(int64_t)r * cd.ns_cap + k];
-            h[(int64_t)r * cd.ns_cap + k] = run;
-            run += x;
+#pragma unroll
+        for (int r = 0; r < SEG; ++r) {
+            if (r < rows) h[(int64_t)r * cd.ns_cap + k] = run;
+            run += x[r];
         }
         out[k] = run;
     }
@@ -351,10 +503,16 @@ __global__ void __launch_bounds__(BLOCK) k_segscan(EngineView v)
     int32_t* base = v.base + cd.key_off;
     for (int k = threadIdx.x; k < ns; k += BLOCK) {
         int run = 0;
-        for (int s = 0; s < cd.n_seg; ++s) {
-            const int x = sg[(int64_t)s * cd.ns_cap + k];
-            sg[(int64_t)s * cd.ns_cap + k] = run;
-            run += x;
+        for (int s0 = 0; s0 < cd.n_seg; s0 += 8) {  // 8 loads in flight per step
+            int x[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                x[u] = (s0 + u < cd.n_seg) ? sg[(int64_t)(s0 + u) * cd.ns_cap + k] : 0;
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                if (s0 + u < cd.n_seg) sg[(int64_t)(s0 + u) * cd.ns_cap + k] = run;
+                run += x[u];
+            }
         }
         cnt[k] = run;
     }
@@ -389,13 +547,16 @@ __global__ void __launch_bounds__(BLOCK) k_segscan(EngineView v)
 
 // ---------------------------------------------------------------------------
 // stable scatter: one warp per chunk walks its points in index order and
-// writes each assigned point to the next free slot of its key's segment, so
-// every segment lists its members in cloud-point index order.
+// writes each assigned point's index to the next free slot of its key's
+// segment of the permutation, so every segment lists its members in
+// cloud-point index order.  Keys of the chunk and the per-key start slots are
+// staged in shared memory first; the ordered walk then touches shared memory
+// only (match_any groups equal keys of 32 consecutive points, the group
+// leader advances the key's cursor).
 // ---------------------------------------------------------------------------
-template <int DIM>
 __global__ void __launch_bounds__(128) k_scatter(EngineView v)
 {
-    extern __shared__ int s_ctr_all[];
+    extern __shared__ int s_dyn[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int item = blockIdx.x * 4 + warp;
     if (item >= v.n_chunks) return;
@@ -408,18 +569,21 @@ __global__ void __launch_bounds__(128) k_scatter(EngineView v)
     int32_t* row = v.hist + cd.hist_off + (int64_t)lc * cd.ns_cap;
     const int32_t* sg = v.segsum + cd.seg_off + (int64_t)seg * cd.ns_cap;
     const int32_t* bs = v.base + cd.key_off;
+    int* s_keys = s_dyn + warp * (v.chunk_max + v.scat_smem);
     const bool in_smem = ns <= v.scat_smem;
-    int32_t* ctr = in_smem ? (s_ctr_all + warp * v.scat_smem) : row;
+    int32_t* ctr = in_smem ? (s_keys + v.chunk_max) : row;
+    const int start = (int)(((int64_t)lc * cd.n_all) / cd.n_chunks);
+    const int end = (int)(((int64_t)(lc + 1) * cd.n_all) / cd.n_chunks);
+    const int len = end - start;
+    const int32_t* keys = v.keys + cd.p_off + start;
+    // stage the chunk's keys and the per-key start slots (independent loads)
+    for (int e = lane; e < len; e += 32) s_keys[e] = keys[e];
     for (int k = lane; k < ns; k += 32) ctr[k] = bs[k] + sg[k] + row[k];
     __syncwarp();
-    const int start = lc * v.chunk_pts;
-    const int end = min(cd.n_all, start + v.chunk_pts);
-    const int32_t* keys = v.keys + cd.p_off;
-    const float* P = v.P + cd.p_off * DIM;
-    float* G = v.grouped + cd.p_off * DIM;
-    for (int off = start; off < end; off += 32) {
+    int32_t* perm = v.perm + cd.p_off;
+    for (int off = 0; off < len; off += 32) {
         const int i = off + lane;
-        const int key = (i < end) ? keys[i] : -1;
+        const int key = (i < len) ? s_keys[i] : -1;
         const unsigned m = __match_any_sync(FULL, key);
         const int leader = __ffs(m) - 1;
         int b = 0;
@@ -428,11 +592,7 @@ __global__ void __launch_bounds__(128) k_scatter(EngineView v)
             ctr[key] = b + __popc(m);
         }
         b = __shfl_sync(FULL, b, leader);
-        if (key >= 0) {
-            const int pos = b + __popc(m & lanemask_lt());
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) G[(int64_t)pos * DIM + d] = P[(int64_t)i * DIM + d];
-        }
+        if (key >= 0) perm[b + __popc(m & lanemask_lt())] = start + i;
         __syncwarp();
     }
 }
@@ -441,12 +601,17 @@ __global__ void __launch_bounds__(128) k_scatter(EngineView v)
 // ordered sum + shift: one warp per chosen slot.  Lane d (< DIM) folds
 // coordinate d of the key's members in index order with rounded adds,
 // exactly as rd/cpu/brute_force/evolve.hpp:71-74 accumulates, then applies the
-// movement test of evolve.hpp:143-177.
+// movement test of evolve.hpp:143-177.  Members are gathered through the
+// permutation written by k_scatter, BP at a time, the next block in flight
+// while the current one is folded.
 // ---------------------------------------------------------------------------
 template <int DIM>
 __global__ void __launch_bounds__(256) k_sum_shift(EngineView v)
 {
-    __shared__ float s_buf[8][32 * DIM];
+    constexpr int BP = 128;             // members staged per step
+    constexpr int R = BP * DIM / 32;    // floats per lane per step
+    __shared__ float s_buf[8][BP * DIM];
+    __shared__ int s_idx[8][BP];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = blockIdx.x * 8 + warp;
     if (g >= v.n_slots) return;
@@ -457,15 +622,43 @@ __global__ void __launch_bounds__(256) k_sum_shift(EngineView v)
     if (k >= v.ns[c]) return;
     const int n = v.cnt[cd.key_off + k];
     if (n == 0) return;
-    const float* G = v.grouped + (cd.p_off + v.base[cd.key_off + k]) * DIM;
+    const int32_t* perm = v.perm + cd.p_off + v.base[cd.key_off + k];
+    const float* P = v.P + cd.p_off * DIM;
     float* buf = s_buf[warp];
-    float sum = 0.0f;
-    for (int off = 0; off < n; off += 32) {
-        const int m = min(32, n - off);
-        for (int e = lane; e < m * DIM; e += 32) buf[e] = G[(int64_t)off * DIM + e];
+    int* sidx = s_idx[warp];
+    float nxt[R];
+    auto fetch = [&](int off) {
+        const int m = min(BP, n - off);
+#pragma unroll
+        for (int u = 0; u < BP / 32; ++u) {
+            const int j = u * 32 + lane;
+            sidx[j] = (j < m) ? perm[off + j] : 0;
+        }
         __syncwarp();
-        if (lane < DIM)
-            for (int j = 0; j < m; ++j) sum = __fadd_rn(sum, buf[j * DIM + lane]);
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+            const int e = u * 32 + lane;
+            const int j = e / DIM, d = e - (e / DIM) * DIM;
+            nxt[u] = (j < m) ? P[(int64_t)sidx[j] * DIM + d] : 0.0f;
+        }
+        __syncwarp();
+    };
+    fetch(0);
+    float sum = 0.0f;
+    for (int off = 0; off < n; off += BP) {
+        const int m = min(BP, n - off);
+#pragma unroll
+        for (int u = 0; u < R; ++u) buf[u * 32 + lane] = nxt[u];
+        __syncwarp();
+        if (off + BP < n) fetch(off + BP);  // next block in flight during the fold
+        if (lane < DIM) {
+            if (m == BP) {
+#pragma unroll 32
+                for (int j = 0; j < BP; ++j) sum = __fadd_rn(sum, buf[j * DIM + lane]);
+            } else {
+                for (int j = 0; j < m; ++j) sum = __fadd_rn(sum, buf[j * DIM + lane]);
+            }
+        }
         __syncwarp();
     }
     int moved = 0;
@@ -792,15 +985,16 @@ cudaError_t prepare_pass_dim(const EngineView& v, const TuneParams& tp)
     RD_PREP_CASE(128, 16)
 #undef RD_PREP_CASE
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_scatter<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                4 * v.scat_smem * 4);
+    return cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                4 * (v.chunk_max + v.scat_smem) * 4);
 }
 
 template <int DIM>
 cudaError_t launch_pass_dim(const EngineView& v, const TuneParams& tp, int assign_grid,
-                            cudaStream_t st)
+                            cudaStream_t st, cudaEvent_t a0, cudaEvent_t a1)
 {
     const int hist_bytes = v.hist_smem * 4;
+    if (a0) cudaEventRecord(a0, st);
 #define RD_ASSIGN_CASE(B, I)                                                                  \
     if (tp.block == B && tp.items == I) {                                                     \
         k_assign<DIM, B, I><<<assign_grid, B, hist_bytes, st>>>(v);                           \
@@ -812,9 +1006,11 @@ cudaError_t launch_pass_dim(const EngineView& v, const TuneParams& tp, int assig
     RD_ASSIGN_CASE(128, 16)
     { return cudaErrorInvalidValue; }
 #undef RD_ASSIGN_CASE
+    if (a1) cudaEventRecord(a1, st);
     if (v.n_segs > 0) k_colscan<<<v.n_segs, 256, 0, st>>>(v);
     k_segscan<1024><<<v.n_clouds, 1024, 0, st>>>(v);
-    if (v.n_chunks > 0) k_scatter<DIM><<<(v.n_chunks + 3) / 4, 128, 4 * v.scat_smem * 4, st>>>(v);
+    if (v.n_chunks > 0)
+        k_scatter<<<(v.n_chunks + 3) / 4, 128, 4 * (v.chunk_max + v.scat_smem) * 4, st>>>(v);
     if (v.n_slots > 0) k_sum_shift<DIM><<<(v.n_slots + 7) / 8, 256, 0, st>>>(v);
     k_control<<<(v.n_clouds + 255) / 256, 256, 0, st>>>(v);
     k_decimate<DIM, 512><<<v.n_groups, 512, 0, st>>>(v);
@@ -825,7 +1021,7 @@ template <int DIM>
 cudaError_t launch_choose_dim(const EngineView& v, cudaStream_t st)
 {
     using CS = ChooseSmem<DIM>;
-    constexpr int B = 512;
+    constexpr int B = 1024;
     const int bytes = CS::HB * 4 + CS::SCAP * 4 + CS::SCAP * DIM * 4 + B * DIM * 8;
     cudaError_t e =
         cudaFuncSetAttribute(k_choose<DIM, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
@@ -834,7 +1030,49 @@ cudaError_t launch_choose_dim(const EngineView& v, cudaStream_t st)
     return cudaGetLastError();
 }
 
+// rounds over [0, n): 4096 points first, doubling; needs v.hash (HB ints) and
+// surv (n bytes)
+template <int DIM>
+cudaError_t launch_choose_rounds_dim(const EngineView& v, int c, int n, uint8_t* surv,
+                                     cudaStream_t st)
+{
+    using CS = ChooseSmem<DIM>;
+    constexpr int B = 1024;
+    const int bytes = CS::HB * 4 + CS::SCAP * 4 + CS::SCAP * DIM * 4 + B * 4;
+    cudaError_t e = cudaFuncSetAttribute(k_choose_resolve<DIM, B>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    int a = 0, size = 4096, first = 1;
+    while (a < n) {
+        const int b = (int)std::min<int64_t>((int64_t)n, (int64_t)a + size);
+        if (first) {
+            e = cudaMemsetAsync(surv, 1, (size_t)(b - a), st);
+            if (e != cudaSuccess) return e;
+        } else {
+            const int grid = std::max(1, std::min((b - a + 255) / 256, 148 * 16));
+            k_choose_filter<DIM><<<grid, 256, 0, st>>>(v, c, a, b, surv);
+        }
+        k_choose_resolve<DIM, B><<<1, B, bytes, st>>>(v, c, a, b, surv, first);
+        a = b;
+        size = (int)std::min<int64_t>((int64_t)size * 2, 1 << 30);
+        first = 0;
+    }
+    return cudaGetLastError();
+}
+
 }  // namespace
+
+cudaError_t launch_choose_rounds(int dim, const EngineView& v, int c, int n, uint8_t* surv,
+                                 cudaStream_t st)
+{
+    switch (dim) {
+        case 2: return launch_choose_rounds_dim<2>(v, c, n, surv, st);
+        case 3: return launch_choose_rounds_dim<3>(v, c, n, surv, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+int choose_hash_buckets() { return ChooseSmem<2>::HB; }
 
 cudaError_t launch_choose(int dim, const EngineView& v, cudaStream_t st)
 {
@@ -855,11 +1093,11 @@ cudaError_t prepare_pass(int dim, const EngineView& v, const TuneParams& tp)
 }
 
 cudaError_t launch_pass(int dim, const EngineView& v, const TuneParams& tp, int assign_grid,
-                        cudaStream_t st)
+                        cudaStream_t st, cudaEvent_t a0, cudaEvent_t a1)
 {
     switch (dim) {
-        case 2: return launch_pass_dim<2>(v, tp, assign_grid, st);
-        case 3: return launch_pass_dim<3>(v, tp, assign_grid, st);
+        case 2: return launch_pass_dim<2>(v, tp, assign_grid, st, a0, a1);
+        case 3: return launch_pass_dim<3>(v, tp, assign_grid, st, a0, a1);
         default: return cudaErrorInvalidValue;
     }
 }
