@@ -159,6 +159,24 @@ RD_API rd_status rd_batch_get_points(rd_batch* h, int32_t cloud, float* out, int
 RD_API rd_status rd_batch_get_stats(rd_batch* h, rd_run_stats* st);
 RD_API rd_status rd_batch_destroy(rd_batch* h);
 
+/* ---------------------------------------------------------------------------
+ * Evolve adjoint (no reference counterpart; the reference is forward-only).
+ * Forward: `iters` evolve passes from S0 (ns chosen points, usually copies of
+ * cloud points) with the movement test off: each non-empty cluster's point
+ * becomes the FP32 mean (index-order sum / count) of its assigned cloud
+ * points; empty clusters keep their point.  Decimation is frozen.
+ * Reverse for L = sum_k <W_k, S_final_k> with the assignments frozen, in FP64:
+ * grad_P (np x dim) = dL/dP through the cluster means; grad_S0 (ns x dim,
+ * optional) = dL/dS0, i.e. what flows through clusters that stayed empty.
+ * checkpoint_every = 0 keeps every pass's assignment (iters x np ints);
+ * k > 0 stores S every k passes and recomputes assignments per segment.
+ * on_device selects device (1) or host (0) pointers for all arrays.
+ * ------------------------------------------------------------------------- */
+RD_API rd_status rd_evolve_adjoint(int dim, const float* P, int64_t np, const float* S0,
+                                   int64_t ns, float r1, int iters, int checkpoint_every,
+                                   const double* W, float* S_final, double* grad_P,
+                                   double* grad_S0, int on_device, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

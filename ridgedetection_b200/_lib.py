@@ -80,6 +80,7 @@ SIGNATURES = {
     "rd_tiled_get_stats": [_vp, ctypes.POINTER(RunStats)],
     "rd_tiled_get_leaf_count": [_vp, _pi64],
     "rd_tiled_destroy": [_vp],
+    "rd_evolve_adjoint": [_i, _vp, _i64, _vp, _i64, _f, _i, _i, _vp, _vp, _vp, _vp, _i, _vp],
     "rd_batch_create": [ctypes.POINTER(_vp)],
     "rd_batch_set_loop_mode": [_vp, _i],
     "rd_batch_run": [_vp, ctypes.POINTER(CloudDesc), _i32, _vp, _i64, _i, _vp],

@@ -2,6 +2,7 @@
 #include "../../include/rd_c_api.h"
 #include "rd_engine_host.hpp"
 #include "rd_tiled.hpp"
+#include "rd_adjoint.hpp"
 
 #include <algorithm>
 #include <cstring>
@@ -453,6 +454,59 @@ rd_status rd_tiled_get_leaf_count(rd_tiled* h, int64_t* n_leaves)
 rd_status rd_tiled_destroy(rd_tiled* h)
 {
     delete h;
+    return RD_OK;
+}
+
+// ------------------------------------------------------------------------
+// evolve adjoint
+// ------------------------------------------------------------------------
+rd_status rd_evolve_adjoint(int dim, const float* P, int64_t np, const float* S0, int64_t ns,
+                            float r1, int iters, int checkpoint_every, const double* W,
+                            float* S_final, double* grad_P, double* grad_S0, int on_device,
+                            void* stream)
+{
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (!P || !S0 || !W || !grad_P) return set_err(RD_ERR_ARG, "null argument");
+    if (np < 1 || np > INT32_MAX - 1024 || ns < 1 || ns > np)
+        return set_err(RD_ERR_ARG, "np/ns out of range");
+    if (iters < 0 || checkpoint_every < 0) return set_err(RD_ERR_ARG, "bad iteration counts");
+    if (!(r1 > 0.0f)) return set_err(RD_ERR_ARG, "r1 must be > 0");
+    thread_local AdjointRunner runner;
+    thread_local DevBuf dP, dS0, dW, dSf, dgP, dgS;
+    cudaStream_t st = (cudaStream_t)stream;
+    const float* pP = P;
+    const float* pS0 = S0;
+    const double* pW = W;
+    float* pSf = S_final;
+    double* pgP = grad_P;
+    double* pgS = grad_S0;
+    if (!on_device) {
+        CK_CUDA(dP.ensure(sizeof(float) * np * dim));
+        CK_CUDA(dS0.ensure(sizeof(float) * ns * dim));
+        CK_CUDA(dW.ensure(sizeof(double) * ns * dim));
+        CK_CUDA(dSf.ensure(sizeof(float) * ns * dim));
+        CK_CUDA(dgP.ensure(sizeof(double) * np * dim));
+        CK_CUDA(dgS.ensure(sizeof(double) * ns * dim));
+        CK_CUDA(cudaMemcpyAsync(dP.p, P, sizeof(float) * np * dim, cudaMemcpyHostToDevice, st));
+        CK_CUDA(cudaMemcpyAsync(dS0.p, S0, sizeof(float) * ns * dim, cudaMemcpyHostToDevice, st));
+        CK_CUDA(cudaMemcpyAsync(dW.p, W, sizeof(double) * ns * dim, cudaMemcpyHostToDevice, st));
+        pP = dP.as<float>();
+        pS0 = dS0.as<float>();
+        pW = dW.as<double>();
+        pSf = dSf.as<float>();
+        pgP = dgP.as<double>();
+        pgS = dgS.as<double>();
+    }
+    int rc = runner.run(dim, pP, np, pS0, ns, r1, iters, checkpoint_every, pW, pSf, pgP, pgS, st);
+    if (rc) return set_err((rd_status)rc, runner.last_error);
+    if (!on_device) {
+        if (S_final)
+            CK_CUDA(cudaMemcpyAsync(S_final, pSf, sizeof(float) * ns * dim, cudaMemcpyDeviceToHost, st));
+        CK_CUDA(cudaMemcpyAsync(grad_P, pgP, sizeof(double) * np * dim, cudaMemcpyDeviceToHost, st));
+        if (grad_S0)
+            CK_CUDA(cudaMemcpyAsync(grad_S0, pgS, sizeof(double) * ns * dim, cudaMemcpyDeviceToHost, st));
+        CK_CUDA(cudaStreamSynchronize(st));
+    }
     return RD_OK;
 }
 

@@ -112,6 +112,10 @@ int Engine::setup(int dim, const std::vector<CloudDesc>& clouds,
     RD_CK(bErr_.ensure(4 * (nc + 1)));
     RD_CK(bPairs_.ensure(8 * (nc + 1)));
     RD_CK(bCtr_.ensure(4 * CTR_COUNT));
+    RD_CK(bActCloud_.ensure(4 * (nc + 1)));
+    RD_CK(bActPre_.ensure(4 * 3 * (nc + 1)));
+    RD_CK(bGroupConv_.ensure(4 * (h_gr_.size() + 1)));
+    RD_CK(bReady_.ensure(4 * (h_gr_.size() + 1)));
     return 0;
 }
 
@@ -143,6 +147,10 @@ EngineView Engine::view() const
     v.err = bErr_.as<int32_t>();
     v.pairs = bPairs_.as<unsigned long long>();
     v.ctr = bCtr_.as<int32_t>();
+    v.act_cloud = bActCloud_.as<int32_t>();
+    v.act_pre = bActPre_.as<int32_t>();
+    v.group_conv = bGroupConv_.as<int32_t>();
+    v.ready = bReady_.as<int32_t>();
     v.dx = bDx_.as<float>();
     v.dcell = bDcell_.as<int32_t>();
     v.dalive = bDalive_.as<int32_t>();
@@ -164,6 +172,8 @@ EngineView Engine::view() const
     v.max_passes = max_passes;
     v.max_outer = max_outer;
     v.max_iters = max_iters;
+    v.n_sms = sms_;
+    v.flags = flags_;
     return v;
 }
 
@@ -283,14 +293,37 @@ int Engine::build_graph(cudaStream_t st)
     return 0;
 }
 
-int Engine::run(cudaStream_t st, bool use_graph)
+int Engine::run(cudaStream_t st, bool use_graph, int mode)
 {
     if (h_cl_.empty()) return 0;
     stats_ = RunStats();
+    flags_ = (mode == RUN_EVOLVE_ONLY) ? ENG_EVOLVE_ONLY : 0;
     RD_CK(upload(bCl_, h_cl_, st));
     RD_CK(upload(bGr_, h_gr_, st));
     RD_CK(upload(bChunkCloud_, h_chunk_cloud_, st));
-    {
+    if (mode == RUN_EVOLVE_ONLY || mode == RUN_DECIMATE_ONLY) {
+        // chosen sets supplied by the caller (given_ns, points already in S)
+        if (given_ns.size() != h_cl_.size()) {
+            last_error = "given chosen counts do not match the clouds";
+            return 1;
+        }
+        for (size_t c = 0; c < h_cl_.size(); ++c)
+            if (given_ns[c] < 0 || given_ns[c] > h_cl_[c].n_own) {
+                last_error = "given chosen count exceeds the cloud's capacity";
+                return 1;
+            }
+        EngineView v0 = view();
+        RD_CK(launch_reset(v0, st));
+        RD_CK(cudaMemcpyAsync(bNs_.p, given_ns.data(), 4 * given_ns.size(),
+                              cudaMemcpyHostToDevice, st));
+        if (int rc = finish_setup_after_choose(st)) return rc;
+        const EngineView v1 = view();
+        RD_CK(launch_set_given(v1, mode == RUN_DECIMATE_ONLY ? 1 : 0, st));
+        if (mode == RUN_DECIMATE_ONLY) {
+            RD_CK(launch_decimate(dim_, v1, st));
+            return collect(st);
+        }
+    } else {
         // one large cloud: GPU-wide choose rounds; otherwise one CTA per cloud
         const bool rounds = h_cl_.size() == 1 && h_cl_[0].n_own >= (1 << 16);
         if (rounds) {
@@ -303,10 +336,19 @@ int Engine::run(cudaStream_t st, bool use_graph)
             RD_CK(launch_choose_rounds(dim_, v0, 0, h_cl_[0].n_own, bSurv_.as<uint8_t>(), st));
         else
             RD_CK(launch_choose(dim_, v0, st));
+        if (mode == RUN_CHOOSE_ONLY) {
+            h_ns_.resize(h_cl_.size());
+            RD_CK(cudaMemcpyAsync(h_ns_.data(), bNs_.p, 4 * h_ns_.size(), cudaMemcpyDeviceToHost,
+                                  st));
+            RD_CK(cudaStreamSynchronize(st));
+            return 0;
+        }
+        if (int rc = finish_setup_after_choose(st)) return rc;
     }
-    if (int rc = finish_setup_after_choose(st)) return rc;
     const EngineView v = view();
     RD_CK(prepare_pass(dim_, v, tune));
+    // work lists of the first iteration
+    RD_CK(launch_loopcond(v, cudaGraphConditionalHandle(), 0, st, 0));
     if (use_graph) {
         if (int rc = build_graph(st)) return rc;
         RD_CK(cudaGraphLaunch(exec_, st));
@@ -335,7 +377,43 @@ int Engine::run(cudaStream_t st, bool use_graph)
         if (a0) cudaEventDestroy(a0);
         if (a1) cudaEventDestroy(a1);
     }
-    // results
+    return collect(st);
+}
+
+int Engine::adjoint_setup(cudaStream_t st)
+{
+    if (h_cl_.size() != 1 || given_ns.size() != 1) {
+        last_error = "adjoint: one cloud with a given chosen set";
+        return 1;
+    }
+    if (given_ns[0] < 1 || given_ns[0] > h_cl_[0].n_own) {
+        last_error = "adjoint: chosen count out of range";
+        return 1;
+    }
+    stats_ = RunStats();
+    flags_ = ENG_ALWAYS_MOVE;
+    RD_CK(upload(bCl_, h_cl_, st));
+    RD_CK(upload(bGr_, h_gr_, st));
+    EngineView v0 = view();
+    RD_CK(launch_reset(v0, st));
+    RD_CK(cudaMemcpyAsync(bNs_.p, given_ns.data(), 4, cudaMemcpyHostToDevice, st));
+    if (int rc = finish_setup_after_choose(st)) return rc;
+    const EngineView v = view();
+    RD_CK(launch_set_given(v, 0, st));
+    RD_CK(prepare_pass(dim_, v, tune));
+    return 0;
+}
+
+int Engine::adjoint_step(cudaStream_t st)
+{
+    const EngineView v = view();
+    RD_CK(launch_loopcond(v, cudaGraphConditionalHandle(), 0, st, 0));  // lists + ticket
+    RD_CK(launch_evolve_step(dim_, v, tune, assign_grid_, st));
+    return 0;
+}
+
+int Engine::collect(cudaStream_t st)
+{
     const size_t nc = h_cl_.size();
     std::vector<int32_t> tp(nc);
     std::vector<unsigned long long> pr(nc);

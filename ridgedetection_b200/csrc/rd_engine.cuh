@@ -23,10 +23,17 @@
 namespace rdb {
 
 enum : int {
+    ENG_EVOLVE_ONLY = 1,   // converged clouds finish without decimation
+    ENG_ALWAYS_MOVE = 2,   // adjoint forward: every non-empty cluster moves to its mean
+};
+
+enum : int {
     CTR_WORK = 0,      // assignment work ticket
     CTR_ACTIVE = 1,    // unfinished clouds after the last control step
     CTR_ITERS = 2,     // loop iterations run
     CTR_ERR = 3,       // OR of global error bits
+    CTR_NACT = 4,      // evolving clouds in the current work lists
+    CTR_NREADY = 5,    // groups ready for decimation in this iteration
     CTR_COUNT = 8,
 };
 
@@ -55,6 +62,10 @@ struct EngineView {
     int32_t* err;                // per cloud: ERRB_* bits
     unsigned long long* pairs;   // per cloud: sum over passes of n_all * ns
     int32_t* ctr;                // CTR_* counters
+    int32_t* act_cloud;          // evolving clouds, in cloud order (n_clouds)
+    int32_t* act_pre;            // 3 x (n_clouds+1) exclusive prefixes of their work items
+    int32_t* group_conv;         // per group: members converged in this round
+    int32_t* ready;              // groups ready for decimation (n_groups)
     // decimation scratch, per group (offsets in GroupDesc / dec_hoff)
     float* dx;                   // coordinates of the group's chosen points
     int32_t* dcell;              // their grid cells
@@ -77,6 +88,8 @@ struct EngineView {
     int32_t max_passes;
     int32_t max_outer;
     int32_t max_iters;
+    int32_t n_sms;
+    int32_t flags;               // ENG_* run-mode bits
 };
 
 // launch configuration picked by the tuner per (dim, cloud size) bucket
@@ -96,9 +109,17 @@ cudaError_t prepare_pass(int dim, const EngineView& v, const TuneParams& tp);
 // a0/a1 (optional) are recorded on `st` right before and after the assign kernel
 cudaError_t launch_pass(int dim, const EngineView& v, const TuneParams& tp, int assign_grid,
                         cudaStream_t st, cudaEvent_t a0 = nullptr, cudaEvent_t a1 = nullptr);
+// Sets the loop condition and rebuilds the work lists of the next iteration
+// (count_iter = 0 for the initial build before the first iteration).
 cudaError_t launch_loopcond(const EngineView& v, cudaGraphConditionalHandle h, int use_handle,
-                            cudaStream_t st);
+                            cudaStream_t st, int count_iter = 1);
 cudaError_t launch_reset(const EngineView& v, cudaStream_t st);
+// phases from the chosen counts already in v.ns (evolve or decimate from a given set)
+cudaError_t launch_set_given(const EngineView& v, int queue_decimation, cudaStream_t st);
+cudaError_t launch_decimate(int dim, const EngineView& v, cudaStream_t st);
+// the five kernels of one evolve pass without control/decimation (adjoint forward)
+cudaError_t launch_evolve_step(int dim, const EngineView& v, const TuneParams& tp, int assign_grid,
+                               cudaStream_t st);
 int assign_smem_bytes(int dim, const TuneParams& tp, int hist_ints);
 int max_assign_blocks_per_sm(int dim, const TuneParams& tp, int hist_ints);
 bool tune_supported(int dim, const TuneParams& tp);

@@ -48,10 +48,26 @@ public:
     int64_t total_points() const { return total_points_; }
     int dim() const { return dim_; }
 
-    // choose -> (evolve -> decimate)* on `st`.  use_graph selects the CUDA
-    // graph WHILE loop; otherwise the host reads the loop flag after each
-    // iteration (the reference's style).  Blocks until the run is complete.
-    int run(cudaStream_t st, bool use_graph);
+    enum RunMode {
+        RUN_FULL = 0,           // choose -> (evolve -> decimate)* to convergence
+        RUN_CHOOSE_ONLY = 1,    // choose only
+        RUN_EVOLVE_ONLY = 2,    // evolve the given chosen sets to convergence
+        RUN_DECIMATE_ONLY = 3,  // one decimation of the given chosen sets
+    };
+    // Runs on `st`.  use_graph selects the CUDA-graph WHILE loop; otherwise the
+    // host reads the loop flag after each iteration (the reference's style).
+    // For RUN_EVOLVE_ONLY / RUN_DECIMATE_ONLY the caller first writes each
+    // cloud's chosen points at its s_off in chosen_mut() and their counts into
+    // given_ns.  Blocks until the run is complete.
+    int run(cudaStream_t st, bool use_graph, int mode = RUN_FULL);
+    float* chosen_mut() { return bS_.as<float>(); }
+    std::vector<int32_t> given_ns;
+    // the adjoint's forward step: assign + ordered mean of one pass, no
+    // movement test (rd_adjoint.cu); keys()/counts() then hold that pass
+    int adjoint_setup(cudaStream_t st);
+    int adjoint_step(cudaStream_t st);
+    const int32_t* keys() const { return bKeys_.as<int32_t>(); }
+    const int32_t* counts() const { return bCnt_.as<int32_t>(); }
 
     // results, valid after run(): per-cloud chosen count and device pointer
     const std::vector<int32_t>& ns() const { return h_ns_; }
@@ -70,6 +86,8 @@ public:
 
 private:
     int finish_setup_after_choose(cudaStream_t st);
+    int collect(cudaStream_t st);
+    int flags_ = 0;
     int build_graph(cudaStream_t st);
     EngineView view() const;
     int fail(const char* what, cudaError_t e);
@@ -93,6 +111,7 @@ private:
     DevBuf bCl_, bGr_, bChunkCloud_, bSlotCloud_, bSegList_;
     DevBuf bP_, bS_, bKeys_, bGrouped_, bHist_, bSegsum_, bCnt_, bBase_, bNext_, bHash_, bSurv_;
     DevBuf bNs_, bPhase_, bCont_, bPasses_, bTotPasses_, bOuter_, bErr_, bPairs_, bCtr_;
+    DevBuf bActCloud_, bActPre_, bGroupConv_, bReady_;
     DevBuf bDx_, bDcell_, bDalive_, bDc1_, bDc2_, bDbstart_, bDitems_, bDecHoff_, bDecHbits_;
 
     cudaStream_t cap_stream_ = nullptr;

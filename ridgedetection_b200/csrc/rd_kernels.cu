@@ -38,6 +38,38 @@ __device__ __forceinline__ uint32_t cell_hash(const int* c)
     return h ^ (h >> 15);
 }
 
+// Work lists over the clouds still evolving, rebuilt by k_loopcond after every
+// iteration: act_cloud[a] is the a-th evolving cloud and act_pre[kind] the
+// exclusive prefix of its work items (chunks, histogram segments or chosen
+// slots), so kernels launched over fixed grids touch only active work.
+enum : int { ACT_CHUNK = 0, ACT_SEG = 1, ACT_SLOT = 2, ACT_KINDS = 3 };
+
+struct ActiveList {
+    const int32_t* pre;
+    const int32_t* cloud;
+    int nact;
+    int total;
+    __device__ ActiveList(const EngineView& v, int kind)
+    {
+        nact = v.ctr[CTR_NACT];
+        pre = v.act_pre + (int64_t)kind * (v.n_clouds + 1);
+        cloud = v.act_cloud;
+        total = pre[nact];
+    }
+    // item t < total -> (cloud, item index inside that cloud)
+    __device__ __forceinline__ void locate(int t, int& c, int& local) const
+    {
+        int lo = 0, hi = nact - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (pre[mid] <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        c = cloud[lo];
+        local = t - pre[lo];
+    }
+};
+
 // offset o in [0, 3^DIM) -> neighbour cell; o == (3^DIM-1)/2 is the home cell
 template <int DIM>
 __device__ __forceinline__ void neighbour_cell(const int* cc, int o, int* out)
@@ -377,16 +409,16 @@ __global__ void __launch_bounds__(BLOCK) k_assign(EngineView v)
     extern __shared__ int s_hist[];
     const int tid = threadIdx.x;
 
+    const ActiveList al(v, ACT_CHUNK);
     for (;;) {
         if (tid == 0) s_item = atomicAdd(&v.ctr[CTR_WORK], 1);
         __syncthreads();
         const int item = s_item;
         __syncthreads();
-        if (item >= v.n_chunks) break;
-        const int c = v.chunk_cloud[item];
-        if (v.phase[c] != PH_EVOLVE) continue;
+        if (item >= al.total) break;
+        int c, lc;
+        al.locate(item, c, lc);
         const CloudDesc cd = v.cl[c];
-        const int lc = item - (int)cd.chunk_begin;
         // chunks split the cloud evenly (at most BLOCK*ITEMS points each)
         const int start = (int)(((int64_t)lc * cd.n_all) / cd.n_chunks);
         const int n = (int)(((int64_t)(lc + 1) * cd.n_all) / cd.n_chunks);  // chunk end
@@ -461,11 +493,10 @@ __global__ void __launch_bounds__(BLOCK) k_assign(EngineView v)
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_colscan(EngineView v)
 {
-    const int item = blockIdx.x;
-    if (item >= v.n_segs) return;
-    const int2 cs = v.seg_list[item];
-    const int c = cs.x, seg = cs.y;
-    if (v.phase[c] != PH_EVOLVE) return;
+    const ActiveList al(v, ACT_SEG);
+    for (int item = blockIdx.x; item < al.total; item += gridDim.x) {
+    int c, seg;
+    al.locate(item, c, seg);
     const CloudDesc cd = v.cl[c];
     const int ns = v.ns[c];
     const int r0 = seg * SEG;
@@ -484,6 +515,7 @@ __global__ void __launch_bounds__(256) k_colscan(EngineView v)
         }
         out[k] = run;
     }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -492,10 +524,24 @@ __global__ void __launch_bounds__(256) k_colscan(EngineView v)
 // prefix of the counts over keys (first grouped slot of each key).
 // ---------------------------------------------------------------------------
 template <int BLOCK>
+__device__ void segscan_one(const EngineView& v, int c, int* s_w, int* s_carry_p);
+
+template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_segscan(EngineView v)
 {
-    const int c = blockIdx.x;
-    if (v.phase[c] != PH_EVOLVE) return;
+    __shared__ int s_w[BLOCK / 32];
+    __shared__ int s_carry;
+    const int nact = v.ctr[CTR_NACT];
+    for (int a = blockIdx.x; a < nact; a += gridDim.x) {
+        __syncthreads();  // previous cloud's readers of s_w / s_carry are done
+        segscan_one<BLOCK>(v, v.act_cloud[a], s_w, &s_carry);
+    }
+}
+
+template <int BLOCK>
+__device__ void segscan_one(const EngineView& v, int c, int* s_w, int* s_carry_p)
+{
+    int& s_carry = *s_carry_p;
     const CloudDesc cd = v.cl[c];
     const int ns = v.ns[c];
     int32_t* sg = v.segsum + cd.seg_off;
@@ -517,8 +563,6 @@ __global__ void __launch_bounds__(BLOCK) k_segscan(EngineView v)
         cnt[k] = run;
     }
     __syncthreads();
-    __shared__ int s_w[BLOCK / 32];
-    __shared__ int s_carry;
     if (threadIdx.x == 0) s_carry = 0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int k0 = 0; k0 < ns; k0 += BLOCK) {
@@ -554,22 +598,29 @@ __global__ void __launch_bounds__(BLOCK) k_segscan(EngineView v)
 // only (match_any groups equal keys of 32 consecutive points, the group
 // leader advances the key's cursor).
 // ---------------------------------------------------------------------------
+__device__ void scatter_chunk(const EngineView& v, int c, int lc, int* s_keys, int lane);
+
 __global__ void __launch_bounds__(128) k_scatter(EngineView v)
 {
     extern __shared__ int s_dyn[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int item = blockIdx.x * 4 + warp;
-    if (item >= v.n_chunks) return;
-    const int c = v.chunk_cloud[item];
-    if (v.phase[c] != PH_EVOLVE) return;
+    const ActiveList al(v, ACT_CHUNK);
+    for (int item = blockIdx.x * 4 + warp; item < al.total; item += gridDim.x * 4) {
+        __syncwarp();
+        int c, lc;
+        al.locate(item, c, lc);
+        scatter_chunk(v, c, lc, s_dyn + warp * (v.chunk_max + v.scat_smem), lane);
+    }
+}
+
+__device__ void scatter_chunk(const EngineView& v, int c, int lc, int* s_keys, int lane)
+{
     const CloudDesc cd = v.cl[c];
     const int ns = v.ns[c];
-    const int lc = item - (int)cd.chunk_begin;
     const int seg = lc / SEG;
     int32_t* row = v.hist + cd.hist_off + (int64_t)lc * cd.ns_cap;
     const int32_t* sg = v.segsum + cd.seg_off + (int64_t)seg * cd.ns_cap;
     const int32_t* bs = v.base + cd.key_off;
-    int* s_keys = s_dyn + warp * (v.chunk_max + v.scat_smem);
     const bool in_smem = ns <= v.scat_smem;
     int32_t* ctr = in_smem ? (s_keys + v.chunk_max) : row;
     const int start = (int)(((int64_t)lc * cd.n_all) / cd.n_chunks);
@@ -605,52 +656,78 @@ __global__ void __launch_bounds__(128) k_scatter(EngineView v)
 // permutation written by k_scatter, BP at a time, the next block in flight
 // while the current one is folded.
 // ---------------------------------------------------------------------------
+constexpr int SUM_BP = 128;  // members staged per step of the ordered fold
+
+template <int DIM>
+__device__ void sum_shift_one(const EngineView& v, int c, int k, float* buf, int* sidx, int lane);
+
 template <int DIM>
 __global__ void __launch_bounds__(256) k_sum_shift(EngineView v)
 {
-    constexpr int BP = 128;             // members staged per step
-    constexpr int R = BP * DIM / 32;    // floats per lane per step
-    __shared__ float s_buf[8][BP * DIM];
-    __shared__ int s_idx[8][BP];
+    __shared__ float s_buf[8][SUM_BP * DIM];
+    __shared__ int s_idx[8][SUM_BP];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int g = blockIdx.x * 8 + warp;
-    if (g >= v.n_slots) return;
-    const int c = v.slot_cloud[g];
-    if (v.phase[c] != PH_EVOLVE) return;
+    const ActiveList al(v, ACT_SLOT);
+    for (int t = blockIdx.x * 8 + warp; t < al.total; t += gridDim.x * 8) {
+        __syncwarp();
+        int c, k;
+        al.locate(t, c, k);
+        sum_shift_one<DIM>(v, c, k, s_buf[warp], s_idx[warp], lane);
+    }
+}
+
+template <int DIM>
+__device__ void sum_shift_one(const EngineView& v, int c, int k, float* buf, int* sidx, int lane)
+{
+    constexpr int BP = SUM_BP;
+    constexpr int R = BP * DIM / 32;    // floats per lane per step
     const CloudDesc cd = v.cl[c];
-    const int k = g - (int)cd.key_off;
-    if (k >= v.ns[c]) return;
     const int n = v.cnt[cd.key_off + k];
     if (n == 0) return;
     const int32_t* perm = v.perm + cd.p_off + v.base[cd.key_off + k];
     const float* P = v.P + cd.p_off * DIM;
-    float* buf = s_buf[warp];
-    int* sidx = s_idx[warp];
     float nxt[R];
-    auto fetch = [&](int off) {
+    // Two-stage pipeline: member indices of block b+2 and coordinates of
+    // block b+1 are in flight while block b is folded.
+    int pnx[BP / 32];
+    auto load_perm = [&](int off) {
         const int m = min(BP, n - off);
 #pragma unroll
         for (int u = 0; u < BP / 32; ++u) {
             const int j = u * 32 + lane;
-            sidx[j] = (j < m) ? perm[off + j] : 0;
+            pnx[u] = (off < n && j < m) ? perm[off + j] : 0;
         }
-        __syncwarp();
+    };
+    auto load_coords = [&](int off) {  // indices of block `off` are in sidx
+        const int m = min(BP, n - off);
 #pragma unroll
         for (int u = 0; u < R; ++u) {
             const int e = u * 32 + lane;
             const int j = e / DIM, d = e - (e / DIM) * DIM;
             nxt[u] = (j < m) ? P[(int64_t)sidx[j] * DIM + d] : 0.0f;
         }
+    };
+    auto stage_perm = [&]() {
+#pragma unroll
+        for (int u = 0; u < BP / 32; ++u) sidx[u * 32 + lane] = pnx[u];
         __syncwarp();
     };
-    fetch(0);
+    load_perm(0);
+    stage_perm();
+    load_coords(0);
+    load_perm(BP);
     float sum = 0.0f;
     for (int off = 0; off < n; off += BP) {
         const int m = min(BP, n - off);
+        __syncwarp();  // every lane is done reading sidx of the previous stage
 #pragma unroll
         for (int u = 0; u < R; ++u) buf[u * 32 + lane] = nxt[u];
+        if (off + BP < n) {
+            stage_perm();               // indices of block off+BP
+            load_coords(off + BP);      // in flight during the fold
+            load_perm(off + 2 * BP);    // in flight during the fold
+        }
         __syncwarp();
-        if (off + BP < n) fetch(off + BP);  // next block in flight during the fold
         if (lane < DIM) {
             if (m == BP) {
 #pragma unroll 32
@@ -664,9 +741,13 @@ __global__ void __launch_bounds__(256) k_sum_shift(EngineView v)
     int moved = 0;
     if (lane < DIM) {
         float* s = v.S + (cd.s_off + k) * DIM + lane;
-        float cval = *s;
-        moved = shift_coord(sum, n, cval);
-        if (moved) *s = cval;
+        if (v.flags & ENG_ALWAYS_MOVE) {
+            *s = __fdiv_rn(sum, (float)n);  // mean, no movement test
+        } else {
+            float cval = *s;
+            moved = shift_coord(sum, n, cval);
+            if (moved) *s = cval;
+        }
     }
     if (__any_sync(FULL, moved) && lane == 0) v.cont[c] = 1;
 }
@@ -676,21 +757,31 @@ __global__ void __launch_bounds__(256) k_sum_shift(EngineView v)
 // ---------------------------------------------------------------------------
 __global__ void k_control(EngineView v)
 {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (blockIdx.x == 0 && threadIdx.x == 0) v.ctr[CTR_WORK] = 0;
-    if (c >= v.n_clouds) return;
-    if (v.phase[c] != PH_EVOLVE) return;
-    const CloudDesc cd = v.cl[c];
-    v.pairs[c] += (unsigned long long)cd.n_all * (unsigned long long)v.ns[c];
-    v.passes[c] += 1;
-    v.total_passes[c] += 1;
-    if (v.cont[c] == 0) {
-        v.phase[c] = PH_CONVERGED;
-    } else if (v.passes[c] >= v.max_passes) {
-        v.err[c] |= ERRB_EVOLVE_CAP;
-        v.phase[c] = PH_CONVERGED;
+    const int nact = v.ctr[CTR_NACT];
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nact; a += gridDim.x * blockDim.x) {
+        const int c = v.act_cloud[a];
+        const CloudDesc cd = v.cl[c];
+        v.pairs[c] += (unsigned long long)cd.n_all * (unsigned long long)v.ns[c];
+        v.passes[c] += 1;
+        v.total_passes[c] += 1;
+        bool conv = false;
+        if (v.cont[c] == 0) {
+            conv = true;
+        } else if (v.passes[c] >= v.max_passes) {
+            v.err[c] |= ERRB_EVOLVE_CAP;
+            conv = true;
+        }
+        v.cont[c] = 0;
+        if (conv && (v.flags & ENG_EVOLVE_ONLY)) {
+            v.phase[c] = PH_DONE;
+        } else if (conv) {
+            v.phase[c] = PH_CONVERGED;
+            // the last member of a group to converge queues the group
+            const GroupDesc gd = v.gr[cd.group];
+            if (atomicAdd(&v.group_conv[cd.group], 1) + 1 == gd.n_clouds)
+                v.ready[atomicAdd(&v.ctr[CTR_NREADY], 1)] = cd.group;
+        }
     }
-    v.cont[c] = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -702,24 +793,14 @@ __global__ void k_control(EngineView v)
 // a warp ballot skips runs of points that cannot be removed.
 // ---------------------------------------------------------------------------
 template <int DIM, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_decimate(EngineView v)
+__device__ void decimate_group(const EngineView& v, const int g)
 {
     constexpr int NB = Pow3<DIM>::v;
-    const int g = blockIdx.x;
     const GroupDesc gd = v.gr[g];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    __shared__ int s_flag, s_total, s_cnt;
+    __shared__ int s_cnt;
     __shared__ int s_off[33];
-    if (tid == 0) { s_flag = 0; s_total = 0; }
     __syncthreads();
-    // all members converged?  (any evolving -> wait; all done -> nothing to do)
-    for (int i = tid; i < gd.n_clouds; i += BLOCK) {
-        const int ph = v.phase[gd.cloud_begin + i];
-        if (ph == PH_EVOLVE) atomicOr(&s_flag, 1);
-        if (ph == PH_CONVERGED) atomicOr(&s_flag, 2);
-    }
-    __syncthreads();
-    if ((s_flag & 1) || !(s_flag & 2)) return;
 
     const CloudDesc c0 = v.cl[gd.cloud_begin];
     const float rsq = sqr_rn(c0.r2);
@@ -924,7 +1005,16 @@ __global__ void __launch_bounds__(BLOCK) k_decimate(EngineView v)
             v.phase[c] = PH_EVOLVE;
         }
     }
-    (void)s_total;
+    if (tid == 0) v.group_conv[g] = 0;
+    __syncthreads();
+}
+
+// one CTA per group queued by k_control in this iteration
+template <int DIM, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_decimate(EngineView v)
+{
+    const int nready = v.ctr[CTR_NREADY];
+    for (int r = blockIdx.x; r < nready; r += gridDim.x) decimate_group<DIM, BLOCK>(v, v.ready[r]);
 }
 
 // ---------------------------------------------------------------------------
@@ -932,17 +1022,76 @@ __global__ void __launch_bounds__(BLOCK) k_decimate(EngineView v)
 // mode) and/or leaves the count in ctr[CTR_ACTIVE] for the host (plain mode).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(1024) k_loopcond(EngineView v, cudaGraphConditionalHandle h,
-                                                   int use_handle)
+                                                   int use_handle, int count_iter)
 {
     __shared__ int s_act;
-    if (threadIdx.x == 0) s_act = 0;
+    __shared__ int s_w[32][4];
+    __shared__ int s_carry[4];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) {
+        s_act = 0;
+        s_carry[0] = s_carry[1] = s_carry[2] = s_carry[3] = 0;
+    }
     __syncthreads();
     int act = 0;
-    for (int c = threadIdx.x; c < v.n_clouds; c += blockDim.x) act += (v.phase[c] != PH_DONE);
+    for (int c = tid; c < v.n_clouds; c += blockDim.x) act += (v.phase[c] != PH_DONE);
     if (act) atomicAdd(&s_act, act);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const int it = v.ctr[CTR_ITERS] + 1;
+    // work lists of the next iteration: evolving clouds, prefixes of their
+    // chunks, histogram segments and chosen slots
+    const int nc = v.n_clouds;
+    for (int c0 = 0; c0 < nc; c0 += blockDim.x) {
+        const int c = c0 + tid;
+        const bool ev = (c < nc) && v.phase[c] == PH_EVOLVE;
+        int x[4];
+        x[0] = ev ? 1 : 0;
+        x[1] = ev ? v.cl[c].n_chunks : 0;
+        x[2] = ev ? v.cl[c].n_seg : 0;
+        x[3] = ev ? v.ns[c] : 0;
+        int incl[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            incl[q] = x[q];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(FULL, incl[q], o);
+                if (lane >= o) incl[q] += y;
+            }
+            if (lane == 31) s_w[warp][q] = incl[q];
+        }
+        __syncthreads();
+        int excl[4], tot[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            int pre = 0, t = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+                pre += (w < warp) ? s_w[w][q] : 0;
+                t += s_w[w][q];
+            }
+            excl[q] = s_carry[q] + pre + incl[q] - x[q];
+            tot[q] = t;
+        }
+        if (ev) {
+            v.act_cloud[excl[0]] = c;
+            v.act_pre[ACT_CHUNK * (nc + 1) + excl[0]] = excl[1];
+            v.act_pre[ACT_SEG * (nc + 1) + excl[0]] = excl[2];
+            v.act_pre[ACT_SLOT * (nc + 1) + excl[0]] = excl[3];
+        }
+        __syncthreads();
+        if (tid == 0) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) s_carry[q] += tot[q];
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        const int nact = s_carry[0];
+        v.act_pre[ACT_CHUNK * (nc + 1) + nact] = s_carry[1];
+        v.act_pre[ACT_SEG * (nc + 1) + nact] = s_carry[2];
+        v.act_pre[ACT_SLOT * (nc + 1) + nact] = s_carry[3];
+        v.ctr[CTR_NACT] = nact;
+        v.ctr[CTR_WORK] = 0;
+        v.ctr[CTR_NREADY] = 0;
+        const int it = v.ctr[CTR_ITERS] + (count_iter ? 1 : 0);
         v.ctr[CTR_ITERS] = it;
         int a = s_act;
         if (it >= v.max_iters && a > 0) {
@@ -954,10 +1103,27 @@ __global__ void __launch_bounds__(1024) k_loopcond(EngineView v, cudaGraphCondit
     }
 }
 
+// chosen counts are given in v.ns: evolving phase for non-empty clouds, or
+// (queue_decimation) converged phase with every group queued for decimation
+__global__ void k_set_given(EngineView v, int queue_decimation)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < v.n_clouds) {
+        if (queue_decimation) v.phase[c] = PH_CONVERGED;
+        else v.phase[c] = (v.ns[c] > 0) ? PH_EVOLVE : PH_DONE;
+    }
+    if (queue_decimation && c < v.n_groups) {
+        v.ready[c] = c;
+        v.group_conv[c] = v.gr[c].n_clouds;
+    }
+    if (c == 0) v.ctr[CTR_NREADY] = queue_decimation ? v.n_groups : 0;
+}
+
 __global__ void k_reset(EngineView v)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c < CTR_COUNT && blockIdx.x == 0) v.ctr[c] = 0;
+    if (c < v.n_groups) v.group_conv[c] = 0;
     if (c >= v.n_clouds) return;
     v.cont[c] = 0;
     v.passes[c] = 0;
@@ -1007,13 +1173,16 @@ cudaError_t launch_pass_dim(const EngineView& v, const TuneParams& tp, int assig
     { return cudaErrorInvalidValue; }
 #undef RD_ASSIGN_CASE
     if (a1) cudaEventRecord(a1, st);
-    if (v.n_segs > 0) k_colscan<<<v.n_segs, 256, 0, st>>>(v);
-    k_segscan<1024><<<v.n_clouds, 1024, 0, st>>>(v);
+    // fixed grids; every kernel walks only the current work lists
+    const int sms = v.n_sms;
+    if (v.n_segs > 0) k_colscan<<<std::min(v.n_segs, sms * 8), 256, 0, st>>>(v);
+    k_segscan<1024><<<std::min(v.n_clouds, sms * 2), 1024, 0, st>>>(v);
     if (v.n_chunks > 0)
-        k_scatter<<<(v.n_chunks + 3) / 4, 128, 4 * (v.chunk_max + v.scat_smem) * 4, st>>>(v);
-    if (v.n_slots > 0) k_sum_shift<DIM><<<(v.n_slots + 7) / 8, 256, 0, st>>>(v);
-    k_control<<<(v.n_clouds + 255) / 256, 256, 0, st>>>(v);
-    k_decimate<DIM, 512><<<v.n_groups, 512, 0, st>>>(v);
+        k_scatter<<<std::min((v.n_chunks + 3) / 4, sms * 8), 128,
+                    4 * (v.chunk_max + v.scat_smem) * 4, st>>>(v);
+    if (v.n_slots > 0) k_sum_shift<DIM><<<std::min((v.n_slots + 7) / 8, sms * 8), 256, 0, st>>>(v);
+    k_control<<<std::min((v.n_clouds + 255) / 256, sms), 256, 0, st>>>(v);
+    k_decimate<DIM, 512><<<std::min(v.n_groups, sms * 2), 512, 0, st>>>(v);
     return cudaGetLastError();
 }
 
@@ -1103,15 +1272,65 @@ cudaError_t launch_pass(int dim, const EngineView& v, const TuneParams& tp, int 
 }
 
 cudaError_t launch_loopcond(const EngineView& v, cudaGraphConditionalHandle h, int use_handle,
-                            cudaStream_t st)
+                            cudaStream_t st, int count_iter)
 {
-    k_loopcond<<<1, 1024, 0, st>>>(v, h, use_handle);
+    k_loopcond<<<1, 1024, 0, st>>>(v, h, use_handle, count_iter);
     return cudaGetLastError();
+}
+
+cudaError_t launch_set_given(const EngineView& v, int queue_decimation, cudaStream_t st)
+{
+    const int n = v.n_clouds > v.n_groups ? v.n_clouds : v.n_groups;
+    k_set_given<<<(n + 255) / 256, 256, 0, st>>>(v, queue_decimation);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_decimate(int dim, const EngineView& v, cudaStream_t st)
+{
+    const int grid = std::max(1, std::min(v.n_groups, v.n_sms * 2));
+    switch (dim) {
+        case 2: k_decimate<2, 512><<<grid, 512, 0, st>>>(v); break;
+        case 3: k_decimate<3, 512><<<grid, 512, 0, st>>>(v); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <int DIM>
+cudaError_t launch_evolve_step_dim(const EngineView& v, const TuneParams& tp, int assign_grid,
+                                   cudaStream_t st)
+{
+    const int hist_bytes = v.hist_smem * 4;
+    const int sms = v.n_sms;
+#define RD_ASSIGN_CASE(B, I) \
+    if (tp.block == B && tp.items == I) k_assign<DIM, B, I><<<assign_grid, B, hist_bytes, st>>>(v); else
+    RD_ASSIGN_CASE(128, 8) RD_ASSIGN_CASE(128, 4) RD_ASSIGN_CASE(256, 4) RD_ASSIGN_CASE(256, 8)
+    RD_ASSIGN_CASE(128, 16)
+    { return cudaErrorInvalidValue; }
+#undef RD_ASSIGN_CASE
+    if (v.n_segs > 0) k_colscan<<<std::min(v.n_segs, sms * 8), 256, 0, st>>>(v);
+    k_segscan<1024><<<std::min(v.n_clouds, sms * 2), 1024, 0, st>>>(v);
+    if (v.n_chunks > 0)
+        k_scatter<<<std::min((v.n_chunks + 3) / 4, sms * 8), 128,
+                    4 * (v.chunk_max + v.scat_smem) * 4, st>>>(v);
+    if (v.n_slots > 0) k_sum_shift<DIM><<<std::min((v.n_slots + 7) / 8, sms * 8), 256, 0, st>>>(v);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_evolve_step(int dim, const EngineView& v, const TuneParams& tp, int assign_grid,
+                               cudaStream_t st)
+{
+    switch (dim) {
+        case 2: return launch_evolve_step_dim<2>(v, tp, assign_grid, st);
+        case 3: return launch_evolve_step_dim<3>(v, tp, assign_grid, st);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t launch_reset(const EngineView& v, cudaStream_t st)
 {
-    const int n = v.n_clouds > CTR_COUNT ? v.n_clouds : CTR_COUNT;
+    int n = v.n_clouds > CTR_COUNT ? v.n_clouds : CTR_COUNT;
+    n = n > v.n_groups ? n : v.n_groups;
     k_reset<<<(n + 255) / 256, 256, 0, st>>>(v);
     return cudaGetLastError();
 }
