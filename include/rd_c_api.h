@@ -160,6 +160,25 @@ RD_API rd_status rd_batch_get_stats(rd_batch* h, rd_run_stats* st);
 RD_API rd_status rd_batch_destroy(rd_batch* h);
 
 /* ---------------------------------------------------------------------------
+ * Device-level steps on caller-owned device buffers (packed ROW_MAJOR f32),
+ * replacing the reference's CUB-style device algorithms:
+ *   rd_choose    rd::gpu::DeviceChoose::choose      (rd/gpu/device/device_choose.cuh,
+ *                dispatch/dispatch_choose.cuh:41); CPU rd::choose (cpu/brute_force/choose.hpp:37)
+ *   rd_evolve    rd::gpu::DeviceEvolve::evolve      (rd/gpu/device/device_evolve.cuh:35-62);
+ *                CPU rd::evolve (cpu/brute_force/evolve.hpp:293)
+ *   rd_decimate  rd::gpu::DeviceDecimate::decimate  (rd/gpu/device/device_decimate.cuh);
+ *                CPU rd::decimate (cpu/brute_force/decimate.hpp:41)
+ * Each call blocks until its result is in place.  d_S must hold np (choose) or
+ * ns (evolve, decimate) points; counts are returned through host pointers.
+ * ------------------------------------------------------------------------- */
+RD_API rd_status rd_choose(int dim, const float* d_P, int64_t np, float r1, float* d_S,
+                           int64_t* ns_out, void* stream);
+RD_API rd_status rd_evolve(int dim, const float* d_P, int64_t np, float* d_S, int64_t ns,
+                           float r1, int64_t* passes_out, void* stream);
+RD_API rd_status rd_decimate(int dim, float* d_S, int64_t ns, float r2, int64_t* ns_out,
+                             void* stream);
+
+/* ---------------------------------------------------------------------------
  * Evolve adjoint (no reference counterpart; the reference is forward-only).
  * Forward: `iters` evolve passes from S0 (ns chosen points, usually copies of
  * cloud points) with the movement test off: each non-empty cluster's point

@@ -14,6 +14,7 @@
 
 using namespace rdb;
 
+
 namespace {
 
 thread_local std::string g_err;
@@ -458,6 +459,87 @@ rd_status rd_tiled_destroy(rd_tiled* h)
 }
 
 // ------------------------------------------------------------------------
+// device-level steps (one cloud, caller-owned device buffers)
+// ------------------------------------------------------------------------
+static rd_status one_cloud_engine(Engine& e, int dim, int64_t n_points, int64_t capacity, float r1,
+                                  float r2)
+{
+    CloudDesc cd;
+    std::memset(&cd, 0, sizeof(cd));
+    cd.n_all = (int32_t)n_points;
+    cd.n_own = (int32_t)capacity;
+    cd.r1 = r1;
+    cd.r2 = r2;
+    GroupDesc gd;
+    std::memset(&gd, 0, sizeof(gd));
+    gd.n_clouds = 1;
+    return from_engine(e.setup(dim, {cd}, {gd}, n_points), e);
+}
+
+rd_status rd_choose(int dim, const float* d_P, int64_t np, float r1, float* d_S, int64_t* ns_out,
+                    void* stream)
+{
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (!d_P || !d_S || !ns_out) return set_err(RD_ERR_ARG, "null argument");
+    if (np < 0 || np > INT32_MAX - 1024 || !(r1 > 0.0f)) return set_err(RD_ERR_ARG, "bad np or r1");
+    *ns_out = 0;
+    if (np == 0) return RD_OK;
+    thread_local Engine& e = *new Engine();  // never destroyed: no CUDA calls at exit
+    cudaStream_t st = (cudaStream_t)stream;
+    if (rd_status s = one_cloud_engine(e, dim, np, np, r1, r1)) return s;
+    CK_CUDA(cudaMemcpyAsync(e.points(), d_P, sizeof(float) * np * dim, cudaMemcpyDeviceToDevice, st));
+    if (int rc = e.run(st, false, Engine::RUN_CHOOSE_ONLY)) return from_engine(rc, e);
+    const int64_t ns = e.ns()[0];
+    CK_CUDA(cudaMemcpyAsync(d_S, e.chosen(), sizeof(float) * ns * dim, cudaMemcpyDeviceToDevice, st));
+    CK_CUDA(cudaStreamSynchronize(st));
+    *ns_out = ns;
+    return RD_OK;
+}
+
+rd_status rd_evolve(int dim, const float* d_P, int64_t np, float* d_S, int64_t ns, float r1,
+                    int64_t* passes_out, void* stream)
+{
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (!d_P || !d_S) return set_err(RD_ERR_ARG, "null argument");
+    if (np < 0 || np > INT32_MAX - 1024 || ns < 0 || ns > INT32_MAX - 1024 || !(r1 > 0.0f))
+        return set_err(RD_ERR_ARG, "bad sizes or r1");
+    if (passes_out) *passes_out = 0;
+    if (ns == 0) return RD_OK;
+    thread_local Engine& e = *new Engine();  // never destroyed: no CUDA calls at exit
+    cudaStream_t st = (cudaStream_t)stream;
+    if (rd_status s = one_cloud_engine(e, dim, np, std::max(np, ns), r1, r1)) return s;
+    if (np) CK_CUDA(cudaMemcpyAsync(e.points(), d_P, sizeof(float) * np * dim, cudaMemcpyDeviceToDevice, st));
+    CK_CUDA(cudaMemcpyAsync(e.chosen_mut(), d_S, sizeof(float) * ns * dim, cudaMemcpyDeviceToDevice, st));
+    e.given_ns.assign(1, (int32_t)ns);
+    const int rc = e.run(st, true, Engine::RUN_EVOLVE_ONLY);
+    if (rc && rc != RD_ERR_NOT_CONVERGED) return from_engine(rc, e);
+    CK_CUDA(cudaMemcpyAsync(d_S, e.chosen(), sizeof(float) * ns * dim, cudaMemcpyDeviceToDevice, st));
+    CK_CUDA(cudaStreamSynchronize(st));
+    if (passes_out) *passes_out = e.stats().total_passes;
+    return from_engine(rc, e);
+}
+
+rd_status rd_decimate(int dim, float* d_S, int64_t ns, float r2, int64_t* ns_out, void* stream)
+{
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (!d_S || !ns_out) return set_err(RD_ERR_ARG, "null argument");
+    if (ns < 0 || ns > INT32_MAX - 1024 || !(r2 > 0.0f)) return set_err(RD_ERR_ARG, "bad ns or r2");
+    *ns_out = ns;
+    if (ns == 0) return RD_OK;
+    thread_local Engine& e = *new Engine();  // never destroyed: no CUDA calls at exit
+    cudaStream_t st = (cudaStream_t)stream;
+    if (rd_status s = one_cloud_engine(e, dim, 0, ns, r2, r2)) return s;
+    CK_CUDA(cudaMemcpyAsync(e.chosen_mut(), d_S, sizeof(float) * ns * dim, cudaMemcpyDeviceToDevice, st));
+    e.given_ns.assign(1, (int32_t)ns);
+    if (int rc = e.run(st, false, Engine::RUN_DECIMATE_ONLY)) return from_engine(rc, e);
+    const int64_t left = e.ns()[0];
+    CK_CUDA(cudaMemcpyAsync(d_S, e.chosen(), sizeof(float) * left * dim, cudaMemcpyDeviceToDevice, st));
+    CK_CUDA(cudaStreamSynchronize(st));
+    *ns_out = left;
+    return RD_OK;
+}
+
+// ------------------------------------------------------------------------
 // evolve adjoint
 // ------------------------------------------------------------------------
 rd_status rd_evolve_adjoint(int dim, const float* P, int64_t np, const float* S0, int64_t ns,
@@ -471,8 +553,14 @@ rd_status rd_evolve_adjoint(int dim, const float* P, int64_t np, const float* S0
         return set_err(RD_ERR_ARG, "np/ns out of range");
     if (iters < 0 || checkpoint_every < 0) return set_err(RD_ERR_ARG, "bad iteration counts");
     if (!(r1 > 0.0f)) return set_err(RD_ERR_ARG, "r1 must be > 0");
-    thread_local AdjointRunner runner;
-    thread_local DevBuf dP, dS0, dW, dSf, dgP, dgS;
+    // per-thread state, never destroyed: no CUDA calls during process exit
+    struct AdjState {
+        AdjointRunner runner;
+        DevBuf dP, dS0, dW, dSf, dgP, dgS;
+    };
+    thread_local AdjState& as = *new AdjState();
+    AdjointRunner& runner = as.runner;
+    DevBuf &dP = as.dP, &dS0 = as.dS0, &dW = as.dW, &dSf = as.dSf, &dgP = as.dgP, &dgS = as.dgS;
     cudaStream_t st = (cudaStream_t)stream;
     const float* pP = P;
     const float* pS0 = S0;
