@@ -53,3 +53,20 @@ def test_argument_errors_need_no_gpu():
     assert lib.rd_batch_run(None, None, 0, None, 0, 0, None) == L.RD_ERR_ARG
     assert lib.rd_abi_version() == 1
     assert lib.rd_supported_dims() & (1 << 2) and lib.rd_supported_dims() & (1 << 3)
+
+
+def test_cpp_facade_compiles_and_links(tmp_path):
+    """include/rd_b200.hpp (the reference-shaped C++ classes) builds against
+    librd_b200.so; nothing is run."""
+    import shutil
+    import subprocess
+    cxx = shutil.which("g++")
+    if cxx is None:
+        pytest.skip("no g++")
+    out = tmp_path / "facade"
+    cmd = [cxx, "-std=c++14", "-I" + os.path.join(ROOT, "include"), "-I/usr/local/cuda/include",
+           os.path.join(ROOT, "tests", "cpp", "facade_compile.cpp"),
+           "-L" + os.path.dirname(L.LIB_PATH), "-lrd_b200", "-L/usr/local/cuda/lib64", "-lcudart",
+           "-o", str(out)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
