@@ -179,6 +179,29 @@ RD_API rd_status rd_decimate(int dim, float* d_S, int64_t ns, float r2, int64_t*
                              void* stream);
 
 /* ---------------------------------------------------------------------------
+ * rd_decimate_noalloc: the decimation of rd_decimate without any device
+ * allocation.  It has no counterpart in the reference.  It exists for callers
+ * that cannot call cudaMalloc: code running while a CUDA graph is captured,
+ * hosts that forbid allocation after start-up, plugins whose device memory
+ * belongs to a framework that gives them no workspace.
+ *   - Scratch is one fixed __device__ array of RD_DECIMATE_NOALLOC_SCRATCH_BYTES
+ *     inside the library; every GPU that loads the library holds it until the
+ *     process exits.  ns above RD_DECIMATE_NOALLOC_MAX_POINTS is rejected with
+ *     RD_ERR_CAPACITY (use rd_decimate instead).
+ *   - The first call on a device looks up the array's device address (with that
+ *     device current); make that first call before any stream capture.
+ *   - All calls share the array: calls whose kernels overlap on the GPU race.
+ *     Serialize them (one stream, or events).
+ *   - d_S (ns points, packed ROW_MAJOR, device) is decimated in place; the
+ *     surviving count is written to the device int *d_ns_out (-1 on an internal
+ *     error).  The call is asynchronous on `stream` and performs no host sync.
+ * ------------------------------------------------------------------------- */
+#define RD_DECIMATE_NOALLOC_MAX_POINTS 32768
+#define RD_DECIMATE_NOALLOC_SCRATCH_BYTES (1536 * 1024)
+RD_API rd_status rd_decimate_noalloc(int dim, float* d_S, int64_t ns, float r2,
+                                     int32_t* d_ns_out, void* stream);
+
+/* ---------------------------------------------------------------------------
  * Evolve adjoint (no reference counterpart; the reference is forward-only).
  * Forward: `iters` evolve passes from S0 (ns chosen points, usually copies of
  * cloud points) with the movement test off: each non-empty cluster's point

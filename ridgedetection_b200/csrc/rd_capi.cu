@@ -14,6 +14,10 @@
 
 using namespace rdb;
 
+namespace rdb {
+int decimate_noalloc(int dim, float* d_S, int64_t ns, float r2, int32_t* d_ns_out, cudaStream_t st);
+extern const char* noalloc_error_message;
+}  // namespace rdb
 
 namespace {
 
@@ -536,6 +540,14 @@ rd_status rd_decimate(int dim, float* d_S, int64_t ns, float r2, int64_t* ns_out
     CK_CUDA(cudaMemcpyAsync(d_S, e.chosen(), sizeof(float) * left * dim, cudaMemcpyDeviceToDevice, st));
     CK_CUDA(cudaStreamSynchronize(st));
     *ns_out = left;
+    return RD_OK;
+}
+
+rd_status rd_decimate_noalloc(int dim, float* d_S, int64_t ns, float r2, int32_t* d_ns_out,
+                              void* stream)
+{
+    const int rc = rdb::decimate_noalloc(dim, d_S, ns, r2, d_ns_out, (cudaStream_t)stream);
+    if (rc) return set_err((rd_status)rc, rdb::noalloc_error_message ? rdb::noalloc_error_message : "");
     return RD_OK;
 }
 
