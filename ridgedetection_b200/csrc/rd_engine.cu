@@ -116,6 +116,8 @@ int Engine::setup(int dim, const std::vector<CloudDesc>& clouds,
     RD_CK(bActPre_.ensure(4 * 3 * (nc + 1)));
     RD_CK(bGroupConv_.ensure(4 * (h_gr_.size() + 1)));
     RD_CK(bReady_.ensure(4 * (h_gr_.size() + 1)));
+    RD_CK(bDbig_.ensure(4 * 4));
+    RD_CK(bDcpre_.ensure(4 * (nc + 1)));
     return 0;
 }
 
@@ -158,6 +160,11 @@ EngineView Engine::view() const
     v.dc2 = bDc2_.as<int32_t>();
     v.dbstart = bDbstart_.as<int32_t>();
     v.ditems = bDitems_.as<int32_t>();
+    v.dnb_off = bDnbOff_.as<int32_t>();
+    v.dnb = bDnb_.as<int32_t>();
+    v.dbig = bDbig_.as<int32_t>();
+    v.dcpre = bDcpre_.as<int32_t>();
+    v.dec_smem_max = dec_smem_max_;
     v.dec_hoff = bDecHoff_.as<int64_t>();
     v.dec_hbits = bDecHbits_.as<int32_t>();
     v.n_clouds = (int32_t)h_cl_.size();
@@ -213,13 +220,14 @@ int Engine::finish_setup_after_choose(cudaStream_t st)
     // group decimation scratch
     h_dec_hoff_.resize(h_gr_.size());
     h_dec_hbits_.resize(h_gr_.size());
-    int64_t sscr = 0, hoff = 0;
+    int64_t sscr = 0, hoff = 0, max_tot = 0;
     for (size_t g = 0; g < h_gr_.size(); ++g) {
         GroupDesc& gd = h_gr_[g];
         int64_t tot = 0;
         for (int i = 0; i < gd.n_clouds; ++i) tot += h_cl_[gd.cloud_begin + i].ns_cap;
         gd.s_scratch = sscr;
         sscr += tot;
+        max_tot = std::max(max_tot, tot);
         const int hb = std::min(20, std::max(6, ceil_log2(std::max<int64_t>(tot, 1))));
         h_dec_hbits_[g] = hb;
         h_dec_hoff_[g] = hoff;
@@ -245,6 +253,9 @@ int Engine::finish_setup_after_choose(cudaStream_t st)
     RD_CK(bDc2_.ensure(4 * (size_t)(sscr + 1)));
     RD_CK(bDitems_.ensure(4 * (size_t)(sscr + 1)));
     RD_CK(bDbstart_.ensure(4 * (size_t)(hoff + 1)));
+    RD_CK(bDnbOff_.ensure(4 * (size_t)(sscr + h_gr_.size() + 1)));
+    RD_CK(bDnb_.ensure(4 * (size_t)(DEC_NB_PER_POINT * sscr + 1)));
+    dec_smem_max_ = (int)std::min<int64_t>(max_tot, DEC_SMEM_MAX_POINTS);
     // persistent assignment grid: every resident CTA slot, at most one per chunk
     int dev = 0, sms = 0;
     RD_CK(cudaGetDevice(&dev));
@@ -258,10 +269,12 @@ int Engine::build_graph(cudaStream_t st)
 {
     (void)st;
     const EngineView v = view();
-    std::vector<unsigned char> key(sizeof(v) + sizeof(TuneParams) + sizeof(int));
+    std::vector<unsigned char> key(sizeof(v) + sizeof(TuneParams) + 2 * sizeof(int));
+    const int fz = fused_ ? 1 : 0;
     std::memcpy(key.data(), &v, sizeof(v));
     std::memcpy(key.data() + sizeof(v), &tune, sizeof(TuneParams));
     std::memcpy(key.data() + sizeof(v) + sizeof(TuneParams), &assign_grid_, sizeof(int));
+    std::memcpy(key.data() + sizeof(v) + sizeof(TuneParams) + sizeof(int), &fz, sizeof(int));
     if (exec_ && key == graph_key_) return 0;
     if (exec_) { cudaGraphExecDestroy(exec_); exec_ = nullptr; }
     if (graph_) { cudaGraphDestroy(graph_); graph_ = nullptr; }
@@ -281,7 +294,8 @@ int Engine::build_graph(cudaStream_t st)
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     RD_CK(cudaStreamBeginCaptureToGraph(cap_stream_, body, nullptr, nullptr, 0,
                                         cudaStreamCaptureModeThreadLocal));
-    cudaError_t e1 = launch_pass(dim_, v, tune, assign_grid_, cap_stream_);
+    cudaError_t e1 = fused_ ? launch_tile_pass(dim_, v, cap_stream_)
+                            : launch_pass(dim_, v, tune, assign_grid_, cap_stream_);
     cudaError_t e2 = launch_loopcond(v, h, 1, cap_stream_);
     cudaGraph_t out = nullptr;
     cudaError_t e3 = cudaStreamEndCapture(cap_stream_, &out);
@@ -345,8 +359,16 @@ int Engine::run(cudaStream_t st, bool use_graph, int mode)
         }
         if (int rc = finish_setup_after_choose(st)) return rc;
     }
+    // Tiled runs (one group of many clouds, every chosen set small enough)
+    // evolve each tile to convergence inside one kernel; everything else runs
+    // lockstep passes over all evolving clouds.
+    int max_ns = 0;
+    for (const CloudDesc& cd : h_cl_) max_ns = std::max(max_ns, cd.ns_cap);
+    fused_ = fuse_tiles && h_gr_.size() == 1 && h_cl_.size() > 1 && max_ns <= TILE_NS_MAX &&
+             flags_ == 0 && !profile_assign;
     const EngineView v = view();
     RD_CK(prepare_pass(dim_, v, tune));
+    if (fused_) RD_CK(prepare_tile_pass(dim_, v));
     // work lists of the first iteration
     RD_CK(launch_loopcond(v, cudaGraphConditionalHandle(), 0, st, 0));
     if (use_graph) {
@@ -361,7 +383,8 @@ int Engine::run(cudaStream_t st, bool use_graph, int mode)
         stats_.assign_ms = 0;
         stats_.assign_launches = 0;
         for (;;) {
-            RD_CK(launch_pass(dim_, v, tune, assign_grid_, st, a0, a1));
+            if (fused_) RD_CK(launch_tile_pass(dim_, v, st));
+            else RD_CK(launch_pass(dim_, v, tune, assign_grid_, st, a0, a1));
             RD_CK(launch_loopcond(v, cudaGraphConditionalHandle(), 0, st));
             int32_t act = 0;
             RD_CK(cudaMemcpyAsync(&act, v.ctr + CTR_ACTIVE, 4, cudaMemcpyDeviceToHost, st));

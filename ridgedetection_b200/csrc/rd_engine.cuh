@@ -27,6 +27,13 @@ enum : int {
     ENG_ALWAYS_MOVE = 2,   // adjoint forward: every non-empty cluster moves to its mean
 };
 
+// neighbour-list capacity of the decimation, per chosen point (lists that do
+// not fit fall back to walking the hash buckets)
+constexpr int DEC_NB_PER_POINT = 32;
+constexpr int DEC_SMEM_MAX_POINTS = 40960;
+// fused per-tile evolve: chosen points per tile it can hold
+constexpr int TILE_NS_MAX = 1024;
+
 enum : int {
     CTR_WORK = 0,      // assignment work ticket
     CTR_ACTIVE = 1,    // unfinished clouds after the last control step
@@ -74,6 +81,11 @@ struct EngineView {
     int32_t* dc2;                // alive neighbours within 2*r2 (self included)
     int32_t* dbstart;            // bucket starts (HB+1 per group)
     int32_t* ditems;             // bucket members
+    int32_t* dnb_off;            // per group: neighbour-list offsets (total+1)
+    int32_t* dnb;                // per group: neighbour lists, DEC_NB_PER_POINT per point
+    int32_t* dbig;               // GPU-wide prepared decimation: {state, group, total}
+    int32_t* dcpre;              // its members' chosen-count prefix (n_clouds+1)
+    int32_t dec_smem_max;       // points whose counts fit the decimation's shared memory
     const int64_t* dec_hoff;     // per group: start of its bucket arrays
     const int32_t* dec_hbits;    // per group: log2 buckets
     int32_t n_clouds;
@@ -91,6 +103,13 @@ struct EngineView {
     int32_t n_sms;
     int32_t flags;               // ENG_* run-mode bits
 };
+
+// dynamic shared memory of the decimation kernel: two int16 counts and an
+// alive byte per point, then a candidate bit per point
+inline int dec_smem_bytes(const EngineView& v)
+{
+    return ((v.dec_smem_max * 5 + 15) / 16) * 16 + 4 * ((v.dec_smem_max + 31) / 32) + 16;
+}
 
 // launch configuration picked by the tuner per (dim, cloud size) bucket
 struct TuneParams {
@@ -116,6 +135,10 @@ cudaError_t launch_loopcond(const EngineView& v, cudaGraphConditionalHandle h, i
 cudaError_t launch_reset(const EngineView& v, cudaStream_t st);
 // phases from the chosen counts already in v.ns (evolve or decimate from a given set)
 cudaError_t launch_set_given(const EngineView& v, int queue_decimation, cudaStream_t st);
+// fused per-tile evolve (every active cloud to convergence, one CTA each) +
+// decimation of the groups that became ready; needs every ns <= TILE_NS_MAX
+cudaError_t prepare_tile_pass(int dim, const EngineView& v);
+cudaError_t launch_tile_pass(int dim, const EngineView& v, cudaStream_t st);
 cudaError_t launch_decimate(int dim, const EngineView& v, cudaStream_t st);
 // the five kernels of one evolve pass without control/decimation (adjoint forward)
 cudaError_t launch_evolve_step(int dim, const EngineView& v, const TuneParams& tp, int assign_grid,

@@ -82,6 +82,7 @@ public:
     int max_iters = 1 << 18;
     TuneParams tune{128, 8};
     bool profile_assign = false;  // host loop only: time every assign launch with events
+    bool fuse_tiles = true;       // tiled runs: per-tile evolve kernel (see run())
     std::string last_error;
 
 private:
@@ -111,7 +112,9 @@ private:
     DevBuf bCl_, bGr_, bChunkCloud_, bSlotCloud_, bSegList_;
     DevBuf bP_, bS_, bKeys_, bGrouped_, bHist_, bSegsum_, bCnt_, bBase_, bNext_, bHash_, bSurv_;
     DevBuf bNs_, bPhase_, bCont_, bPasses_, bTotPasses_, bOuter_, bErr_, bPairs_, bCtr_;
-    DevBuf bActCloud_, bActPre_, bGroupConv_, bReady_;
+    DevBuf bActCloud_, bActPre_, bGroupConv_, bReady_, bDnbOff_, bDnb_, bDbig_, bDcpre_;
+    int dec_smem_max_ = 0;
+    bool fused_ = false;
     DevBuf bDx_, bDcell_, bDalive_, bDc1_, bDc2_, bDbstart_, bDitems_, bDecHoff_, bDecHbits_;
 
     cudaStream_t cap_stream_ = nullptr;

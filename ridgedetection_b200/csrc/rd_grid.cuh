@@ -192,5 +192,296 @@ __device__ void decimate_scan(const float* X, const int total, const float r2, c
     __syncthreads();
 }
 
+
+// Visits every point q != i within 2*r2 of point i of X (bucketed by the
+// counting sort in items/bstart, cells in cell): f(q, within_r2).
+template <int DIM, class F>
+__device__ __forceinline__ void dec_for_neighbours(const int i, const float* X,
+                                                   const int32_t* cell, const int32_t* items,
+                                                   const int32_t* bstart, const uint32_t hmask,
+                                                   const float rsq, const float rsq4, F&& f)
+{
+    constexpr int NB = Pow3<DIM>::v;
+    float p[DIM];
+    int cc[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        p[d] = X[(int64_t)i * DIM + d];
+        cc[d] = cell[(int64_t)i * DIM + d];
+    }
+    for (int o = 0; o < NB; ++o) {
+        int nc[DIM];
+        neighbour_cell<DIM>(cc, o, nc);
+        const uint32_t b = cell_hash<DIM>(nc) & hmask;
+        const int lo = (b == 0) ? 0 : bstart[b - 1];
+        const int hi = bstart[b];
+        for (int t = lo; t < hi; ++t) {
+            const int q = items[t];
+            if (q == i) continue;
+            bool same = true;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) same = same && (cell[(int64_t)q * DIM + d] == nc[d]);
+            if (!same) continue;
+            float s[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) s[d] = X[(int64_t)q * DIM + d];
+            const float sq = sqdist_exact<DIM>(p, s);
+            if (sq <= rsq4) f(q, sq <= rsq);
+        }
+    }
+}
+
+// Same decimation as decimate_scan, faster for large sets: every point's
+// neighbours within 2*r2 are listed once (CSR in nb_off/nb, the sign bit
+// marking "also within r2"), so a removal decrements its neighbours' counts
+// with one coalesced read of its list; counts and alive flags live in shared
+// memory (smem, 5 bytes per point) when total <= smem_max.  Falls back to
+// decimate_scan when the lists do not fit in nb_cap.  alive[] (global)
+// receives the survivors either way.
+template <int DIM, int BLOCK>
+__device__ void decimate_scan_lists(const float* X, const int total, const float r2,
+                                    const int nocopy, int32_t* cell, int32_t* alive, int32_t* c1g,
+                                    int32_t* c2g, int32_t* items, int32_t* bstart,
+                                    const uint32_t hmask, int32_t* nb_off, int32_t* nb,
+                                    const int64_t nb_cap, unsigned char* smem, const int smem_max,
+                                    int32_t* err, const int prepared = 0)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const float rsq = sqr_rn(r2);
+    const float rsq4 = __fmul_rn(4.0f, rsq);
+    const double inv = 1.0 / (2.0 * (double)r2 * (1.0 + 1.0 / 1024.0));
+    const bool in_smem = total <= smem_max;
+    int16_t* c1s = reinterpret_cast<int16_t*>(smem);
+    int16_t* c2s = c1s + smem_max;
+    unsigned char* as = reinterpret_cast<unsigned char*>(c2s + smem_max);
+    // candidate bitmap (alive and removable right now), 16-byte aligned after the flags
+    uint32_t* cand = reinterpret_cast<uint32_t*>(
+        smem + ((2 * sizeof(int16_t) * smem_max + smem_max + 15) / 16) * 16);
+    __shared__ int s_carry, s_overflow;
+    __shared__ int s_w[BLOCK / 32];
+
+    if (prepared) {  // buckets, counts and lists were built by the GPU-wide kernels
+        for (int i = tid; i < total; i += BLOCK) {
+            if (in_smem) {
+                c1s[i] = (int16_t)c1g[i];
+                c2s[i] = (int16_t)c2g[i];
+                as[i] = 1;
+            }
+            alive[i] = 1;
+        }
+        __syncthreads();
+    } else {
+    for (int h = tid; h <= (int)hmask + 1; h += BLOCK) bstart[h] = 0;
+    if (tid == 0) { s_carry = 0; s_overflow = 0; }
+    __syncthreads();
+    for (int i = tid; i < total; i += BLOCK) {
+        int cc[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            cc[d] = cell_of(X[(int64_t)i * DIM + d], inv);
+            cell[(int64_t)i * DIM + d] = cc[d];
+        }
+        atomicAdd(&bstart[(cell_hash<DIM>(cc) & hmask) + 1], 1);
+    }
+    __syncthreads();
+    if (warp == 0) {
+        int carry = 0;
+        for (int h0 = 0; h0 <= (int)hmask + 1; h0 += 32) {
+            const int h = h0 + lane;
+            int x = (h <= (int)hmask + 1) ? bstart[h] : 0;
+            int incl = x;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += y;
+            }
+            if (h <= (int)hmask + 1) bstart[h] = carry + incl;
+            carry += __shfl_sync(FULL, incl, 31);
+        }
+    }
+    __syncthreads();
+    for (int i = tid; i < total; i += BLOCK) {
+        int cc[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) cc[d] = cell[(int64_t)i * DIM + d];
+        const int slot = atomicAdd(&bstart[cell_hash<DIM>(cc) & hmask], 1);
+        items[slot] = i;
+    }
+    __syncthreads();
+    auto for_neighbours = [&](int i, auto&& f) {
+        dec_for_neighbours<DIM>(i, X, cell, items, bstart, hmask, rsq, rsq4, f);
+    };
+    // counts (self included) and list lengths
+    for (int i = tid; i < total; i += BLOCK) {
+        int n1 = 1, n2 = 1;
+        for_neighbours(i, [&](int, bool w1) { ++n2; n1 += w1; });
+        if (in_smem) {
+            c1s[i] = (int16_t)n1;
+            c2s[i] = (int16_t)n2;
+            as[i] = 1;
+        } else {
+            c1g[i] = n1;
+            c2g[i] = n2;
+        }
+        alive[i] = 1;
+        nb_off[i] = n2 - 1;
+    }
+    __syncthreads();
+    // exclusive prefix of list lengths
+    for (int i0 = 0; i0 < total; i0 += BLOCK) {
+        const int i = i0 + tid;
+        const int x = (i < total) ? nb_off[i] : 0;
+        int incl = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) s_w[warp] = incl;
+        __syncthreads();
+        int pre = 0, tot = 0;
+        for (int w = 0; w < BLOCK / 32; ++w) {
+            pre += (w < warp) ? s_w[w] : 0;
+            tot += s_w[w];
+        }
+        const int carry = s_carry;
+        if (i < total) nb_off[i] = carry + pre + incl - x;
+        __syncthreads();
+        if (tid == 0) s_carry = carry + tot;
+        __syncthreads();
+    }
+    if (tid == 0) {
+        nb_off[total] = s_carry;
+        s_overflow = (int64_t)s_carry > nb_cap;
+    }
+    __syncthreads();
+    if (s_overflow) {  // lists do not fit: bucket-walk version
+        decimate_scan<DIM, BLOCK>(X, total, r2, nocopy, cell, alive, c1g, c2g, items, bstart, hmask,
+                                  err);
+        return;
+    }
+    for (int i = tid; i < total; i += BLOCK) {
+        int k = nb_off[i];
+        for_neighbours(i, [&](int q, bool w1) { nb[k++] = w1 ? (q | (int)0x80000000) : q; });
+    }
+    __syncthreads();
+    }
+    if (in_smem) {
+        // Candidate bitmap: bit i set <=> point i is alive and removable now.
+        // The in-order scan then jumps from candidate to candidate; a removal
+        // re-evaluates exactly the neighbours whose counts it changed, so the
+        // bitmap stays exact and the scan visits what the sequential list
+        // walk of decimate.hpp would remove, in the same order.
+        const int nwords = (total + 31) >> 5;
+        for (int i0 = 0; i0 < nwords * 32; i0 += BLOCK) {
+            const int i = i0 + tid;
+            const bool q = (i < total) && (c1s[i] >= 4 || c2s[i] < 3);
+            const unsigned bal = __ballot_sync(FULL, q);
+            if (lane == 0 && (i >> 5) < nwords) cand[i >> 5] = bal;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            // first candidate >= pos, or -1
+            auto next_cand = [&](int pos) -> int {
+                int wi = pos >> 5;
+                if (wi >= nwords) return -1;
+                const uint32_t first = cand[wi] & (0xffffffffu << (pos & 31));
+                if (first) return (wi << 5) + __ffs(first) - 1;
+                for (int w0 = wi + 1; w0 < nwords; w0 += 32) {
+                    const int w = w0 + lane;
+                    const uint32_t word = (w < nwords) ? cand[w] : 0u;
+                    const unsigned bal = __ballot_sync(FULL, word != 0u);
+                    if (bal) {
+                        const int src = __ffs(bal) - 1;
+                        const uint32_t wb = __shfl_sync(FULL, word, src);
+                        return ((w0 + src) << 5) + __ffs(wb) - 1;
+                    }
+                }
+                return -1;
+            };
+            int cnt = total, left = -1, guard = 0;
+            bool stop = false;
+            while (left != cnt && cnt > 3 && !stop) {
+                if (++guard > total + 2) { if (lane == 0) atomicOr(err, ERRB_DEC_CAP); break; }
+                left = cnt;
+                int pos = 0;
+                for (;;) {
+                    const int j = next_cand(pos);
+                    if (j < 0) break;
+                    if (nocopy && cnt - 1 < 3) { stop = true; break; }
+                    if (lane == 0) {
+                        as[j] = 0;
+                        alive[j] = 0;
+                        atomicAnd(&cand[j >> 5], ~(1u << (j & 31)));
+                    }
+                    --cnt;
+                    const int e0 = nb_off[j], e1 = nb_off[j + 1];
+                    for (int t = e0 + lane; t < e1; t += 32) {  // distinct neighbours per lane
+                        const int e = nb[t];
+                        const int q = e & 0x7fffffff;
+                        const int a = (c1s[q] -= (e < 0) ? 1 : 0);
+                        const int b = (c2s[q] -= 1);
+                        const uint32_t bit = 1u << (q & 31);
+                        if (as[q] && (a >= 4 || b < 3)) atomicOr(&cand[q >> 5], bit);
+                        else atomicAnd(&cand[q >> 5], ~bit);
+                    }
+                    __syncwarp();
+                    if (!nocopy && cnt < 3) break;
+                    pos = j + 1;
+                }
+                if (!nocopy && cnt < 3) break;
+            }
+        }
+        __syncthreads();
+        return;
+    }
+    // sequential in-order scan (warp 0), as decimate_scan
+    if (warp == 0) {
+        auto get_alive = [&](int w) -> bool { return in_smem ? as[w] != 0 : alive[w] != 0; };
+        auto removable = [&](int w) -> bool {
+            const int a = in_smem ? c1s[w] : c1g[w];
+            const int b = in_smem ? c2s[w] : c2g[w];
+            return a >= 4 || b < 3;
+        };
+        int cnt = total, left = -1, guard = 0;
+        bool stop = false;
+        while (left != cnt && cnt > 3 && !stop) {
+            if (++guard > total + 2) { if (lane == 0) atomicOr(err, ERRB_DEC_CAP); break; }
+            left = cnt;
+            int i = 0;
+            while (i < total) {
+                const int w = i + lane;
+                const bool pred = (w < total) && get_alive(w) && removable(w);
+                const unsigned bal = __ballot_sync(FULL, pred);
+                if (bal == 0) { i += 32; continue; }
+                const int j = i + __ffs(bal) - 1;
+                if (nocopy && cnt - 1 < 3) { stop = true; break; }
+                if (lane == 0) {
+                    if (in_smem) as[j] = 0;
+                    alive[j] = 0;
+                }
+                --cnt;
+                const int e0 = nb_off[j], e1 = nb_off[j + 1];
+                for (int t = e0 + lane; t < e1; t += 32) {  // distinct neighbours per lane
+                    const int e = nb[t];
+                    const int q = e & 0x7fffffff;
+                    if (in_smem) {
+                        c2s[q] -= 1;
+                        if (e < 0) c1s[q] -= 1;
+                    } else {
+                        c2g[q] -= 1;
+                        if (e < 0) c1g[q] -= 1;
+                    }
+                }
+                __syncwarp();
+                if (!nocopy && cnt < 3) break;
+                i = j + 1;
+            }
+            if (!nocopy && cnt < 3) break;
+        }
+    }
+    __syncthreads();
+}
+
 }  // namespace
 }  // namespace rdb

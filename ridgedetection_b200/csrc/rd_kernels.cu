@@ -394,37 +394,48 @@ __global__ void __launch_bounds__(BLOCK) k_assign(EngineView v)
         const float* P = v.P + cd.p_off * DIM;
         const float* gS = v.S + cd.s_off * DIM;
 
+        // Two-level argmin.  The inner loop keeps only the running minimum
+        // (one min per pair instead of compare + two selects) and records the
+        // block of KB chosen points in which it last decreased; the exact
+        // index is then the first point of that block at exactly the minimum.
+        // Strict decrease per block and first match inside the block give the
+        // reference's rule: lowest index among equal minima.
+        constexpr int KB = 8;
+        constexpr float FAR = 1e30f;  // padding: (FAR - p)^2 overflows to +inf
         float p[ITEMS][DIM];
         float best[ITEMS];
-        int bi[ITEMS];
+        int blk[ITEMS];
 #pragma unroll
         for (int j = 0; j < ITEMS; ++j) {
             const int i = start + j * BLOCK + tid;
 #pragma unroll
             for (int d = 0; d < DIM; ++d) p[j][d] = (i < n) ? P[(int64_t)i * DIM + d] : 0.0f;
             best[j] = FLT_MAX;
-            bi[j] = -1;
+            blk[j] = -1;
         }
         for (int t0 = 0; t0 < ns; t0 += TS) {
             const int tl = min(TS, ns - t0);
+            const int tlp = (tl + KB - 1) / KB * KB;
             __syncthreads();
-            for (int e = tid; e < tl; e += BLOCK) {
+            for (int e = tid; e < tlp; e += BLOCK) {
 #pragma unroll
-                for (int d = 0; d < DIM; ++d) sS[e * DP + d] = gS[(int64_t)(t0 + e) * DIM + d];
+                for (int d = 0; d < DIM; ++d)
+                    sS[e * DP + d] = (e < tl) ? gS[(int64_t)(t0 + e) * DIM + d] : FAR;
             }
             __syncthreads();
-#pragma unroll 4
-            for (int kk = 0; kk < tl; ++kk) {
-                float s[DIM];
-                load_chosen<DIM>(sS, kk, s);
-                const int k = t0 + kk;
+            for (int kb = 0; kb < tlp; kb += KB) {
+                float old[ITEMS];
 #pragma unroll
-                for (int j = 0; j < ITEMS; ++j) {
-                    const float sq = sqdist_exact<DIM>(s, p[j]);
-                    const bool lt = sq < best[j];
-                    best[j] = lt ? sq : best[j];
-                    bi[j] = lt ? k : bi[j];
+                for (int j = 0; j < ITEMS; ++j) old[j] = best[j];
+#pragma unroll
+                for (int u = 0; u < KB; ++u) {
+                    float s[DIM];
+                    load_chosen<DIM>(sS, kb + u, s);
+#pragma unroll
+                    for (int j = 0; j < ITEMS; ++j) best[j] = fminf(best[j], sqdist_exact<DIM>(s, p[j]));
                 }
+#pragma unroll
+                for (int j = 0; j < ITEMS; ++j) blk[j] = (best[j] < old[j]) ? (t0 + kb) : blk[j];
             }
         }
         const float rsq = sqr_rn(cd.r1);
@@ -432,7 +443,18 @@ __global__ void __launch_bounds__(BLOCK) k_assign(EngineView v)
 #pragma unroll
         for (int j = 0; j < ITEMS; ++j) {
             const int i = start + j * BLOCK + tid;
-            key[j] = (i < n && best[j] <= rsq) ? bi[j] : -1;
+            int idx = -1;
+            if (i < n && best[j] <= rsq && blk[j] >= 0) {
+                for (int u = 0; u < KB; ++u) {
+                    const int k = blk[j] + u;
+                    if (k >= ns) break;
+                    float s[DIM];
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) s[d] = gS[(int64_t)k * DIM + d];
+                    if (sqdist_exact<DIM>(s, p[j]) == best[j]) { idx = k; break; }
+                }
+            }
+            key[j] = idx;
             if (i < n) v.keys[cd.p_off + i] = key[j];
         }
         // chunk histogram row (row length ns_cap, first ns entries used)
@@ -644,16 +666,14 @@ __global__ void __launch_bounds__(256) k_sum_shift(EngineView v)
     }
 }
 
+// Sequential FP32 fold, in list order, of the points P[perm[0..n)] (one warp;
+// the sum of coordinate d is returned in lane d < DIM).
 template <int DIM>
-__device__ void sum_shift_one(const EngineView& v, int c, int k, float* buf, int* sidx, int lane)
+__device__ float fold_members(const int32_t* __restrict__ perm, const int n,
+                              const float* __restrict__ P, float* buf, int* sidx, const int lane)
 {
     constexpr int BP = SUM_BP;
     constexpr int R = BP * DIM / 32;    // floats per lane per step
-    const CloudDesc cd = v.cl[c];
-    const int n = v.cnt[cd.key_off + k];
-    if (n == 0) return;
-    const int32_t* perm = v.perm + cd.p_off + v.base[cd.key_off + k];
-    const float* P = v.P + cd.p_off * DIM;
     float nxt[R];
     // Two-stage pipeline: member indices of block b+2 and coordinates of
     // block b+1 are in flight while block b is folded.
@@ -706,6 +726,17 @@ __device__ void sum_shift_one(const EngineView& v, int c, int k, float* buf, int
         }
         __syncwarp();
     }
+    return sum;
+}
+
+template <int DIM>
+__device__ void sum_shift_one(const EngineView& v, int c, int k, float* buf, int* sidx, int lane)
+{
+    const CloudDesc cd = v.cl[c];
+    const int n = v.cnt[cd.key_off + k];
+    if (n == 0) return;
+    const float sum = fold_members<DIM>(v.perm + cd.p_off + v.base[cd.key_off + k], n,
+                                        v.P + cd.p_off * DIM, buf, sidx, lane);
     int moved = 0;
     if (lane < DIM) {
         float* s = v.S + (cd.s_off + k) * DIM + lane;
@@ -718,6 +749,184 @@ __device__ void sum_shift_one(const EngineView& v, int c, int k, float* buf, int
         }
     }
     if (__any_sync(FULL, moved) && lane == 0) v.cont[c] = 1;
+}
+
+// ---------------------------------------------------------------------------
+// Fused per-tile evolve (tiled runs): one CTA evolves one tile to convergence
+// without leaving the kernel, so tiles proceed independently instead of in
+// lockstep passes.  Every pass is the same exact computation as the pass
+// pipeline (assign with the two-level argmin, stable grouping, index-order
+// fold, movement test), done inside the CTA:
+//   * warp w owns the contiguous point range [w n/W, (w+1) n/W); its per-key
+//     counts go to hist[w][key];
+//   * a key's members are laid out warp range by warp range, each range in
+//     index order (match_any ranks inside 32-point steps), i.e. in index order;
+//   * warp w folds keys w, w+W, ... (fold_members) and applies the shift.
+// Shared memory: chosen points (TILE_NS_MAX, padded to float4 for DIM 3),
+// W x (ns+1) counters, key bases.
+// ---------------------------------------------------------------------------
+template <int DIM, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_tile_evolve(EngineView v)
+{
+    constexpr int W = BLOCK / 32;
+    constexpr int DP = PadDim<DIM>::v;
+    constexpr int KB = 8;
+    constexpr float FAR = 1e30f;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float* sS = reinterpret_cast<float*>(smem_raw);                         // TILE_NS_MAX*DP
+    int* hist = reinterpret_cast<int*>(sS + TILE_NS_MAX * DP);             // W*(TILE_NS_MAX+1)
+    int* kbase = hist + W * (TILE_NS_MAX + 1);                              // TILE_NS_MAX+1
+    __shared__ float s_buf[W][SUM_BP * DIM];
+    __shared__ int s_idx[W][SUM_BP];
+    __shared__ int s_moved;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nact = v.ctr[CTR_NACT];
+    for (int a = blockIdx.x; a < nact; a += gridDim.x) {
+        const int c = v.act_cloud[a];
+        const CloudDesc cd = v.cl[c];
+        const int n = cd.n_all;
+        const int ns = v.ns[c];
+        const float* P = v.P + cd.p_off * DIM;
+        float* gS = v.S + cd.s_off * DIM;
+        int32_t* keys = v.keys + cd.p_off;
+        int32_t* perm = v.perm + cd.p_off;
+        const float rsq = sqr_rn(cd.r1);
+        const int nsp = (ns + KB - 1) / KB * KB;
+        __syncthreads();
+        for (int e = tid; e < nsp; e += BLOCK)
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) sS[e * DP + d] = (e < ns) ? gS[(int64_t)e * DIM + d] : FAR;
+        const int r0 = (int)(((int64_t)warp * n) / W), r1w = (int)(((int64_t)(warp + 1) * n) / W);
+        int pass = 0;
+        for (;;) {
+            // 1. assignment of the warp's range + per-warp key counts
+            for (int k = lane; k <= ns; k += 32) hist[warp * (TILE_NS_MAX + 1) + k] = 0;
+            __syncthreads();
+            for (int i0 = r0; i0 < r1w; i0 += 32) {
+                const int i = i0 + lane;
+                int key = -1;
+                if (i < r1w) {
+                    float p[DIM];
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) p[d] = P[(int64_t)i * DIM + d];
+                    float best = FLT_MAX;
+                    int blk = -1;
+                    for (int kb = 0; kb < nsp; kb += KB) {
+                        const float old = best;
+#pragma unroll
+                        for (int u = 0; u < KB; ++u) {
+                            float s[DIM];
+                            load_chosen<DIM>(sS, kb + u, s);
+                            best = fminf(best, sqdist_exact<DIM>(s, p));
+                        }
+                        blk = (best < old) ? kb : blk;
+                    }
+                    if (best <= rsq && blk >= 0) {
+                        for (int u = 0; u < KB && blk + u < ns; ++u) {
+                            float s[DIM];
+                            load_chosen<DIM>(sS, blk + u, s);
+                            if (sqdist_exact<DIM>(s, p) == best) { key = blk + u; break; }
+                        }
+                    }
+                    keys[i] = key;
+                    if (key >= 0) atomicAdd(&hist[warp * (TILE_NS_MAX + 1) + key], 1);
+                }
+            }
+            __syncthreads();
+            // 2. key bases and per-warp starts (thread per key)
+            for (int k = tid; k < ns; k += BLOCK) {
+                int tot = 0;
+                for (int w = 0; w < W; ++w) tot += hist[w * (TILE_NS_MAX + 1) + k];
+                kbase[k + 1] = tot;  // counts for the scan below
+            }
+            if (tid == 0) { kbase[0] = 0; s_moved = 0; }
+            __syncthreads();
+            if (warp == 0) {  // inclusive scan of counts -> kbase[k] = first slot of key k
+                int carry = 0;
+                for (int k0 = 0; k0 < ns; k0 += 32) {
+                    const int k = k0 + lane;
+                    const int x = (k < ns) ? kbase[k + 1] : 0;
+                    int incl = x;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int y = __shfl_up_sync(FULL, incl, o);
+                        if (lane >= o) incl += y;
+                    }
+                    if (k < ns) kbase[k + 1] = carry + incl;
+                    carry += __shfl_sync(FULL, incl, 31);
+                }
+            }
+            __syncthreads();
+            for (int k = tid; k < ns; k += BLOCK) {
+                int run = kbase[k];
+                for (int w = 0; w < W; ++w) {
+                    const int x = hist[w * (TILE_NS_MAX + 1) + k];
+                    hist[w * (TILE_NS_MAX + 1) + k] = run;
+                    run += x;
+                }
+            }
+            __syncthreads();
+            // 3. stable placement, warp range by warp range
+            int* cur = hist + warp * (TILE_NS_MAX + 1);
+            for (int i0 = r0; i0 < r1w; i0 += 32) {
+                const int i = i0 + lane;
+                const int key = (i < r1w) ? keys[i] : -1;
+                const unsigned m = __match_any_sync(FULL, key);
+                const int leader = __ffs(m) - 1;
+                int b = 0;
+                if (key >= 0 && lane == leader) {
+                    b = cur[key];
+                    cur[key] = b + __popc(m);
+                }
+                b = __shfl_sync(FULL, b, leader);
+                if (key >= 0) perm[b + __popc(m & lanemask_lt())] = i;
+            }
+            __syncthreads();
+            // 4. index-order fold and movement test, warp w takes keys w, w+W, ...
+            for (int k = warp; k < ns; k += W) {
+                const int cnt = kbase[k + 1] - kbase[k];
+                if (cnt == 0) continue;
+                const float sum = fold_members<DIM>(perm + kbase[k], cnt, P, s_buf[warp], s_idx[warp], lane);
+                int moved = 0;
+                if (lane < DIM) {
+                    float cval = sS[k * DP + lane];
+                    moved = shift_coord(sum, cnt, cval);
+                    if (moved) sS[k * DP + lane] = cval;
+                }
+                if (__any_sync(FULL, moved) && lane == 0) s_moved = 1;
+            }
+            __syncthreads();
+            ++pass;
+            if (tid == 0) {
+                v.pairs[c] += (unsigned long long)n * (unsigned long long)ns;
+            }
+            if (!s_moved) break;
+            if (pass >= v.max_passes) {
+                if (tid == 0) v.err[c] |= ERRB_EVOLVE_CAP;
+                break;
+            }
+        }
+        // results back and control (as k_control does after the last pass)
+        for (int e = tid; e < ns; e += BLOCK)
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) gS[(int64_t)e * DIM + d] = sS[e * DP + d];
+        if (tid == 0) {
+            v.passes[c] += pass;
+            v.total_passes[c] += pass;
+            v.cont[c] = 0;
+            v.phase[c] = PH_CONVERGED;
+            const GroupDesc gd = v.gr[cd.group];
+            if (atomicAdd(&v.group_conv[cd.group], 1) + 1 == gd.n_clouds)
+                v.ready[atomicAdd(&v.ctr[CTR_NREADY], 1)] = cd.group;
+        }
+    }
+}
+
+int tile_evolve_smem_bytes(int dim)
+{
+    const int dp = (dim == 3) ? 4 : dim;
+    const int w = 8;
+    return TILE_NS_MAX * dp * 4 + w * (TILE_NS_MAX + 1) * 4 + (TILE_NS_MAX + 1) * 4;
 }
 
 // ---------------------------------------------------------------------------
@@ -779,17 +988,24 @@ __device__ void decimate_group(const EngineView& v, const int g)
     const uint32_t hmask = (1u << hbits) - 1;
     int32_t* bstart = v.dbstart + v.dec_hoff[g];
 
-    // gather the group's chosen points (cloud order) into X
+    // gather the group's chosen points (cloud order) into X, unless the
+    // GPU-wide preparation kernels already did (large group)
+    const int prepared = (v.dbig[0] == 1 && v.dbig[1] == g) ? 1 : 0;
     int total = 0;
     for (int i = 0; i < gd.n_clouds; ++i) {
         const int c = gd.cloud_begin + i;
         const CloudDesc cd = v.cl[c];
         const int ns = v.ns[c];
-        for (int e = tid; e < ns * DIM; e += BLOCK) X[(int64_t)total * DIM + e] = v.S[cd.s_off * DIM + e];
+        if (!prepared)
+            for (int e = tid; e < ns * DIM; e += BLOCK) X[(int64_t)total * DIM + e] = v.S[cd.s_off * DIM + e];
         total += ns;
     }
-    decimate_scan<DIM, BLOCK>(X, total, c0.r2, gd.nocopy, cell, alive, c1, c2, items, bstart, hmask,
-                              &v.err[gd.cloud_begin]);
+    extern __shared__ __align__(16) unsigned char dec_smem[];
+    decimate_scan_lists<DIM, BLOCK>(X, total, c0.r2, gd.nocopy, cell, alive, c1, c2, items, bstart,
+                                    hmask, v.dnb_off + gd.s_scratch + g,
+                                    v.dnb + (int64_t)DEC_NB_PER_POINT * gd.s_scratch,
+                                    (int64_t)DEC_NB_PER_POINT * total, dec_smem, v.dec_smem_max,
+                                    &v.err[gd.cloud_begin], prepared);
     // compaction back into each cloud, in order
     int running = 0, total_after = 0;
     for (int ci = 0; ci < gd.n_clouds; ++ci) {
@@ -837,8 +1053,258 @@ __device__ void decimate_group(const EngineView& v, const int g)
             v.phase[c] = PH_EVOLVE;
         }
     }
-    if (tid == 0) v.group_conv[g] = 0;
+    if (tid == 0) {
+        v.group_conv[g] = 0;
+        if (prepared) v.dbig[0] = 0;
+    }
     __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// GPU-wide preparation of a large decimation (tiled runs: one group of
+// thousands of tiles).  When exactly one group is ready and it holds more
+// than DEC_BIG_MIN points, these kernels build its gathered points, hash
+// buckets, neighbour counts and neighbour lists across all SMs; k_decimate
+// then only runs the in-order scan.  dbig = {state, group, total}: state 1 =
+// prepared, 2 = lists overflowed (k_decimate rebuilds on its own), 0 = idle.
+// ---------------------------------------------------------------------------
+constexpr int DEC_BIG_MIN = 4096;
+
+__global__ void __launch_bounds__(1024) k_decbig_setup(EngineView v)
+{
+    __shared__ int s_w[32];
+    __shared__ int s_carry;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) { v.dbig[0] = 0; s_carry = 0; }
+    if (v.ctr[CTR_NREADY] != 1) return;
+    const int g = v.ready[0];
+    const GroupDesc gd = v.gr[g];
+    __syncthreads();
+    // exclusive prefix of the members' chosen counts -> dcpre
+    for (int i0 = 0; i0 < gd.n_clouds; i0 += 1024) {
+        const int i = i0 + tid;
+        const int x = (i < gd.n_clouds) ? v.ns[gd.cloud_begin + i] : 0;
+        int incl = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) s_w[warp] = incl;
+        __syncthreads();
+        int pre = 0, tot = 0;
+        for (int w = 0; w < 32; ++w) {
+            pre += (w < warp) ? s_w[w] : 0;
+            tot += s_w[w];
+        }
+        const int carry = s_carry;
+        if (i < gd.n_clouds) v.dcpre[i] = carry + pre + incl - x;
+        __syncthreads();
+        if (tid == 0) s_carry = carry + tot;
+        __syncthreads();
+    }
+    const int total = s_carry;
+    if (total <= DEC_BIG_MIN) return;
+    const int hbits = v.dec_hbits[g];
+    int32_t* bstart = v.dbstart + v.dec_hoff[g];
+    for (int h = tid; h <= (1 << hbits); h += 1024) bstart[h] = 0;
+    if (tid == 0) {
+        v.dcpre[gd.n_clouds] = total;
+        v.dbig[1] = g;
+        v.dbig[2] = total;
+        v.dbig[0] = 1;
+    }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256) k_decbig_gather(EngineView v)
+{
+    if (v.dbig[0] != 1) return;
+    const int g = v.dbig[1], total = v.dbig[2];
+    const GroupDesc gd = v.gr[g];
+    const CloudDesc c0 = v.cl[gd.cloud_begin];
+    const double inv = 1.0 / (2.0 * (double)c0.r2 * (1.0 + 1.0 / 1024.0));
+    const uint32_t hmask = (1u << v.dec_hbits[g]) - 1;
+    float* X = v.dx + gd.s_scratch * DIM;
+    int32_t* cell = v.dcell + gd.s_scratch * DIM;
+    int32_t* bstart = v.dbstart + v.dec_hoff[g];
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        int lo = 0, hi = gd.n_clouds - 1;  // last member with dcpre <= t
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (v.dcpre[mid] <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        const CloudDesc cd = v.cl[gd.cloud_begin + lo];
+        const int local = t - v.dcpre[lo];
+        int cc[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            const float x = v.S[(cd.s_off + local) * DIM + d];
+            X[(int64_t)t * DIM + d] = x;
+            cc[d] = cell_of(x, inv);
+            cell[(int64_t)t * DIM + d] = cc[d];
+        }
+        atomicAdd(&bstart[(cell_hash<DIM>(cc) & hmask) + 1], 1);
+    }
+}
+
+// exclusive prefix over the big group's buckets (bstart[b] -> start of bucket b)
+__global__ void __launch_bounds__(1024) k_decbig_scan_buckets(EngineView v)
+{
+    if (v.dbig[0] != 1) return;
+    __shared__ int s_w[32];
+    __shared__ int s_carry;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = v.dbig[1];
+    const int n = (1 << v.dec_hbits[g]) + 1;
+    int32_t* bstart = v.dbstart + v.dec_hoff[g];
+    if (tid == 0) s_carry = 0;
+    __syncthreads();
+    for (int i0 = 0; i0 < n; i0 += 1024) {
+        const int i = i0 + tid;
+        const int x = (i < n) ? bstart[i] : 0;
+        int incl = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) s_w[warp] = incl;
+        __syncthreads();
+        int pre = 0, tot = 0;
+        for (int w = 0; w < 32; ++w) {
+            pre += (w < warp) ? s_w[w] : 0;
+            tot += s_w[w];
+        }
+        const int carry = s_carry;
+        if (i < n) bstart[i] = carry + pre + incl;  // inclusive of the shifted counts
+        __syncthreads();
+        if (tid == 0) s_carry = carry + tot;
+        __syncthreads();
+    }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256) k_decbig_fill(EngineView v)
+{
+    if (v.dbig[0] != 1) return;
+    const int g = v.dbig[1], total = v.dbig[2];
+    const GroupDesc gd = v.gr[g];
+    const uint32_t hmask = (1u << v.dec_hbits[g]) - 1;
+    const int32_t* cell = v.dcell + gd.s_scratch * DIM;
+    int32_t* items = v.ditems + gd.s_scratch;
+    int32_t* bstart = v.dbstart + v.dec_hoff[g];
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        int cc[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) cc[d] = cell[(int64_t)t * DIM + d];
+        items[atomicAdd(&bstart[cell_hash<DIM>(cc) & hmask], 1)] = t;
+    }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256) k_decbig_count(EngineView v)
+{
+    if (v.dbig[0] != 1) return;
+    const int g = v.dbig[1], total = v.dbig[2];
+    const GroupDesc gd = v.gr[g];
+    const CloudDesc c0 = v.cl[gd.cloud_begin];
+    const float rsq = sqr_rn(c0.r2);
+    const float rsq4 = __fmul_rn(4.0f, rsq);
+    const uint32_t hmask = (1u << v.dec_hbits[g]) - 1;
+    const float* X = v.dx + gd.s_scratch * DIM;
+    const int32_t* cell = v.dcell + gd.s_scratch * DIM;
+    const int32_t* items = v.ditems + gd.s_scratch;
+    const int32_t* bstart = v.dbstart + v.dec_hoff[g];
+    int32_t* c1 = v.dc1 + gd.s_scratch;
+    int32_t* c2 = v.dc2 + gd.s_scratch;
+    int32_t* nb_off = v.dnb_off + gd.s_scratch + g;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        int n1 = 1, n2 = 1;
+        dec_for_neighbours<DIM>(t, X, cell, items, bstart, hmask, rsq, rsq4,
+                                [&](int, bool w1) { ++n2; n1 += w1; });
+        c1[t] = n1;
+        c2[t] = n2;
+        nb_off[t] = n2 - 1;
+    }
+}
+
+// exclusive prefix of the list lengths; flags overflow of the list capacity
+__global__ void __launch_bounds__(1024) k_decbig_scan_lists(EngineView v)
+{
+    if (v.dbig[0] != 1) return;
+    __shared__ int s_w[32];
+    __shared__ int s_carry;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = v.dbig[1], total = v.dbig[2];
+    const GroupDesc gd = v.gr[g];
+    int32_t* nb_off = v.dnb_off + gd.s_scratch + g;
+    if (tid == 0) s_carry = 0;
+    __syncthreads();
+    for (int i0 = 0; i0 < total; i0 += 1024) {
+        const int i = i0 + tid;
+        const int x = (i < total) ? nb_off[i] : 0;
+        int incl = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) s_w[warp] = incl;
+        __syncthreads();
+        int pre = 0, tot = 0;
+        for (int w = 0; w < 32; ++w) {
+            pre += (w < warp) ? s_w[w] : 0;
+            tot += s_w[w];
+        }
+        const int carry = s_carry;
+        if (i < total) nb_off[i] = carry + pre + incl - x;
+        __syncthreads();
+        if (tid == 0) s_carry = carry + tot;
+        __syncthreads();
+    }
+    if (tid == 0) {
+        nb_off[total] = s_carry;
+        if ((int64_t)s_carry > (int64_t)DEC_NB_PER_POINT * total) v.dbig[0] = 2;
+    }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256) k_decbig_lists(EngineView v)
+{
+    if (v.dbig[0] != 1) return;
+    const int g = v.dbig[1], total = v.dbig[2];
+    const GroupDesc gd = v.gr[g];
+    const CloudDesc c0 = v.cl[gd.cloud_begin];
+    const float rsq = sqr_rn(c0.r2);
+    const float rsq4 = __fmul_rn(4.0f, rsq);
+    const uint32_t hmask = (1u << v.dec_hbits[g]) - 1;
+    const float* X = v.dx + gd.s_scratch * DIM;
+    const int32_t* cell = v.dcell + gd.s_scratch * DIM;
+    const int32_t* items = v.ditems + gd.s_scratch;
+    const int32_t* bstart = v.dbstart + v.dec_hoff[g];
+    const int32_t* nb_off = v.dnb_off + gd.s_scratch + g;
+    int32_t* nb = v.dnb + (int64_t)DEC_NB_PER_POINT * gd.s_scratch;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        int k = nb_off[t];
+        dec_for_neighbours<DIM>(t, X, cell, items, bstart, hmask, rsq, rsq4,
+                                [&](int q, bool w1) { nb[k++] = w1 ? (q | (int)0x80000000) : q; });
+    }
+}
+
+template <int DIM>
+cudaError_t launch_decbig(const EngineView& v, cudaStream_t st)
+{
+    const int grid = v.n_sms * 8;
+    k_decbig_setup<<<1, 1024, 0, st>>>(v);
+    k_decbig_gather<DIM><<<grid, 256, 0, st>>>(v);
+    k_decbig_scan_buckets<<<1, 1024, 0, st>>>(v);
+    k_decbig_fill<DIM><<<grid, 256, 0, st>>>(v);
+    k_decbig_count<DIM><<<grid, 256, 0, st>>>(v);
+    k_decbig_scan_lists<<<1, 1024, 0, st>>>(v);
+    k_decbig_lists<DIM><<<grid, 256, 0, st>>>(v);
+    return cudaGetLastError();
 }
 
 // one CTA per group queued by k_control in this iteration
@@ -955,6 +1421,7 @@ __global__ void k_reset(EngineView v)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c < CTR_COUNT && blockIdx.x == 0) v.ctr[c] = 0;
+    if (c == 0) v.dbig[0] = 0;
     if (c < v.n_groups) v.group_conv[c] = 0;
     if (c >= v.n_clouds) return;
     v.cont[c] = 0;
@@ -982,6 +1449,9 @@ cudaError_t prepare_pass_dim(const EngineView& v, const TuneParams& tp)
     RD_PREP_CASE(128, 8) RD_PREP_CASE(128, 4) RD_PREP_CASE(256, 4) RD_PREP_CASE(256, 8)
     RD_PREP_CASE(128, 16)
 #undef RD_PREP_CASE
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_decimate<DIM, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             dec_smem_bytes(v));
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 4 * (v.chunk_max + v.scat_smem) * 4);
@@ -1014,7 +1484,7 @@ cudaError_t launch_pass_dim(const EngineView& v, const TuneParams& tp, int assig
                     4 * (v.chunk_max + v.scat_smem) * 4, st>>>(v);
     if (v.n_slots > 0) k_sum_shift<DIM><<<std::min((v.n_slots + 7) / 8, sms * 8), 256, 0, st>>>(v);
     k_control<<<std::min((v.n_clouds + 255) / 256, sms), 256, 0, st>>>(v);
-    k_decimate<DIM, 512><<<std::min(v.n_groups, sms * 2), 512, 0, st>>>(v);
+    k_decimate<DIM, 512><<<std::min(v.n_groups, sms * 2), 512, dec_smem_bytes(v), st>>>(v);
     return cudaGetLastError();
 }
 
@@ -1110,6 +1580,37 @@ cudaError_t launch_loopcond(const EngineView& v, cudaGraphConditionalHandle h, i
     return cudaGetLastError();
 }
 
+cudaError_t prepare_tile_pass(int dim, const EngineView& v)
+{
+    const int smem = tile_evolve_smem_bytes(dim);
+    cudaError_t e = cudaSuccess;
+    if (dim == 2) e = cudaFuncSetAttribute(k_tile_evolve<2, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    else if (dim == 3) e = cudaFuncSetAttribute(k_tile_evolve<3, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    else return cudaErrorInvalidValue;
+    if (e != cudaSuccess) return e;
+    if (dim == 2) return cudaFuncSetAttribute(k_decimate<2, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, dec_smem_bytes(v));
+    return cudaFuncSetAttribute(k_decimate<3, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, dec_smem_bytes(v));
+}
+
+cudaError_t launch_tile_pass(int dim, const EngineView& v, cudaStream_t st)
+{
+    const int smem = tile_evolve_smem_bytes(dim);
+    const int grid = std::max(1, std::min(v.n_clouds, v.n_sms * 3));
+    const int dgrid = std::max(1, std::min(v.n_groups, v.n_sms * 2));
+    if (dim == 2) {
+        k_tile_evolve<2, 256><<<grid, 256, smem, st>>>(v);
+        launch_decbig<2>(v, st);
+        k_decimate<2, 512><<<dgrid, 512, dec_smem_bytes(v), st>>>(v);
+    } else if (dim == 3) {
+        k_tile_evolve<3, 256><<<grid, 256, smem, st>>>(v);
+        launch_decbig<3>(v, st);
+        k_decimate<3, 512><<<dgrid, 512, dec_smem_bytes(v), st>>>(v);
+    } else {
+        return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t launch_set_given(const EngineView& v, int queue_decimation, cudaStream_t st)
 {
     const int n = v.n_clouds > v.n_groups ? v.n_clouds : v.n_groups;
@@ -1120,11 +1621,20 @@ cudaError_t launch_set_given(const EngineView& v, int queue_decimation, cudaStre
 cudaError_t launch_decimate(int dim, const EngineView& v, cudaStream_t st)
 {
     const int grid = std::max(1, std::min(v.n_groups, v.n_sms * 2));
+    const int smem = dec_smem_bytes(v);
+    cudaError_t e = cudaSuccess;
     switch (dim) {
-        case 2: k_decimate<2, 512><<<grid, 512, 0, st>>>(v); break;
-        case 3: k_decimate<3, 512><<<grid, 512, 0, st>>>(v); break;
+        case 2:
+            e = cudaFuncSetAttribute(k_decimate<2, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            if (e == cudaSuccess) k_decimate<2, 512><<<grid, 512, smem, st>>>(v);
+            break;
+        case 3:
+            e = cudaFuncSetAttribute(k_decimate<3, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            if (e == cudaSuccess) k_decimate<3, 512><<<grid, 512, smem, st>>>(v);
+            break;
         default: return cudaErrorInvalidValue;
     }
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 
