@@ -165,6 +165,7 @@ EngineView Engine::view() const
     v.dbig = bDbig_.as<int32_t>();
     v.dcpre = bDcpre_.as<int32_t>();
     v.dec_smem_max = dec_smem_max_;
+    v.dec_nb_pp = dec_nb_pp_;
     v.dec_hoff = bDecHoff_.as<int64_t>();
     v.dec_hbits = bDecHbits_.as<int32_t>();
     v.n_clouds = (int32_t)h_cl_.size();
@@ -226,6 +227,7 @@ int Engine::finish_setup_after_choose(cudaStream_t st)
         int64_t tot = 0;
         for (int i = 0; i < gd.n_clouds; ++i) tot += h_cl_[gd.cloud_begin + i].ns_cap;
         gd.s_scratch = sscr;
+        gd.s_cap = (int32_t)tot;
         sscr += tot;
         max_tot = std::max(max_tot, tot);
         const int hb = std::min(20, std::max(6, ceil_log2(std::max<int64_t>(tot, 1))));
@@ -254,7 +256,10 @@ int Engine::finish_setup_after_choose(cudaStream_t st)
     RD_CK(bDitems_.ensure(4 * (size_t)(sscr + 1)));
     RD_CK(bDbstart_.ensure(4 * (size_t)(hoff + 1)));
     RD_CK(bDnbOff_.ensure(4 * (size_t)(sscr + h_gr_.size() + 1)));
-    RD_CK(bDnb_.ensure(4 * (size_t)(DEC_NB_PER_POINT * sscr + 1)));
+    dec_nb_pp_ = (int)std::max<int64_t>(
+        DEC_NB_MIN_PER_POINT,
+        std::min<int64_t>(DEC_NB_MAX_PER_POINT, DEC_NB_BUDGET / std::max<int64_t>(sscr, 1)));
+    RD_CK(bDnb_.ensure(4 * (size_t)((int64_t)dec_nb_pp_ * sscr + 1)));
     dec_smem_max_ = (int)std::min<int64_t>(max_tot, DEC_SMEM_MAX_POINTS);
     // persistent assignment grid: every resident CTA slot, at most one per chunk
     int dev = 0, sms = 0;

@@ -27,10 +27,16 @@ enum : int {
     ENG_ALWAYS_MOVE = 2,   // adjoint forward: every non-empty cluster moves to its mean
 };
 
-// neighbour-list capacity of the decimation, per chosen point (lists that do
-// not fit fall back to walking the hash buckets)
-constexpr int DEC_NB_PER_POINT = 32;
-constexpr int DEC_SMEM_MAX_POINTS = 40960;
+// neighbour-list capacity of the decimation, per chosen point: at least
+// DEC_NB_MIN_PER_POINT, more while the whole list buffer stays within
+// DEC_NB_BUDGET entries (lists that do not fit fall back to walking the hash
+// buckets)
+constexpr int DEC_NB_MIN_PER_POINT = 32;
+constexpr int DEC_NB_MAX_PER_POINT = 4096;
+constexpr int64_t DEC_NB_BUDGET = int64_t(1) << 28;
+// points whose int16 counts live in the decimation's shared memory (a count
+// never exceeds the number of points, so int16 holds it)
+constexpr int DEC_SMEM_MAX_POINTS = 32752;
 // fused per-tile evolve: chosen points per tile it can hold
 constexpr int TILE_NS_MAX = 1024;
 
@@ -82,10 +88,11 @@ struct EngineView {
     int32_t* dbstart;            // bucket starts (HB+1 per group)
     int32_t* ditems;             // bucket members
     int32_t* dnb_off;            // per group: neighbour-list offsets (total+1)
-    int32_t* dnb;                // per group: neighbour lists, DEC_NB_PER_POINT per point
+    int32_t* dnb;                // per group: neighbour lists, dec_nb_pp per scratch slot
     int32_t* dbig;               // GPU-wide prepared decimation: {state, group, total}
     int32_t* dcpre;              // its members' chosen-count prefix (n_clouds+1)
-    int32_t dec_smem_max;       // points whose counts fit the decimation's shared memory
+    int32_t dec_smem_max;        // points whose counts fit the decimation's shared memory
+    int32_t dec_nb_pp;           // neighbour-list entries per scratch slot
     const int64_t* dec_hoff;     // per group: start of its bucket arrays
     const int32_t* dec_hbits;    // per group: log2 buckets
     int32_t n_clouds;

@@ -114,6 +114,7 @@ private:
     DevBuf bNs_, bPhase_, bCont_, bPasses_, bTotPasses_, bOuter_, bErr_, bPairs_, bCtr_;
     DevBuf bActCloud_, bActPre_, bGroupConv_, bReady_, bDnbOff_, bDnb_, bDbig_, bDcpre_;
     int dec_smem_max_ = 0;
+    int dec_nb_pp_ = DEC_NB_MIN_PER_POINT;
     bool fused_ = false;
     DevBuf bDx_, bDcell_, bDalive_, bDc1_, bDc2_, bDbstart_, bDitems_, bDecHoff_, bDecHbits_;
 

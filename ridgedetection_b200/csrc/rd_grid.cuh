@@ -31,7 +31,11 @@ __device__ __forceinline__ uint32_t cell_hash(const int* c)
     return h ^ (h >> 15);
 }
 
-
+// barrier `id` (1..15; 0 is __syncthreads) over `n` threads, whole warps
+__device__ __forceinline__ void named_bar_sync(int id, int n)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
 
 // offset o in [0, 3^DIM) -> neighbour cell; o == (3^DIM-1)/2 is the home cell
 template <int DIM>
@@ -380,6 +384,23 @@ __device__ void decimate_scan_lists(const float* X, const int total, const float
             if (lane == 0 && (i >> 5) < nwords) cand[i >> 5] = bal;
         }
         __syncthreads();
+        // A removal decrements the counts of its listed neighbours (distinct
+        // points, one thread each) and re-evaluates their candidate bits.
+        auto update = [&](int t) {
+            const int e = nb[t];
+            const int q = e & 0x7fffffff;
+            const int a = (c1s[q] -= (e < 0) ? 1 : 0);
+            const int b = (c2s[q] -= 1);
+            const uint32_t bit = 1u << (q & 31);
+            if (as[q] && (a >= 4 || b < 3)) atomicOr(&cand[q >> 5], bit);
+            else atomicAnd(&cand[q >> 5], ~bit);
+        };
+        // Warp 0 drives the scan; a list longer than DEC_WIDE_LIST is
+        // processed by the whole CTA: the other warps wait on named barrier 1
+        // for a command (list range, or -1 = done) and report completion on
+        // named barrier 2.
+        constexpr int DEC_WIDE_LIST = 96;
+        __shared__ int s_cmd[2];
         if (warp == 0) {
             // first candidate >= pos, or -1
             auto next_cand = [&](int pos) -> int {
@@ -416,20 +437,32 @@ __device__ void decimate_scan_lists(const float* X, const int total, const float
                     }
                     --cnt;
                     const int e0 = nb_off[j], e1 = nb_off[j + 1];
-                    for (int t = e0 + lane; t < e1; t += 32) {  // distinct neighbours per lane
-                        const int e = nb[t];
-                        const int q = e & 0x7fffffff;
-                        const int a = (c1s[q] -= (e < 0) ? 1 : 0);
-                        const int b = (c2s[q] -= 1);
-                        const uint32_t bit = 1u << (q & 31);
-                        if (as[q] && (a >= 4 || b < 3)) atomicOr(&cand[q >> 5], bit);
-                        else atomicAnd(&cand[q >> 5], ~bit);
+                    if (BLOCK > 32 && e1 - e0 > DEC_WIDE_LIST) {
+                        if (lane == 0) { s_cmd[0] = e0; s_cmd[1] = e1; }
+                        named_bar_sync(1, BLOCK);
+                        for (int t = e0 + lane; t < e1; t += BLOCK) update(t);
+                        named_bar_sync(2, BLOCK);
+                    } else {
+                        for (int t = e0 + lane; t < e1; t += 32) update(t);
+                        __syncwarp();
                     }
-                    __syncwarp();
                     if (!nocopy && cnt < 3) break;
                     pos = j + 1;
                 }
                 if (!nocopy && cnt < 3) break;
+            }
+            if (BLOCK > 32) {
+                if (lane == 0) s_cmd[0] = -1;
+                named_bar_sync(1, BLOCK);
+            }
+        } else {
+            for (;;) {
+                named_bar_sync(1, BLOCK);
+                const int e0 = s_cmd[0];
+                if (e0 < 0) break;
+                const int e1 = s_cmd[1];
+                for (int t = e0 + tid; t < e1; t += BLOCK) update(t);
+                named_bar_sync(2, BLOCK);
             }
         }
         __syncthreads();

@@ -67,8 +67,8 @@ struct GroupDesc {
     int32_t cloud_begin;
     int32_t n_clouds;
     int32_t nocopy;      // decimateNoCopy semantics (tiled) instead of decimate
-    int32_t pad;
-    int64_t s_scratch;   // scratch slots for the group's decimation
+    int32_t s_cap;       // scratch slots of the group (its members' chosen capacity)
+    int64_t s_scratch;   // first scratch slot of the group's decimation
 };
 
 constexpr int SEG = 16;  // histogram rows per segment in the column scan

@@ -1003,8 +1003,8 @@ __device__ void decimate_group(const EngineView& v, const int g)
     extern __shared__ __align__(16) unsigned char dec_smem[];
     decimate_scan_lists<DIM, BLOCK>(X, total, c0.r2, gd.nocopy, cell, alive, c1, c2, items, bstart,
                                     hmask, v.dnb_off + gd.s_scratch + g,
-                                    v.dnb + (int64_t)DEC_NB_PER_POINT * gd.s_scratch,
-                                    (int64_t)DEC_NB_PER_POINT * total, dec_smem, v.dec_smem_max,
+                                    v.dnb + (int64_t)v.dec_nb_pp * gd.s_scratch,
+                                    (int64_t)v.dec_nb_pp * gd.s_cap, dec_smem, v.dec_smem_max,
                                     &v.err[gd.cloud_begin], prepared);
     // compaction back into each cloud, in order
     int running = 0, total_after = 0;
@@ -1266,7 +1266,7 @@ __global__ void __launch_bounds__(1024) k_decbig_scan_lists(EngineView v)
     }
     if (tid == 0) {
         nb_off[total] = s_carry;
-        if ((int64_t)s_carry > (int64_t)DEC_NB_PER_POINT * total) v.dbig[0] = 2;
+        if ((int64_t)s_carry > (int64_t)v.dec_nb_pp * gd.s_cap) v.dbig[0] = 2;
     }
 }
 
@@ -1285,7 +1285,7 @@ __global__ void __launch_bounds__(256) k_decbig_lists(EngineView v)
     const int32_t* items = v.ditems + gd.s_scratch;
     const int32_t* bstart = v.dbstart + v.dec_hoff[g];
     const int32_t* nb_off = v.dnb_off + gd.s_scratch + g;
-    int32_t* nb = v.dnb + (int64_t)DEC_NB_PER_POINT * gd.s_scratch;
+    int32_t* nb = v.dnb + (int64_t)v.dec_nb_pp * gd.s_scratch;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
         int k = nb_off[t];
         dec_for_neighbours<DIM>(t, X, cell, items, bstart, hmask, rsq, rsq4,

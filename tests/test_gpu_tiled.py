@@ -39,11 +39,16 @@ def test_tiled_matches_reference_golden(rdb, path, mode):
     ("spiral_split", 30_000, 0.2, 0.4, 1500, (3, 5)),
     ("helix", 40_000, 0.15, 0.3, 40_001, (4, 4, 3)),
     ("sine_one_tile", 5_000, 0.3, 0.6, 5_001, (1, 1)),
+    # 3106 tiles: the global decimation holds more than 4096 chosen points
+    # (GPU-wide preparation) with neighbour lists long enough for the
+    # CTA-wide count updates
+    ("spiral_4k_tiles", 200_000, 0.2, 0.4, 200_001, (64, 64)),
 ])
 def test_tiled_matches_oracle(rdb, case):
     kind, n, r1, r2, cap, tpd = case
     P = {"spiral": lambda: G.spiral2d(n, seed=41), "spiral_split": lambda: G.spiral2d(n, seed=42),
-         "helix": lambda: G.helix3d(n, seed=43), "sine_one_tile": lambda: G.sine2d(n, seed=44)}[kind]()
+         "helix": lambda: G.helix3d(n, seed=43), "sine_one_tile": lambda: G.sine2d(n, seed=44),
+         "spiral_4k_tiles": lambda: G.spiral2d(n, seed=45)}[kind]()
     S_ref, st_ref, nl_ref = O.ridge_tiled(P, r1, r2, cap, tpd)
     S, st, nl = rdb.tiled_ridge_detection(P, r1, r2, cap, tpd)
     assert nl == nl_ref
