@@ -73,6 +73,16 @@ RD_API int rd_supported_dims(void);
  * current device from an independent-chain FMA kernel timed with CUDA events,
  * in TFLOP/s (2 flops per FMA).  Used as the FP32 roofline denominator. */
 RD_API rd_status rd_probe_fp32_peak(double* tflops, void* stream);
+/* Building block of the evolve step (no reference counterpart; the reference
+ * forms the same sums inline, rd/cpu/brute_force/evolve.hpp:71-74): for each
+ * coordinate d < dim, out[d] = the left-to-right FP32 sum, starting from 0 with
+ * one rounding per term, of d_P[d_idx[i]*dim + d] for i = 0..n-1.  method 0
+ * evaluates it as a chain of adds, method 1 with the warp-parallel exact
+ * evaluation and method 2 with the CTA-wide exact evaluation that the evolve
+ * kernels use for large clusters; all are bit-identical to the serial loop.  All pointers are device pointers; d_out
+ * holds dim floats.  Runs on `stream` and waits for it. */
+RD_API rd_status rd_ordered_sum(int dim, const float* d_P, const int32_t* d_idx, int64_t n,
+                                float* d_out, int method, void* stream);
 
 /* ---------------------------------------------------------------------------
  * Brute force, one cloud.  Mirrors rd::gpu::bruteForce::RidgeDetection:

@@ -243,6 +243,19 @@ rd_status rd_probe_fp32_peak(double* tflops, void* stream)
     return RD_OK;
 }
 
+rd_status rd_ordered_sum(int dim, const float* d_P, const int32_t* d_idx, int64_t n,
+                         float* d_out, int method, void* stream)
+{
+    if (dim != 2 && dim != 3) return set_err(RD_ERR_ARG, "dim must be 2 or 3");
+    if (n < 0 || n > INT32_MAX) return set_err(RD_ERR_ARG, "n out of range");
+    if ((n > 0 && (!d_P || !d_idx)) || !d_out) return set_err(RD_ERR_ARG, "null argument");
+    if (method < 0 || method > 2) return set_err(RD_ERR_ARG, "method must be 0, 1 or 2");
+    cudaStream_t st = (cudaStream_t)stream;
+    CK_CUDA(launch_ordered_sum(dim, d_P, d_idx, (int)n, d_out, method, st));
+    CK_CUDA(cudaStreamSynchronize(st));
+    return RD_OK;
+}
+
 // ------------------------------------------------------------------------
 // brute force
 // ------------------------------------------------------------------------

@@ -147,6 +147,9 @@ cudaError_t launch_set_given(const EngineView& v, int queue_decimation, cudaStre
 cudaError_t prepare_tile_pass(int dim, const EngineView& v);
 cudaError_t launch_tile_pass(int dim, const EngineView& v, cudaStream_t st);
 cudaError_t launch_decimate(int dim, const EngineView& v, cudaStream_t st);
+// out[d] = ordered FP32 sum of P[idx[i]*dim + d] (method 0 chain, 1 parallel exact)
+cudaError_t launch_ordered_sum(int dim, const float* P, const int32_t* idx, int n, float* out,
+                               int method, cudaStream_t st);
 // the five kernels of one evolve pass without control/decimation (adjoint forward)
 cudaError_t launch_evolve_step(int dim, const EngineView& v, const TuneParams& tp, int assign_grid,
                                cudaStream_t st);

@@ -9,6 +9,7 @@
 // (DIM-1) add + compare + 2 selects, all explicitly rounded.
 #include "rd_engine.cuh"
 #include "rd_grid.cuh"
+#include "rd_fold.cuh"
 
 #include <cuda_runtime.h>
 
@@ -647,6 +648,12 @@ __device__ void scatter_chunk(const EngineView& v, int c, int lc, int* s_keys, i
 // while the current one is folded.
 // ---------------------------------------------------------------------------
 constexpr int SUM_BP = 128;  // members staged per step of the ordered fold
+// points (keys) per lane loaded together by the fused tile kernel's
+// assignment (placement) loop
+constexpr int TILE_PPL = 8;
+// members from which the fused tile kernel folds a key with the whole CTA
+// (exact parallel evaluation, rd_fold.cuh) instead of one warp's add chain
+constexpr int FOLD_CTA_MIN = 4096;
 
 template <int DIM>
 __device__ void sum_shift_one(const EngineView& v, int c, int k, float* buf, int* sidx, int lane);
@@ -735,8 +742,9 @@ __device__ void sum_shift_one(const EngineView& v, int c, int k, float* buf, int
     const CloudDesc cd = v.cl[c];
     const int n = v.cnt[cd.key_off + k];
     if (n == 0) return;
-    const float sum = fold_members<DIM>(v.perm + cd.p_off + v.base[cd.key_off + k], n,
-                                        v.P + cd.p_off * DIM, buf, sidx, lane);
+    const int32_t* mp = v.perm + cd.p_off + v.base[cd.key_off + k];
+    const float* Pc = v.P + cd.p_off * DIM;
+    const float sum = fold_members<DIM>(mp, n, Pc, buf, sidx, lane);
     int moved = 0;
     if (lane < DIM) {
         float* s = v.S + (cd.s_off + k) * DIM + lane;
@@ -779,6 +787,7 @@ __global__ void __launch_bounds__(BLOCK) k_tile_evolve(EngineView v)
     __shared__ float s_buf[W][SUM_BP * DIM];
     __shared__ int s_idx[W][SUM_BP];
     __shared__ int s_moved;
+    __shared__ FoldCtaSmem<W, DIM> s_fold;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nact = v.ctr[CTR_NACT];
     for (int a = blockIdx.x; a < nact; a += gridDim.x) {
@@ -800,36 +809,59 @@ __global__ void __launch_bounds__(BLOCK) k_tile_evolve(EngineView v)
         int pass = 0;
         for (;;) {
             // 1. assignment of the warp's range + per-warp key counts
+            //    (counts added once per distinct key of a warp step)
             for (int k = lane; k <= ns; k += 32) hist[warp * (TILE_NS_MAX + 1) + k] = 0;
             __syncthreads();
-            for (int i0 = r0; i0 < r1w; i0 += 32) {
-                const int i = i0 + lane;
-                int key = -1;
-                if (i < r1w) {
-                    float p[DIM];
+            int* whist = hist + warp * (TILE_NS_MAX + 1);
+            for (int i0 = r0; i0 < r1w; i0 += 32 * TILE_PPL) {
+                float p[TILE_PPL][DIM];
 #pragma unroll
-                    for (int d = 0; d < DIM; ++d) p[d] = P[(int64_t)i * DIM + d];
-                    float best = FLT_MAX;
-                    int blk = -1;
-                    for (int kb = 0; kb < nsp; kb += KB) {
-                        const float old = best;
+                for (int h = 0; h < TILE_PPL; ++h) {
+                    const int i = i0 + h * 32 + lane;
 #pragma unroll
-                        for (int u = 0; u < KB; ++u) {
-                            float s[DIM];
-                            load_chosen<DIM>(sS, kb + u, s);
-                            best = fminf(best, sqdist_exact<DIM>(s, p));
+                    for (int d = 0; d < DIM; ++d) p[h][d] = (i < r1w) ? P[(int64_t)i * DIM + d] : 0.0f;
+                }
+#pragma unroll
+                for (int h = 0; h < TILE_PPL; ++h) {
+                    const int i = i0 + h * 32 + lane;
+                    int key = -1;
+                    if (i < r1w) {
+                        if (ns <= KB) {
+                            // first index of the minimum, directly
+                            float best = FLT_MAX;
+                            int bk = -1;
+                            for (int k = 0; k < ns; ++k) {
+                                float s[DIM];
+                                load_chosen<DIM>(sS, k, s);
+                                const float dd = sqdist_exact<DIM>(s, p[h]);
+                                if (dd < best) { best = dd; bk = k; }
+                            }
+                            key = (best <= rsq) ? bk : -1;
+                        } else {
+                            float best = FLT_MAX;
+                            int blk = -1;
+                            for (int kb = 0; kb < nsp; kb += KB) {
+                                const float old = best;
+#pragma unroll
+                                for (int u = 0; u < KB; ++u) {
+                                    float s[DIM];
+                                    load_chosen<DIM>(sS, kb + u, s);
+                                    best = fminf(best, sqdist_exact<DIM>(s, p[h]));
+                                }
+                                blk = (best < old) ? kb : blk;
+                            }
+                            if (best <= rsq && blk >= 0) {
+                                for (int u = 0; u < KB && blk + u < ns; ++u) {
+                                    float s[DIM];
+                                    load_chosen<DIM>(sS, blk + u, s);
+                                    if (sqdist_exact<DIM>(s, p[h]) == best) { key = blk + u; break; }
+                                }
+                            }
                         }
-                        blk = (best < old) ? kb : blk;
+                        keys[i] = key;
                     }
-                    if (best <= rsq && blk >= 0) {
-                        for (int u = 0; u < KB && blk + u < ns; ++u) {
-                            float s[DIM];
-                            load_chosen<DIM>(sS, blk + u, s);
-                            if (sqdist_exact<DIM>(s, p) == best) { key = blk + u; break; }
-                        }
-                    }
-                    keys[i] = key;
-                    if (key >= 0) atomicAdd(&hist[warp * (TILE_NS_MAX + 1) + key], 1);
+                    const unsigned mm = __match_any_sync(FULL, key);
+                    if (key >= 0 && lane == __ffs(mm) - 1) atomicAdd(&whist[key], __popc(mm));
                 }
             }
             __syncthreads();
@@ -866,26 +898,51 @@ __global__ void __launch_bounds__(BLOCK) k_tile_evolve(EngineView v)
                 }
             }
             __syncthreads();
-            // 3. stable placement, warp range by warp range
+            // 3. stable placement, warp range by warp range (keys of
+            //    TILE_PPL warp steps loaded ahead of the dependent placement
+            //    chain)
             int* cur = hist + warp * (TILE_NS_MAX + 1);
-            for (int i0 = r0; i0 < r1w; i0 += 32) {
-                const int i = i0 + lane;
-                const int key = (i < r1w) ? keys[i] : -1;
-                const unsigned m = __match_any_sync(FULL, key);
-                const int leader = __ffs(m) - 1;
-                int b = 0;
-                if (key >= 0 && lane == leader) {
-                    b = cur[key];
-                    cur[key] = b + __popc(m);
+            for (int i0 = r0; i0 < r1w; i0 += 32 * TILE_PPL) {
+                int kq[TILE_PPL];
+#pragma unroll
+                for (int h = 0; h < TILE_PPL; ++h) {
+                    const int i = i0 + h * 32 + lane;
+                    kq[h] = (i < r1w) ? keys[i] : -1;
                 }
-                b = __shfl_sync(FULL, b, leader);
-                if (key >= 0) perm[b + __popc(m & lanemask_lt())] = i;
+#pragma unroll
+                for (int h = 0; h < TILE_PPL; ++h) {
+                    const int i = i0 + h * 32 + lane;
+                    const int key = kq[h];
+                    const unsigned m = __match_any_sync(FULL, key);
+                    const int leader = __ffs(m) - 1;
+                    int b = 0;
+                    if (key >= 0 && lane == leader) {
+                        b = cur[key];
+                        cur[key] = b + __popc(m);
+                    }
+                    b = __shfl_sync(FULL, b, leader);
+                    if (key >= 0) perm[b + __popc(m & lanemask_lt())] = i;
+                }
             }
             __syncthreads();
-            // 4. index-order fold and movement test, warp w takes keys w, w+W, ...
+            // 4a. very large keys, one at a time, folded by the whole CTA
+            for (int k = 0; k < ns; ++k) {
+                const int cnt = kbase[k + 1] - kbase[k];
+                if (cnt < FOLD_CTA_MIN) continue;
+                fold_members_cta<W, DIM>(perm + kbase[k], cnt, P, s_fold);
+                if (tid < DIM) {
+                    float cval = sS[k * DP + tid];
+                    if (shift_coord(s_fold.s[tid], cnt, cval)) {
+                        sS[k * DP + tid] = cval;
+                        s_moved = 1;
+                    }
+                }
+                __syncthreads();
+            }
+            // 4b. index-order fold and movement test, warp w takes keys w, w+W, ...
             for (int k = warp; k < ns; k += W) {
                 const int cnt = kbase[k + 1] - kbase[k];
-                if (cnt == 0) continue;
+                if (cnt == 0 || cnt >= FOLD_CTA_MIN) continue;
                 const float sum = fold_members<DIM>(perm + kbase[k], cnt, P, s_buf[warp], s_idx[warp], lane);
                 int moved = 0;
                 if (lane < DIM) {
@@ -1608,6 +1665,42 @@ cudaError_t launch_tile_pass(int dim, const EngineView& v, cudaStream_t st)
     } else {
         return cudaErrorInvalidValue;
     }
+    return cudaGetLastError();
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(32) k_ordered_sum(const float* P, const int32_t* idx, int n,
+                                                   float* out, int method)
+{
+    __shared__ float s_buf[SUM_BP * DIM];
+    __shared__ int s_idx[SUM_BP];
+    const int lane = threadIdx.x;
+    const float r = (method == 1) ? fold_members_par<DIM>(idx, n, P, lane)
+                                  : fold_members<DIM>(idx, n, P, s_buf, s_idx, lane);
+    if (lane < DIM) out[lane] = r;
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256) k_ordered_sum_cta(const float* P, const int32_t* idx, int n,
+                                                         float* out)
+{
+    __shared__ FoldCtaSmem<8, DIM> sm;
+    fold_members_cta<8, DIM>(idx, n, P, sm);
+    if (threadIdx.x < DIM) out[threadIdx.x] = sm.s[threadIdx.x];
+}
+
+cudaError_t launch_ordered_sum(int dim, const float* P, const int32_t* idx, int n, float* out,
+                               int method, cudaStream_t st)
+{
+    if (method == 2) {
+        if (dim == 2) k_ordered_sum_cta<2><<<1, 256, 0, st>>>(P, idx, n, out);
+        else if (dim == 3) k_ordered_sum_cta<3><<<1, 256, 0, st>>>(P, idx, n, out);
+        else return cudaErrorInvalidValue;
+        return cudaGetLastError();
+    }
+    if (dim == 2) k_ordered_sum<2><<<1, 32, 0, st>>>(P, idx, n, out, method);
+    else if (dim == 3) k_ordered_sum<3><<<1, 32, 0, st>>>(P, idx, n, out, method);
+    else return cudaErrorInvalidValue;
     return cudaGetLastError();
 }
 
