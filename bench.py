@@ -48,9 +48,14 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="helix3d_1m",
-                    choices=["helix3d_1m", "sine2d_20k", "batch"])
+                    choices=["helix3d_1m", "sine2d_20k", "batch", "spiral2d_10m_tiled"])
     ap.add_argument("--clouds", type=int, default=4096, help="batch workload: number of clouds")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-run", action="store_true",
+                    help="no timing and no JSON line: after --warmup solves, run --steps "
+                         "solves with the host-driven loop so that a profiler sees every "
+                         "kernel launch (graph-launched kernels inside a conditional "
+                         "node are not profiled)")
     return ap.parse_args()
 
 
@@ -60,7 +65,35 @@ def workload(name):
         return G.helix3d(1_000_000), 0.15, 0.3
     if name == "sine2d_20k":
         return G.sine2d(20_000), 0.3, 0.6
+    if name == "spiral2d_10m_tiled":
+        return G.spiral2d(10_000_000), 0.2, 0.4
     raise ValueError(name)
+
+
+def run_profile(args):
+    """Solves with the host-driven loop for profilers (see --profile-run)."""
+    import torch
+    import ridgedetection_b200 as rdb
+    P, r1, r2 = workload(args.workload)
+    n, dim = P.shape
+    dP = torch.from_numpy(P).cuda()
+    if args.workload == "spiral2d_10m_tiled":
+        rd = rdb.TiledRidgeDetection(n, dim, loop_mode=rdb.LOOP_HOST)
+        rd.set_points(dP)
+        solve = lambda: rd(r1, r2, n + 1, (64, 64))  # noqa: E731
+    else:
+        rdb.autotune(dim, n, max(1, rdb.choose_count(dP, r1)), reps=4)
+        rd = rdb.BruteForceRidgeDetection(n, r1, r2, dim, loop_mode=rdb.LOOP_HOST)
+        rd.set_points(dP)
+        solve = rd.ridge_detection
+    for _ in range(args.warmup):
+        solve()
+    for _ in range(args.steps):
+        solve()
+    torch.cuda.synchronize()
+    st = rd.stats()
+    print(json.dumps({"profile_run": args.workload, "solves": args.warmup + args.steps,
+                      "loop_iters_last": st.loop_iters, "evolve_passes_last": st.evolve_passes}))
 
 
 class ClockSampler:
@@ -195,6 +228,10 @@ def run_b200_bf(args, world, rank, local):
     stream = torch.cuda.current_stream()
     dP = torch.from_numpy(P).to(dev)
     l2_flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    # launch shape of the assignment kernel from the project's autotuner, on a
+    # synthetic cloud of this size with the chosen count of the first choose
+    # (setup, outside every timed region)
+    tb, ti, tus = rdb.autotune(dim, n, max(1, rdb.choose_count(dP, r1)), reps=4)
     rd = rdb.BruteForceRidgeDetection(n, r1, r2, dim)
     rd.set_points(dP)
 
@@ -293,7 +330,9 @@ def run_b200_bf(args, world, rank, local):
         "config": {"workload": f"{args.workload}: brute-force full solve, N={n}, dim={dim}, "
                                f"r1={r1}, r2={r2}",
                    "l2": "flushed (256 MiB write) between timed steps",
-                   "loop": "CUDA graph WHILE node", "parallelism": f"replicas x{world}"},
+                   "loop": "CUDA graph WHILE node", "parallelism": f"replicas x{world}",
+                   "assign_shape": {"block": tb, "items": ti, "source": "rd_autotune",
+                                    "tuned_us_per_launch": tus}},
         "solves_per_s": world * 1e3 / ms_max,
         "pairs_per_step": pairs_step, "loop_iters_per_step": iters_step,
         "ns_final": ns_final,
@@ -367,6 +406,9 @@ def run_b200_batch(args, world, rank, local):
 def main():
     args = parse_args()
     world, rank, local = dist_setup(args)
+    if args.profile_run:
+        run_profile(args)
+        return
     if args.impl == "reference":
         run_reference_arm(args, world, rank)
         return

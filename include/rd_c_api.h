@@ -73,6 +73,23 @@ RD_API int rd_supported_dims(void);
  * current device from an independent-chain FMA kernel timed with CUDA events,
  * in TFLOP/s (2 flops per FMA).  Used as the FP32 roofline denominator. */
 RD_API rd_status rd_probe_fp32_peak(double* tflops, void* stream);
+/* Launch-shape tuning (no reference counterpart: the reference's launch
+ * shapes are compile-time constants).  When an engine is set up, the
+ * assignment kernel's shape -- CTA size `block` and points per thread
+ * `items` -- is looked up for (dim, floor(log2(points of the largest
+ * cloud))).  Supported shapes: block 128 with items 4, 8 or 16, block 256
+ * with items 4 or 8; unset buckets use 128 x 8.  The table is process-wide
+ * and thread-safe; shapes change speed only, never results. */
+RD_API rd_status rd_tune_set(int dim, int64_t n, int block, int items);
+RD_API rd_status rd_tune_get(int dim, int64_t n, int* block, int* items);
+RD_API rd_status rd_tune_reset(void);
+/* Times every supported shape on a synthetic cloud of n uniform points with
+ * ns chosen points (assignment kernel, CUDA events, mean over `reps` evolve
+ * passes), stores the fastest for (dim, bucket of n) and returns it with its
+ * time per launch in microseconds.  Runs on `stream` and waits for it. */
+RD_API rd_status rd_autotune(int dim, int64_t n, int64_t ns, int reps, int* block, int* items,
+                             double* us_per_launch, void* stream);
+
 /* Building block of the evolve step (no reference counterpart; the reference
  * forms the same sums inline, rd/cpu/brute_force/evolve.hpp:71-74): for each
  * coordinate d < dim, out[d] = the left-to-right FP32 sum, starting from 0 with

@@ -61,6 +61,12 @@ SIGNATURES = {
     "rd_abi_version": [],
     "rd_supported_dims": [],
     "rd_probe_fp32_peak": [ctypes.POINTER(ctypes.c_double), _vp],
+    "rd_tune_set": [ctypes.c_int, ctypes.c_int64, ctypes.c_int, ctypes.c_int],
+    "rd_tune_get": [ctypes.c_int, ctypes.c_int64, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
+    "rd_tune_reset": [],
+    "rd_autotune": [ctypes.c_int, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
+                    ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                    ctypes.POINTER(ctypes.c_double), _vp],
     "rd_ordered_sum": [ctypes.c_int, _vp, _vp, ctypes.c_int64, _vp, ctypes.c_int, _vp],
     "rd_bf_create": [ctypes.POINTER(_vp), _i, _i, _i, _i64, _f, _f],
     "rd_bf_set_points": [_vp, _vp, _i64, _i, _vp],

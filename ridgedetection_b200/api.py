@@ -290,3 +290,51 @@ def pack_clouds(clouds: Sequence[Tuple[np.ndarray, float, float]]):
         off += P.size
     packed = np.concatenate(parts) if parts else np.zeros(0, np.float32)
     return np.ascontiguousarray(packed, dtype=np.float32), descs
+
+
+# ---------------------------------------------------------------------------
+# launch-shape tuning (no reference counterpart)
+# ---------------------------------------------------------------------------
+
+def tune_set(dim: int, n: int, block: int, items: int) -> None:
+    """Use CTA size ``block`` and ``items`` points per thread for the
+    assignment kernel of clouds of dimension ``dim`` whose size is in the
+    power-of-two bucket of ``n``."""
+    L.check(L.lib().rd_tune_set(dim, n, block, items))
+
+
+def tune_get(dim: int, n: int) -> Tuple[int, int]:
+    """(block, items) the engine will use for a ``dim``-D cloud of ``n`` points."""
+    b, i = ctypes.c_int(0), ctypes.c_int(0)
+    L.check(L.lib().rd_tune_get(dim, n, ctypes.byref(b), ctypes.byref(i)))
+    return b.value, i.value
+
+
+def tune_reset() -> None:
+    """Forget every tuned or set shape (back to the default 128 x 8)."""
+    L.check(L.lib().rd_tune_reset())
+
+
+def choose_count(P, r1: float) -> int:
+    """Number of points the greedy r1-ball choose keeps for the cloud P (a
+    float32 CUDA tensor or numpy array, ROW_MAJOR n x dim)."""
+    import torch
+    dP = P if _is_torch_cuda(P) else torch.from_numpy(np.ascontiguousarray(P, np.float32)).cuda()
+    n, dim = dP.shape
+    S = torch.empty_like(dP)
+    ns = ctypes.c_int64(0)
+    stream = torch.cuda.current_stream().cuda_stream
+    L.check(L.lib().rd_choose(dim, ctypes.c_void_p(dP.data_ptr()), n, float(r1),
+                              ctypes.c_void_p(S.data_ptr()), ctypes.byref(ns),
+                              ctypes.c_void_p(stream)))
+    return int(ns.value)
+
+
+def autotune(dim: int, n: int, ns: int, reps: int = 5) -> Tuple[int, int, float]:
+    """Time every supported assignment shape on a synthetic ``dim``-D cloud of
+    ``n`` points with ``ns`` chosen points, keep the fastest for the size
+    bucket of ``n`` and return (block, items, microseconds per launch)."""
+    b, i, us = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_double(0)
+    L.check(L.lib().rd_autotune(dim, n, ns, reps, ctypes.byref(b), ctypes.byref(i),
+                                ctypes.byref(us), None))
+    return b.value, i.value, us.value

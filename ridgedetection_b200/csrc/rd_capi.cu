@@ -243,6 +243,89 @@ rd_status rd_probe_fp32_peak(double* tflops, void* stream)
     return RD_OK;
 }
 
+// ------------------------------------------------------------------------
+// launch-shape tuning
+// ------------------------------------------------------------------------
+static rd_status one_cloud_engine(Engine& e, int dim, int64_t n_points, int64_t capacity, float r1,
+                                  float r2);
+
+static bool shape_ok(int dim, int block, int items)
+{
+    return dim_ok(dim) && tune_supported(dim, TuneParams{block, items});
+}
+
+rd_status rd_tune_set(int dim, int64_t n, int block, int items)
+{
+    if (!shape_ok(dim, block, items)) return set_err(RD_ERR_UNSUPPORTED, "unsupported dim or launch shape");
+    if (n < 1) return set_err(RD_ERR_ARG, "n must be positive");
+    tune_store(dim, n, TuneParams{block, items});
+    return RD_OK;
+}
+
+rd_status rd_tune_get(int dim, int64_t n, int* block, int* items)
+{
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (!block || !items) return set_err(RD_ERR_ARG, "null argument");
+    const TuneParams tp = tune_lookup(dim, n);
+    *block = tp.block;
+    *items = tp.items;
+    return RD_OK;
+}
+
+rd_status rd_tune_reset(void)
+{
+    tune_clear();
+    return RD_OK;
+}
+
+rd_status rd_autotune(int dim, int64_t n, int64_t ns, int reps, int* block, int* items,
+                      double* us_per_launch, void* stream)
+{
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (!block || !items) return set_err(RD_ERR_ARG, "null argument");
+    if (n < 1 || n > INT32_MAX - 1024 || ns < 1 || ns > n || reps < 1 || reps > 1000)
+        return set_err(RD_ERR_ARG, "need 1 <= ns <= n and 1 <= reps <= 1000");
+    cudaStream_t st = (cudaStream_t)stream;
+    // synthetic cloud: n uniform points in the unit cube, the first ns of them
+    // as the chosen set, r1 large enough that every point is assigned
+    std::vector<float> pts((size_t)n * dim);
+    uint64_t x = 0x9E3779B97F4A7C15ull;
+    for (float& f : pts) {
+        x = x * 6364136223846793005ull + 1442695040888963407ull;
+        f = (float)((x >> 40) & 0xFFFFFF) / 16777216.0f;
+    }
+    double best = -1.0;
+    TuneParams bt{128, 8};
+    for (const TuneParams& tp : tune_candidates()) {
+        if (!tune_supported(dim, tp)) continue;
+        Engine e;
+        e.tune = tp;
+        e.tune_locked = true;
+        e.max_passes = reps;
+        e.profile_assign = true;
+        if (rd_status s = one_cloud_engine(e, dim, n, n, 2.0f, 2.0f)) return s;
+        CK_CUDA(cudaMemcpyAsync(e.points(), pts.data(), sizeof(float) * n * dim, cudaMemcpyHostToDevice, st));
+        CK_CUDA(cudaMemcpyAsync(e.chosen_mut(), pts.data(), sizeof(float) * ns * dim, cudaMemcpyHostToDevice, st));
+        e.given_ns.assign(1, (int32_t)ns);
+        const int rc = e.run(st, false, Engine::RUN_EVOLVE_ONLY);
+        if (rc && rc != RD_ERR_NOT_CONVERGED) return from_engine(rc, e);
+        const RunStats& rs = e.stats();
+        if (rs.assign_launches <= 0) continue;
+        const double us = 1e3 * rs.assign_ms / (double)rs.assign_launches;
+        if (best < 0 || us < best) {
+            best = us;
+            bt = tp;
+        }
+    }
+    CK_CUDA(cudaStreamSynchronize(st));
+    if (best < 0) return set_err(RD_ERR_CUDA, "no launch shape could be timed");
+    tune_store(dim, n, bt);
+    *block = bt.block;
+    *items = bt.items;
+    if (us_per_launch) *us_per_launch = best;
+    return RD_OK;
+}
+
 rd_status rd_ordered_sum(int dim, const float* d_P, const int32_t* d_idx, int64_t n,
                          float* d_out, int method, void* stream)
 {

@@ -3,8 +3,51 @@
 
 #include <algorithm>
 #include <cstring>
+#include <map>
+#include <mutex>
 
 namespace rdb {
+
+// ---------------------------------------------------------------------------
+// tuning table
+// ---------------------------------------------------------------------------
+namespace {
+std::mutex g_tune_mu;
+std::map<std::pair<int, int>, TuneParams> g_tune;
+}  // namespace
+
+int tune_bucket(int64_t n)
+{
+    int b = 0;
+    while (b < 62 && (int64_t(1) << (b + 1)) <= std::max<int64_t>(n, 1)) ++b;
+    return b;
+}
+
+TuneParams tune_lookup(int dim, int64_t n)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find({dim, tune_bucket(n)});
+    return (it != g_tune.end()) ? it->second : TuneParams{128, 8};
+}
+
+void tune_store(int dim, int64_t n, const TuneParams& tp)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[{dim, tune_bucket(n)}] = tp;
+}
+
+void tune_clear()
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune.clear();
+}
+
+const std::vector<TuneParams>& tune_candidates()
+{
+    static const std::vector<TuneParams> c = {{128, 4}, {128, 8}, {128, 16}, {256, 4}, {256, 8}};
+    return c;
+}
+
 
 cudaError_t DevBuf::ensure(size_t want)
 {
@@ -63,6 +106,11 @@ int Engine::setup(int dim, const std::vector<CloudDesc>& clouds,
     if (dim != 2 && dim != 3) {
         last_error = "dim must be 2 or 3";
         return 6;  // RD_ERR_UNSUPPORTED
+    }
+    if (!tune_locked) {
+        int64_t nmax = 1;
+        for (const CloudDesc& cd : clouds) nmax = std::max<int64_t>(nmax, cd.n_all);
+        tune = tune_lookup(dim, nmax);
     }
     if (!tune_supported(dim, tune)) {
         last_error = "unsupported tuning parameters";

@@ -31,6 +31,16 @@ struct RunStats {
     int64_t assign_launches = 0;
 };
 
+// Process-wide tuning table: (dim, size bucket) -> assign launch shape.  The
+// bucket of a cloud of n points is floor(log2(n)); entries come from
+// rd_autotune (measured) or rd_tune_set (given).  Thread-safe.
+int tune_bucket(int64_t n);
+TuneParams tune_lookup(int dim, int64_t n);
+void tune_store(int dim, int64_t n, const TuneParams& tp);
+void tune_clear();
+// supported launch shapes, in a fixed order
+const std::vector<TuneParams>& tune_candidates();
+
 class Engine {
 public:
     Engine();
@@ -81,6 +91,7 @@ public:
     int max_outer = 4096;
     int max_iters = 1 << 18;
     TuneParams tune{128, 8};
+    bool tune_locked = false;     // keep `tune`; otherwise setup() takes tune_lookup()
     bool profile_assign = false;  // host loop only: time every assign launch with events
     bool fuse_tiles = true;       // tiled runs: per-tile evolve kernel (see run())
     std::string last_error;

@@ -89,6 +89,29 @@ __device__ __forceinline__ float sqdist_exact(const float* a, const float* b)
     return acc;
 }
 
+// The same distance for two points at once: differences and squares on the
+// packed FP32 pipe of sm_100 (each lane of __fadd2_rn / __fmul2_rn rounds like
+// the scalar op; np[d] holds (-p0[d], -p1[d]) and s + (-p) == s - p exactly),
+// the accumulation in scalar adds.  A packed add whose operand is a packed
+// product is fused into a packed FMA by the compiler even with contraction
+// disabled, which would change the rounding; scalar adds of the product
+// lanes are not.
+template <int DIM>
+__device__ __forceinline__ float2 sqdist2_exact(const float* s, const float2* np)
+{
+    float2 t = __fadd2_rn(make_float2(s[0], s[0]), np[0]);
+    const float2 q0 = __fmul2_rn(t, t);
+    float a0 = q0.x, a1 = q0.y;
+#pragma unroll
+    for (int d = 1; d < DIM; ++d) {
+        t = __fadd2_rn(make_float2(s[d], s[d]), np[d]);
+        const float2 q = __fmul2_rn(t, t);
+        a0 = __fadd_rn(a0, q.x);
+        a1 = __fadd_rn(a1, q.y);
+    }
+    return make_float2(a0, a1);
+}
+
 __device__ __forceinline__ float sqr_rn(float r) { return __fmul_rn(r, r); }
 
 // shift of one coordinate (rd/cpu/brute_force/evolve.hpp:143-177); returns 1

@@ -403,7 +403,9 @@ __global__ void __launch_bounds__(BLOCK) k_assign(EngineView v)
         // reference's rule: lowest index among equal minima.
         constexpr int KB = 8;
         constexpr float FAR = 1e30f;  // padding: (FAR - p)^2 overflows to +inf
+        static_assert(ITEMS % 2 == 0, "points are processed in pairs");
         float p[ITEMS][DIM];
+        float2 np2[ITEMS / 2][DIM];  // negated coordinates of point pairs (2jj, 2jj+1)
         float best[ITEMS];
         int blk[ITEMS];
 #pragma unroll
@@ -414,6 +416,10 @@ __global__ void __launch_bounds__(BLOCK) k_assign(EngineView v)
             best[j] = FLT_MAX;
             blk[j] = -1;
         }
+#pragma unroll
+        for (int jj = 0; jj < ITEMS / 2; ++jj)
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) np2[jj][d] = make_float2(-p[2 * jj][d], -p[2 * jj + 1][d]);
         for (int t0 = 0; t0 < ns; t0 += TS) {
             const int tl = min(TS, ns - t0);
             const int tlp = (tl + KB - 1) / KB * KB;
@@ -433,7 +439,11 @@ __global__ void __launch_bounds__(BLOCK) k_assign(EngineView v)
                     float s[DIM];
                     load_chosen<DIM>(sS, kb + u, s);
 #pragma unroll
-                    for (int j = 0; j < ITEMS; ++j) best[j] = fminf(best[j], sqdist_exact<DIM>(s, p[j]));
+                    for (int jj = 0; jj < ITEMS / 2; ++jj) {
+                        const float2 q = sqdist2_exact<DIM>(s, np2[jj]);
+                        best[2 * jj] = fminf(best[2 * jj], q.x);
+                        best[2 * jj + 1] = fminf(best[2 * jj + 1], q.y);
+                    }
                 }
 #pragma unroll
                 for (int j = 0; j < ITEMS; ++j) blk[j] = (best[j] < old[j]) ? (t0 + kb) : blk[j];
