@@ -36,9 +36,11 @@ sys.path.insert(0, ROOT)
 
 METRIC = "evolve pairs/s"
 UNIT = "pairs/s"
-# DRAM traffic of one k_assign launch on the helix3d_1m workload from ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum); see profiles/.  None = not captured.
-ASSIGN_TRAFFIC_BYTES = None
+# DRAM traffic of one k_assign launch on the helix3d_1m workload from one ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum = 12,039,936 + 0 bytes,
+# profiles/k_assign_helix3d_1m.md); the algorithmic bytes are the 1,000,000
+# points x 12 B read once.  Applies to helix3d_1m only.
+ASSIGN_TRAFFIC_BYTES = {"helix3d_1m": 12_039_936}
 
 
 def parse_args():
@@ -82,7 +84,7 @@ def run_profile(args):
         rd.set_points(dP)
         solve = lambda: rd(r1, r2, n + 1, (64, 64))  # noqa: E731
     else:
-        rdb.autotune(dim, n, max(1, rdb.choose_count(dP, r1)), reps=4)
+        rdb.autotune(dim, n, max(1, rdb.choose_count(dP, r1)), reps=6, points=dP, r1=r1)
         rd = rdb.BruteForceRidgeDetection(n, r1, r2, dim, loop_mode=rdb.LOOP_HOST)
         rd.set_points(dP)
         solve = rd.ridge_detection
@@ -231,7 +233,7 @@ def run_b200_bf(args, world, rank, local):
     # launch shape of the assignment kernel from the project's autotuner, on a
     # synthetic cloud of this size with the chosen count of the first choose
     # (setup, outside every timed region)
-    tb, ti, tus = rdb.autotune(dim, n, max(1, rdb.choose_count(dP, r1)), reps=4)
+    tb, ti, tus = rdb.autotune(dim, n, max(1, rdb.choose_count(dP, r1)), reps=6, points=dP, r1=r1)
     rd = rdb.BruteForceRidgeDetection(n, r1, r2, dim)
     rd.set_points(dP)
 
@@ -344,7 +346,11 @@ def run_b200_bf(args, world, rank, local):
                      "flops_per_pair": flops_per_pair,
                      "assign_ms_per_launch": assign_ms_avg,
                      "assign_launches": pst.assign_launches,
-                     "traffic": ASSIGN_TRAFFIC_BYTES},
+                     # the exact distance takes 9 separately rounded FP32
+                     # operations per pair (no FMA may be used), so the pipe's
+                     # ceiling in these units is half the FMA FLOP rate
+                     "frac_of_nonfused_peak": achieved_tflops / (peak.value / 2),
+                     "traffic": ASSIGN_TRAFFIC_BYTES.get(args.workload)},
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(P.nbytes),
                 "d2h_bytes_per_step": int(ns_final * dim * 4)},
         "gpu_launches": args.steps * (2 + 8 * iters_step),

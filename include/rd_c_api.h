@@ -83,12 +83,15 @@ RD_API rd_status rd_probe_fp32_peak(double* tflops, void* stream);
 RD_API rd_status rd_tune_set(int dim, int64_t n, int block, int items);
 RD_API rd_status rd_tune_get(int dim, int64_t n, int* block, int* items);
 RD_API rd_status rd_tune_reset(void);
-/* Times every supported shape on a synthetic cloud of n uniform points with
- * ns chosen points (assignment kernel, CUDA events, mean over `reps` evolve
- * passes), stores the fastest for (dim, bucket of n) and returns it with its
- * time per launch in microseconds.  Runs on `stream` and waits for it. */
-RD_API rd_status rd_autotune(int dim, int64_t n, int64_t ns, int reps, int* block, int* items,
-                             double* us_per_launch, void* stream);
+/* Times every supported shape on the cloud d_P (device, n x dim ROW_MAJOR;
+ * NULL = n synthetic points uniform in the unit cube) with its first ns points
+ * as the chosen set and assignment radius r1: the assignment kernel is timed
+ * with CUDA events over `reps` evolve passes, twice per shape, keeping each
+ * shape's better mean.  Stores the fastest for (dim, bucket of n) and returns
+ * it with its time per launch in microseconds.  Runs on `stream` and waits
+ * for it; d_P is not modified. */
+RD_API rd_status rd_autotune(int dim, const float* d_P, int64_t n, int64_t ns, float r1, int reps,
+                             int* block, int* items, double* us_per_launch, void* stream);
 
 /* Building block of the evolve step (no reference counterpart; the reference
  * forms the same sums inline, rd/cpu/brute_force/evolve.hpp:71-74): for each

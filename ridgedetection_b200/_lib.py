@@ -64,7 +64,7 @@ SIGNATURES = {
     "rd_tune_set": [ctypes.c_int, ctypes.c_int64, ctypes.c_int, ctypes.c_int],
     "rd_tune_get": [ctypes.c_int, ctypes.c_int64, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
     "rd_tune_reset": [],
-    "rd_autotune": [ctypes.c_int, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
+    "rd_autotune": [ctypes.c_int, _vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_float, ctypes.c_int,
                     ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                     ctypes.POINTER(ctypes.c_double), _vp],
     "rd_ordered_sum": [ctypes.c_int, _vp, _vp, ctypes.c_int64, _vp, ctypes.c_int, _vp],

@@ -330,11 +330,20 @@ def choose_count(P, r1: float) -> int:
     return int(ns.value)
 
 
-def autotune(dim: int, n: int, ns: int, reps: int = 5) -> Tuple[int, int, float]:
-    """Time every supported assignment shape on a synthetic ``dim``-D cloud of
-    ``n`` points with ``ns`` chosen points, keep the fastest for the size
-    bucket of ``n`` and return (block, items, microseconds per launch)."""
+def autotune(dim: int, n: int, ns: int, reps: int = 5, points=None,
+             r1: float = 2.0) -> Tuple[int, int, float]:
+    """Time every supported assignment shape and keep the fastest for the size
+    bucket of ``n``; returns (block, items, microseconds per launch).  With
+    ``points`` (a float32 CUDA tensor, n x dim) the timing runs on that cloud
+    with its first ``ns`` points as the chosen set and radius ``r1``;
+    otherwise on ``n`` synthetic uniform points."""
     b, i, us = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_double(0)
-    L.check(L.lib().rd_autotune(dim, n, ns, reps, ctypes.byref(b), ctypes.byref(i),
-                                ctypes.byref(us), None))
+    ptr = None
+    if points is not None:
+        if not _is_torch_cuda(points):
+            raise TypeError("points must be a CUDA tensor")
+        ptr = ctypes.c_void_p(points.contiguous().data_ptr())
+        n = int(points.shape[0])
+    L.check(L.lib().rd_autotune(dim, ptr, n, ns, float(r1), reps, ctypes.byref(b),
+                                ctypes.byref(i), ctypes.byref(us), None))
     return b.value, i.value, us.value

@@ -278,46 +278,57 @@ rd_status rd_tune_reset(void)
     return RD_OK;
 }
 
-rd_status rd_autotune(int dim, int64_t n, int64_t ns, int reps, int* block, int* items,
-                      double* us_per_launch, void* stream)
+rd_status rd_autotune(int dim, const float* d_P, int64_t n, int64_t ns, float r1, int reps,
+                      int* block, int* items, double* us_per_launch, void* stream)
 {
     if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
     if (!block || !items) return set_err(RD_ERR_ARG, "null argument");
-    if (n < 1 || n > INT32_MAX - 1024 || ns < 1 || ns > n || reps < 1 || reps > 1000)
-        return set_err(RD_ERR_ARG, "need 1 <= ns <= n and 1 <= reps <= 1000");
+    if (n < 1 || n > INT32_MAX - 1024 || ns < 1 || ns > n || reps < 1 || reps > 1000 || !(r1 > 0.0f))
+        return set_err(RD_ERR_ARG, "need 1 <= ns <= n, 1 <= reps <= 1000 and r1 > 0");
     cudaStream_t st = (cudaStream_t)stream;
-    // synthetic cloud: n uniform points in the unit cube, the first ns of them
-    // as the chosen set, r1 large enough that every point is assigned
-    std::vector<float> pts((size_t)n * dim);
-    uint64_t x = 0x9E3779B97F4A7C15ull;
-    for (float& f : pts) {
-        x = x * 6364136223846793005ull + 1442695040888963407ull;
-        f = (float)((x >> 40) & 0xFFFFFF) / 16777216.0f;
+    // without a cloud: n uniform points in the unit cube
+    std::vector<float> pts;
+    if (!d_P) {
+        pts.resize((size_t)n * dim);
+        uint64_t x = 0x9E3779B97F4A7C15ull;
+        for (float& f : pts) {
+            x = x * 6364136223846793005ull + 1442695040888963407ull;
+            f = (float)((x >> 40) & 0xFFFFFF) / 16777216.0f;
+        }
     }
-    double best = -1.0;
-    TuneParams bt{128, 8};
-    for (const TuneParams& tp : tune_candidates()) {
-        if (!tune_supported(dim, tp)) continue;
-        Engine e;
-        e.tune = tp;
-        e.tune_locked = true;
-        e.max_passes = reps;
-        e.profile_assign = true;
-        if (rd_status s = one_cloud_engine(e, dim, n, n, 2.0f, 2.0f)) return s;
-        CK_CUDA(cudaMemcpyAsync(e.points(), pts.data(), sizeof(float) * n * dim, cudaMemcpyHostToDevice, st));
-        CK_CUDA(cudaMemcpyAsync(e.chosen_mut(), pts.data(), sizeof(float) * ns * dim, cudaMemcpyHostToDevice, st));
-        e.given_ns.assign(1, (int32_t)ns);
-        const int rc = e.run(st, false, Engine::RUN_EVOLVE_ONLY);
-        if (rc && rc != RD_ERR_NOT_CONVERGED) return from_engine(rc, e);
-        const RunStats& rs = e.stats();
-        if (rs.assign_launches <= 0) continue;
-        const double us = 1e3 * rs.assign_ms / (double)rs.assign_launches;
-        if (best < 0 || us < best) {
-            best = us;
-            bt = tp;
+    const cudaMemcpyKind kind = d_P ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    const float* src = d_P ? d_P : pts.data();
+    const std::vector<TuneParams>& cand = tune_candidates();
+    std::vector<double> us(cand.size(), -1.0);
+    for (int round = 0; round < 2; ++round) {
+        for (size_t ci = 0; ci < cand.size(); ++ci) {
+            const TuneParams& tp = cand[ci];
+            if (!tune_supported(dim, tp)) continue;
+            Engine e;
+            e.tune = tp;
+            e.tune_locked = true;
+            e.max_passes = reps;
+            e.profile_assign = true;
+            if (rd_status s = one_cloud_engine(e, dim, n, n, r1, r1)) return s;
+            CK_CUDA(cudaMemcpyAsync(e.points(), src, sizeof(float) * n * dim, kind, st));
+            CK_CUDA(cudaMemcpyAsync(e.chosen_mut(), src, sizeof(float) * ns * dim, kind, st));
+            e.given_ns.assign(1, (int32_t)ns);
+            const int rc = e.run(st, false, Engine::RUN_EVOLVE_ONLY);
+            if (rc && rc != RD_ERR_NOT_CONVERGED) return from_engine(rc, e);
+            const RunStats& rs = e.stats();
+            if (rs.assign_launches <= 0) continue;
+            const double t = 1e3 * rs.assign_ms / (double)rs.assign_launches;
+            if (us[ci] < 0 || t < us[ci]) us[ci] = t;
         }
     }
     CK_CUDA(cudaStreamSynchronize(st));
+    double best = -1.0;
+    TuneParams bt{128, 8};
+    for (size_t ci = 0; ci < cand.size(); ++ci)
+        if (us[ci] >= 0 && (best < 0 || us[ci] < best)) {
+            best = us[ci];
+            bt = cand[ci];
+        }
     if (best < 0) return set_err(RD_ERR_CUDA, "no launch shape could be timed");
     tune_store(dim, n, bt);
     *block = bt.block;
