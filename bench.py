@@ -53,6 +53,9 @@ def parse_args():
                     choices=["helix3d_1m", "sine2d_20k", "batch", "spiral2d_10m_tiled"])
     ap.add_argument("--clouds", type=int, default=4096, help="batch workload: number of clouds")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shape", default=None,
+                    help="BLOCK,ITEMS of the assignment kernel instead of the autotuner's pick "
+                         "(a profiler distorts the tuner's timings)")
     ap.add_argument("--profile-run", action="store_true",
                     help="no timing and no JSON line: after --warmup solves, run --steps "
                          "solves with the host-driven loop so that a profiler sees every "
@@ -84,7 +87,10 @@ def run_profile(args):
         rd.set_points(dP)
         solve = lambda: rd(r1, r2, n + 1, (64, 64))  # noqa: E731
     else:
-        rdb.autotune(dim, n, max(1, rdb.choose_count(dP, r1)), reps=6, points=dP, r1=r1)
+        if args.shape:
+            rdb.tune_set(dim, n, *[int(x) for x in args.shape.split(",")])
+        else:
+            rdb.autotune(dim, n, max(1, rdb.choose_count(dP, r1)), reps=6, points=dP, r1=r1)
         rd = rdb.BruteForceRidgeDetection(n, r1, r2, dim, loop_mode=rdb.LOOP_HOST)
         rd.set_points(dP)
         solve = rd.ridge_detection
@@ -188,6 +194,25 @@ def run_reference_arm(args, world, rank):
     if oracle.ref(True) is None:
         print(json.dumps({"impl": "reference",
                           "unavailable": "oracle/_ref/librdref_omp.so was not built"}))
+        return
+    if args.workload == "spiral2d_10m_tiled":
+        vals = []
+        cb = None
+        for _ in range(args.warmup + args.steps):
+            cb = cpu_baseline_tiled(r1, r2)
+            vals.append(cb["value"])
+        val = statistics.mean(vals[args.warmup:])
+        cb["value"] = val
+        print(json.dumps({
+            "impl": "reference", "metric": "tiled ridge points/s", "value": val,
+            "unit": "points/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * 1_000_000 / val, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "cores": cb["cores"]},
+            "cpu_baseline": cb,
+            "e2e": {"value": val, "unit": "points/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+        }))
         return
     S0 = oracle.choose(P, r1)
     threads = os.cpu_count() or 1
@@ -362,6 +387,165 @@ def run_b200_bf(args, world, rank, local):
         torch.distributed.destroy_process_group()
 
 
+def measured_hbm_gbs():
+    """HBM copy bandwidth measured on this pool (MEASURED_PEAKS.json), else the
+    recipe's fallback."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback 6.65 TB/s"
+
+
+def cpu_baseline_tiled(r1, r2, n_sample=1_000_000):
+    """The reference's tiled pipeline (EXT_TILE_TREE_MIXED_RD, OpenMP) on a
+    bounded sample: the same spiral generator at n_sample points, 64x64 tiles."""
+    import oracle
+    from ridgedetection_b200 import generators as G
+    if oracle.ref(True) is None:
+        return None
+    Ps = G.spiral2d(n_sample)
+    threads = os.cpu_count() or 1
+    t = time.perf_counter()
+    oracle.ref_ridge_tiled(Ps, r1, r2, n_sample + 1, (64, 64), threads=threads, openmp=True)
+    dt = time.perf_counter() - t
+    return {"value": n_sample / dt, "unit": "points/s", "cores": threads, "kind": "reference",
+            "sample": f"one OpenMP tiled solve (EXT_TILE_TREE_MIXED_RD) of a {n_sample}-point "
+                      f"spiral from the same generator, 64x64 tiles, {dt:.1f} s"}
+
+
+def run_b200_tiled(args, world, rank, local):
+    """Tiled 10M-point spiral: full solves (device tile build, fused per-tile
+    evolve, global decimation) through the C ABI, replicas across ranks."""
+    import torch
+    import ridgedetection_b200 as rdb
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+    P, r1, r2 = workload(args.workload)
+    n, dim = P.shape
+    tiles = (64, 64)
+    stream = torch.cuda.current_stream()
+    dP = torch.from_numpy(P).to(dev)
+    l2_flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    rd = rdb.TiledRidgeDetection(n, dim)
+    rd.set_points(dP)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+            torch.cuda.synchronize()
+
+    for _ in range(max(3, args.warmup)):
+        rd(r1, r2, n + 1, tiles)
+    torch.cuda.synchronize()
+    st = rd.stats()
+    pairs_step, point_passes = st.pairs, st.point_passes
+
+    clock = ClockSampler(local)
+    clock.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    barrier()
+    for k in range(args.steps):
+        l2_flush.zero_()
+        ev[k][0].record(stream)
+        rd(r1, r2, n + 1, tiles)
+        ev[k][1].record(stream)
+    barrier()
+    clocks = clock.stop()
+    ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
+    ms_t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(ms_t, op=torch.distributed.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    ns_final = rd.ns_
+
+    # e2e: pinned host cloud in, ridge out, both inside the timing
+    hP = torch.from_numpy(P).pin_memory()
+    hout = torch.empty((n, dim), dtype=torch.float32).pin_memory()
+    e2e = []
+    barrier()
+    for k in range(args.steps):
+        l2_flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        rd.set_points(hP.numpy())
+        rd(r1, r2, n + 1, tiles)
+        rd.get_chosen_points(hout[: rd.ns_].numpy())
+        b.record(stream)
+        b.synchronize()
+        e2e.append(a.elapsed_time(b))
+    barrier()
+    e2e_t = torch.tensor([sum(e2e) / len(e2e)], device=dev, dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(e2e_t, op=torch.distributed.ReduceOp.MAX)
+    e2e_ms = float(e2e_t.item())
+
+    # dominant kernel: the fused per-tile evolve, timed per launch in a
+    # host-loop solve.  Algorithmic bytes: every pass of a tile streams its
+    # points (own + halo) once, DIM x 4 B each.
+    rdp = rdb.TiledRidgeDetection(n, dim, loop_mode=rdb.LOOP_HOST)
+    rdp.set_points(dP)
+    rdp.set_profiling(True)
+    rdp(r1, r2, n + 1, tiles)
+    pst = rdp.stats()
+    rdp.close()
+    launches = max(1, pst.assign_launches)
+    kern_ms = pst.assign_ms / launches
+    bytes_launch = pst.point_passes * dim * 4 / launches
+    achieved = bytes_launch / (kern_ms * 1e-3) / 1e9
+    peak, peak_src = measured_hbm_gbs()
+    timers = rd.get_timers()
+    if world > 1:
+        torch.distributed.barrier()
+    rd.close()
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline_tiled(r1, r2)
+        except Exception as e:  # the baseline is reported, never the target
+            cpu = {"value": None, "unit": "points/s", "cores": os.cpu_count(),
+                   "kind": "reference", "sample": f"failed: {e}"}
+    line = {
+        "metric": "tiled ridge points/s", "value": world * n / (ms_max * 1e-3),
+        "unit": "points/s", "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": ms_max, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{args.workload}: tiled (extended tiles, mixed) full solve, "
+                               f"N={n}, dim={dim}, r1={r1}, r2={r2}, 64x64 tiles, "
+                               f"max tile capacity N+1",
+                   "l2": "flushed (256 MiB write) between timed steps",
+                   "loop": "CUDA graph WHILE node", "parallelism": f"replicas x{world}"},
+        "solves_per_s": world * 1e3 / ms_max,
+        "evolve_pairs_per_s": world * pairs_step / (ms_max * 1e-3),
+        "pairs_per_step": pairs_step, "ns_final": ns_final,
+        "timers_ms": timers,
+        "roofline": {"bound": "hbm", "kernel": "k_tile_evolve", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_src,
+                     "bytes_per_launch": bytes_launch, "kernel_ms_per_launch": kern_ms,
+                     "launches": pst.assign_launches, "traffic": None},
+        "e2e": {"value": world * n / (e2e_ms * 1e-3), "unit": "points/s",
+                "h2d_bytes_per_step": int(P.nbytes), "d2h_bytes_per_step": int(ns_final * dim * 4)},
+        "gpu_launches": args.steps * (12 + 10 * max(1, st.loop_iters)),
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
 def run_b200_batch(args, world, rank, local):
     """Batched workload: graph-driven batched solve vs the plain per-cloud loop."""
     import torch
@@ -420,6 +604,8 @@ def main():
         return
     if args.workload == "batch":
         run_b200_batch(args, world, rank, local)
+    elif args.workload == "spiral2d_10m_tiled":
+        run_b200_tiled(args, world, rank, local)
     else:
         run_b200_bf(args, world, rank, local)
 

@@ -63,6 +63,8 @@ typedef struct rd_run_stats {
     int32_t pad;
     double  assign_ms;      /* profiling runs only: summed assign-kernel time (ms)   */
     int64_t assign_launches;/* profiling runs only: assign-kernel launches timed     */
+    double  point_passes;   /* sum over clouds of (points x evolve passes): point   */
+                            /* coordinates the assignment streams, in points        */
 } rd_run_stats;
 
 RD_API const char* rd_last_error(void);
@@ -160,6 +162,10 @@ RD_API rd_status rd_tiled_get_points(rd_tiled* h, float* out, int64_t pitch, int
 RD_API rd_status rd_tiled_get_timers(rd_tiled* h, float* whole, float* build, float* rd_tiles,
                                      float* refinement);
 RD_API rd_status rd_tiled_get_stats(rd_tiled* h, rd_run_stats* st);
+/* enable = 1: host-loop runs time every launch of the fused per-tile evolve
+ * kernel with CUDA events (reported in rd_run_stats.assign_ms /
+ * assign_launches; no reference counterpart) */
+RD_API rd_status rd_tiled_set_profiling(rd_tiled* h, int enable);
 RD_API rd_status rd_tiled_get_leaf_count(rd_tiled* h, int64_t* n_leaves);
 RD_API rd_status rd_tiled_destroy(rd_tiled* h);
 

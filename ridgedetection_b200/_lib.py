@@ -39,7 +39,8 @@ class RunStats(ctypes.Structure):
     _fields_ = [("loop_iters", ctypes.c_int64), ("evolve_passes", ctypes.c_int64),
                 ("max_passes", ctypes.c_int64), ("pairs", ctypes.c_double),
                 ("err_bits", ctypes.c_int32), ("pad", ctypes.c_int32),
-                ("assign_ms", ctypes.c_double), ("assign_launches", ctypes.c_int64)]
+                ("assign_ms", ctypes.c_double), ("assign_launches", ctypes.c_int64),
+                ("point_passes", ctypes.c_double)]
 
 
 class CloudDesc(ctypes.Structure):
@@ -85,6 +86,7 @@ SIGNATURES = {
     "rd_tiled_get_points": [_vp, _vp, _i64, _i, _vp],
     "rd_tiled_get_timers": [_vp, _pf, _pf, _pf, _pf],
     "rd_tiled_get_stats": [_vp, ctypes.POINTER(RunStats)],
+    "rd_tiled_set_profiling": [_vp, _i],
     "rd_tiled_get_leaf_count": [_vp, _pi64],
     "rd_tiled_destroy": [_vp],
     "rd_choose": [_i, _vp, _i64, _f, _vp, _pi64, _vp],

@@ -197,6 +197,10 @@ class TiledRidgeDetection:
         L.check(self._lib.rd_tiled_get_leaf_count(self._h, ctypes.byref(n)))
         return int(n.value)
 
+    def set_profiling(self, enable: bool = True) -> None:
+        """Host-loop runs time every fused tile-evolve launch (stats().assign_ms)."""
+        L.check(self._lib.rd_tiled_set_profiling(self._h, 1 if enable else 0))
+
     def stats(self) -> L.RunStats:
         s = L.RunStats()
         L.check(self._lib.rd_tiled_get_stats(self._h, ctypes.byref(s)))

@@ -154,6 +154,7 @@ void fill_stats(const RunStats& s, rd_run_stats* o)
     o->err_bits = s.err_bits;
     o->assign_ms = s.assign_ms;
     o->assign_launches = s.assign_launches;
+    o->point_passes = s.point_passes;
 }
 
 // independent FMA chains: 8 per thread, ITER rounds
@@ -212,7 +213,7 @@ extern "C" {
 
 const char* rd_last_error(void) { return g_err.c_str(); }
 
-int rd_abi_version(void) { return 1; }
+int rd_abi_version(void) { return 2; }
 
 int rd_supported_dims(void) { return (1 << 2) | (1 << 3); }
 
@@ -492,6 +493,13 @@ rd_status rd_tiled_set_points(rd_tiled* h, const float* pts, int64_t pitch, int 
     h->have_result = false;
     return load_points(pts, h->in_layout, pitch, h->np, h->dim, src_on_device, h->pts.as<float>(),
                        h->staging, (cudaStream_t)stream);
+}
+
+rd_status rd_tiled_set_profiling(rd_tiled* h, int enable)
+{
+    if (!h) return set_err(RD_ERR_ARG, "null handle");
+    h->run.set_profiling(enable != 0);
+    return RD_OK;
 }
 
 rd_status rd_tiled_set_loop_mode(rd_tiled* h, int mode)

@@ -418,7 +418,7 @@ int Engine::run(cudaStream_t st, bool use_graph, int mode)
     int max_ns = 0;
     for (const CloudDesc& cd : h_cl_) max_ns = std::max(max_ns, cd.ns_cap);
     fused_ = fuse_tiles && h_gr_.size() == 1 && h_cl_.size() > 1 && max_ns <= TILE_NS_MAX &&
-             flags_ == 0 && !profile_assign;
+             flags_ == 0;
     const EngineView v = view();
     RD_CK(prepare_pass(dim_, v, tune));
     if (fused_) RD_CK(prepare_tile_pass(dim_, v));
@@ -436,7 +436,7 @@ int Engine::run(cudaStream_t st, bool use_graph, int mode)
         stats_.assign_ms = 0;
         stats_.assign_launches = 0;
         for (;;) {
-            if (fused_) RD_CK(launch_tile_pass(dim_, v, st));
+            if (fused_) RD_CK(launch_tile_pass(dim_, v, st, a0, a1));
             else RD_CK(launch_pass(dim_, v, tune, assign_grid_, st, a0, a1));
             RD_CK(launch_loopcond(v, cudaGraphConditionalHandle(), 0, st));
             int32_t act = 0;
@@ -507,6 +507,7 @@ int Engine::collect(cudaStream_t st)
         stats_.total_passes += tp[c];
         stats_.max_passes = std::max<int64_t>(stats_.max_passes, tp[c]);
         stats_.pairs += (double)pr[c];
+        stats_.point_passes += (double)h_cl_[c].n_all * (double)tp[c];
         stats_.err_bits |= h_err_[c];
     }
     if (stats_.err_bits & (ERRB_EVOLVE_CAP | ERRB_OUTER_CAP | ERRB_DEC_CAP)) {

@@ -145,7 +145,9 @@ cudaError_t launch_set_given(const EngineView& v, int queue_decimation, cudaStre
 // fused per-tile evolve (every active cloud to convergence, one CTA each) +
 // decimation of the groups that became ready; needs every ns <= TILE_NS_MAX
 cudaError_t prepare_tile_pass(int dim, const EngineView& v);
-cudaError_t launch_tile_pass(int dim, const EngineView& v, cudaStream_t st);
+// a0/a1 (optional) are recorded right before and after the tile-evolve kernel
+cudaError_t launch_tile_pass(int dim, const EngineView& v, cudaStream_t st,
+                             cudaEvent_t a0 = nullptr, cudaEvent_t a1 = nullptr);
 cudaError_t launch_decimate(int dim, const EngineView& v, cudaStream_t st);
 // out[d] = ordered FP32 sum of P[idx[i]*dim + d] (method 0 chain, 1 parallel exact)
 cudaError_t launch_ordered_sum(int dim, const float* P, const int32_t* idx, int n, float* out,

@@ -29,6 +29,7 @@ struct RunStats {
     int err_bits = 0;
     double assign_ms = 0;         // host-loop runs with profile_assign: assign kernel time
     int64_t assign_launches = 0;
+    double point_passes = 0;      // sum over clouds of n_all * evolve passes
 };
 
 // Process-wide tuning table: (dim, size bucket) -> assign launch shape.  The

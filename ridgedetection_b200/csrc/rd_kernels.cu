@@ -1659,17 +1659,22 @@ cudaError_t prepare_tile_pass(int dim, const EngineView& v)
     return cudaFuncSetAttribute(k_decimate<3, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, dec_smem_bytes(v));
 }
 
-cudaError_t launch_tile_pass(int dim, const EngineView& v, cudaStream_t st)
+cudaError_t launch_tile_pass(int dim, const EngineView& v, cudaStream_t st, cudaEvent_t a0,
+                             cudaEvent_t a1)
 {
     const int smem = tile_evolve_smem_bytes(dim);
     const int grid = std::max(1, std::min(v.n_clouds, v.n_sms * 3));
     const int dgrid = std::max(1, std::min(v.n_groups, v.n_sms * 2));
     if (dim == 2) {
+        if (a0) cudaEventRecord(a0, st);
         k_tile_evolve<2, 256><<<grid, 256, smem, st>>>(v);
+        if (a1) cudaEventRecord(a1, st);
         launch_decbig<2>(v, st);
         k_decimate<2, 512><<<dgrid, 512, dec_smem_bytes(v), st>>>(v);
     } else if (dim == 3) {
+        if (a0) cudaEventRecord(a0, st);
         k_tile_evolve<3, 256><<<grid, 256, smem, st>>>(v);
+        if (a1) cudaEventRecord(a1, st);
         launch_decbig<3>(v, st);
         k_decimate<3, 512><<<dgrid, 512, dec_smem_bytes(v), st>>>(v);
     } else {

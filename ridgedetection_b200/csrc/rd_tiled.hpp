@@ -45,6 +45,8 @@ public:
     const float* result() const { return bOut_.as<float>(); }  // ns x dim, leaf pre-order
     const TiledTimers& timers() const { return tm_; }
     const RunStats& stats() const { return eng_.stats(); }
+    // host-loop runs time every fused tile-evolve launch (RunStats.assign_ms)
+    void set_profiling(bool on) { eng_.profile_assign = on; }
     std::string last_error;
 
 private:
