@@ -50,7 +50,8 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="helix3d_1m",
-                    choices=["helix3d_1m", "sine2d_20k", "batch", "spiral2d_10m_tiled"])
+                    choices=["helix3d_1m", "sine2d_20k", "batch", "spiral2d_10m_tiled",
+                             "spiral2d_1m_tiled"])
     ap.add_argument("--clouds", type=int, default=4096, help="batch workload: number of clouds")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--shape", default=None,
@@ -72,6 +73,8 @@ def workload(name):
         return G.sine2d(20_000), 0.3, 0.6
     if name == "spiral2d_10m_tiled":
         return G.spiral2d(10_000_000), 0.2, 0.4
+    if name == "spiral2d_1m_tiled":  # small case of the same generator, for profilers
+        return G.spiral2d(1_000_000), 0.2, 0.4
     raise ValueError(name)
 
 
@@ -82,7 +85,7 @@ def run_profile(args):
     P, r1, r2 = workload(args.workload)
     n, dim = P.shape
     dP = torch.from_numpy(P).cuda()
-    if args.workload == "spiral2d_10m_tiled":
+    if args.workload.endswith("_tiled"):
         rd = rdb.TiledRidgeDetection(n, dim, loop_mode=rdb.LOOP_HOST)
         rd.set_points(dP)
         solve = lambda: rd(r1, r2, n + 1, (64, 64))  # noqa: E731
@@ -195,7 +198,7 @@ def run_reference_arm(args, world, rank):
         print(json.dumps({"impl": "reference",
                           "unavailable": "oracle/_ref/librdref_omp.so was not built"}))
         return
-    if args.workload == "spiral2d_10m_tiled":
+    if args.workload.endswith("_tiled"):
         vals = []
         cb = None
         for _ in range(args.warmup + args.steps):
@@ -604,7 +607,7 @@ def main():
         return
     if args.workload == "batch":
         run_b200_batch(args, world, rank, local)
-    elif args.workload == "spiral2d_10m_tiled":
+    elif args.workload.endswith("_tiled"):
         run_b200_tiled(args, world, rank, local)
     else:
         run_b200_bf(args, world, rank, local)
