@@ -21,6 +21,7 @@
 #include <cstddef>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 namespace rd {
 namespace b200 {
@@ -182,5 +183,36 @@ private:
 };
 
 }  // namespace tiled
+
+// rd::orderSamples (rd/cpu/brute_force/order.hpp:45) with the brute-force
+// class's condition (squared distance <= r2*r2), on the device: chains of
+// point indices of the ns x DIM ROW_MAJOR device points dS, each chain front
+// to back.  The reference returns a list of deques of point pointers; the
+// indices here are (pointer - S) / DIM of those.
+inline std::vector<std::vector<int>> orderSamples(const float* dS, int dim, long long ns, float r2,
+                                                  cudaStream_t stream = nullptr)
+{
+    std::vector<std::vector<int>> chains;
+    int32_t* dOrder = nullptr;
+    int32_t* dStart = nullptr;
+    check_cuda(cudaMalloc(&dOrder, sizeof(int32_t) * (size_t)(ns + 1)));
+    check_cuda(cudaMalloc(&dStart, sizeof(int32_t) * (size_t)(ns + 1)));
+    int64_t nch = 0;
+    const rd_status s = rd_order_chains(dim, dS, ns, r2, dOrder, dStart, &nch, stream);
+    std::vector<int32_t> order((size_t)ns), start((size_t)nch + 1);
+    if (s == RD_OK) {
+        check_cuda(cudaMemcpy(order.data(), dOrder, sizeof(int32_t) * (size_t)ns,
+                              cudaMemcpyDeviceToHost));
+        check_cuda(cudaMemcpy(start.data(), dStart, sizeof(int32_t) * (size_t)(nch + 1),
+                              cudaMemcpyDeviceToHost));
+    }
+    cudaFree(dOrder);
+    cudaFree(dStart);
+    check(s);
+    for (int64_t c = 0; c < nch; ++c)
+        chains.emplace_back(order.begin() + start[(size_t)c], order.begin() + start[(size_t)c + 1]);
+    return chains;
+}
+
 }  // namespace b200
 }  // namespace rd

@@ -95,6 +95,19 @@ RD_API rd_status rd_tune_reset(void);
 RD_API rd_status rd_autotune(int dim, const float* d_P, int64_t n, int64_t ns, float r1, int reps,
                              int* block, int* items, double* us_per_launch, void* stream);
 
+/* Orders a ridge into chains: rd::orderSamples (rd/cpu/brute_force/order.hpp:45)
+ * with the condition of the brute-force class's order_ option
+ * (ridge_detection.inl:148-168), squared distance <= r2*r2.  Every remaining
+ * point, in index order, seeds a chain that then takes the first later
+ * remaining point within r2 of its front (tested first) or back, until none
+ * is left.  d_S: ns x dim ROW_MAJOR device points.  d_order (ns ints)
+ * receives the point indices chain by chain, each chain front to back;
+ * d_chain_start (ns + 1 ints) the offset of every chain plus the total; the
+ * chain count goes to *n_chains (host).  Identical to the reference's chains.
+ * Runs on `stream` and waits for it. */
+RD_API rd_status rd_order_chains(int dim, const float* d_S, int64_t ns, float r2, int32_t* d_order,
+                                 int32_t* d_chain_start, int64_t* n_chains, void* stream);
+
 /* Building block of the evolve step (no reference counterpart; the reference
  * forms the same sums inline, rd/cpu/brute_force/evolve.hpp:71-74): for each
  * coordinate d < dim, out[d] = the left-to-right FP32 sum, starting from 0 with

@@ -76,6 +76,8 @@ def lib():
                                       ctypes.POINTER(Stats)]
         L.rdo_hausdorff.restype = ctypes.c_double
         L.rdo_hausdorff.argtypes = [_F, _i64, _F, _i64, _int]
+        L.rdo_order.restype = _i64
+        L.rdo_order.argtypes = [_F, _i64, _int, _flt, _I32, _I32]
         L.rdo_evolve_adjoint.restype = _int
         L.rdo_evolve_adjoint.argtypes = [_F, _i64, _F, _i64, _int, _flt, _int, _D, _D, _D, _F]
         _lib = L
@@ -103,6 +105,8 @@ def ref(openmp: bool = False):
             L.ref_decimate_nocopy.argtypes = [_F, _i64, _I64, _int, _flt]
             L.ref_bf_ridge.restype = _i64
             L.ref_bf_ridge.argtypes = [_F, _i64, _int, _flt, _flt, _F, _int]
+            L.ref_order.restype = _i64
+            L.ref_order.argtypes = [_F, _i64, _int, _flt, _I32, _I32]
             L.ref_tiled_ridge.restype = _i64
             L.ref_tiled_ridge.argtypes = [_F, _i64, _int, _flt, _flt, _i64, _I64, _int, _int,
                                           _F, _F]
@@ -283,3 +287,25 @@ def ref_ridge_tiled(P, r1, r2, max_tile_capacity, tiles_per_dim, threads=1, open
     ns = L.ref_tiled_ridge(_fp(P), P.shape[0], P.shape[1], r1, r2, max_tile_capacity,
                            tpd.ctypes.data_as(_I64), threads, 0, _fp(S), _fp(times))
     return S[:ns].copy(), times
+
+
+def order(S, r2):
+    """Greedy chains of order.hpp:45-141: (order, chain_start) int32 arrays."""
+    S = _f32(S)
+    ns = S.shape[0]
+    o = np.empty(max(ns, 1), np.int32)
+    cs = np.empty(ns + 1, np.int32)
+    nch = lib().rdo_order(_fp(S), ns, S.shape[1], r2,
+                          o.ctypes.data_as(_I32), cs.ctypes.data_as(_I32))
+    return o[:ns].copy(), cs[:nch + 1].copy()
+
+
+def ref_order(S, r2):
+    """The same chains from the reference's own rd::orderSamples."""
+    L = ref(False)
+    S = _f32(S)
+    ns = S.shape[0]
+    o = np.empty(max(ns, 1), np.int32)
+    cs = np.empty(ns + 1, np.int32)
+    nch = L.ref_order(_fp(S), ns, S.shape[1], r2, o.ctypes.data_as(_I32), cs.ctypes.data_as(_I32))
+    return o[:ns].copy(), cs[:nch + 1].copy()

@@ -580,3 +580,50 @@ int rdo_evolve_adjoint(const float* P, int64_t np, const float* S0, int64_t ns, 
     free(keys); free(cnt); free(S); free(sums); free(g);
     return 0;
 }
+
+/* ------------------------------------------------------------------------- */
+/* rd/cpu/brute_force/order.hpp:45-141 (orderSamples) with the condition of   */
+/* ridge_detection.inl:148-168 (squared distance <= r2*r2): greedy chains.     */
+/* Every remaining point, in index order, seeds a chain; the chain then takes  */
+/* the first later remaining point within r2 of its front (tested first) or of */
+/* its back, again and again.  order[] receives every chain front to back,     */
+/* chain_start[] the offsets (n_chains + 1 entries).  Returns n_chains.        */
+/* ------------------------------------------------------------------------- */
+int64_t rdo_order(const float* S, int64_t ns, int dim, float r2, int32_t* order,
+                  int32_t* chain_start)
+{
+    const float rsq = r2 * r2;
+    unsigned char* alive = (unsigned char*)malloc((size_t)ns + 1);
+    int32_t* deq = (int32_t*)malloc(sizeof(int32_t) * (size_t)(2 * ns + 1));
+    memset(alive, 1, (size_t)ns + 1);
+    int64_t out = 0, nch = 0;
+    for (int64_t p = 0; p < ns; ++p) {
+        if (!alive[p]) continue;
+        alive[p] = 0;
+        int64_t head = ns, tail = ns;
+        deq[ns] = (int32_t)p;
+        for (;;) {
+            int64_t hit = -1;
+            int front = 0;
+            for (int64_t j = p + 1; j < ns; ++j) {
+                if (!alive[j]) continue;
+                if (sqdist(S + j * dim, S + (int64_t)deq[head] * dim, dim) <= rsq) {
+                    hit = j; front = 1; break;
+                }
+                if (sqdist(S + j * dim, S + (int64_t)deq[tail] * dim, dim) <= rsq) {
+                    hit = j; break;
+                }
+            }
+            if (hit < 0) break;
+            alive[hit] = 0;
+            if (front) deq[--head] = (int32_t)hit;
+            else deq[++tail] = (int32_t)hit;
+        }
+        chain_start[nch++] = (int32_t)out;
+        for (int64_t k = head; k <= tail; ++k) order[out++] = deq[k];
+    }
+    chain_start[nch] = (int32_t)out;
+    free(alive);
+    free(deq);
+    return nch;
+}

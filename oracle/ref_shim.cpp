@@ -29,6 +29,7 @@
 #include "rd/cpu/brute_force/evolve.hpp"
 #include "rd/cpu/brute_force/decimate.hpp"
 #include "rd/cpu/tiled/rd_tiled.hpp"
+#include "rd/cpu/brute_force/order.hpp"
 
 #include <cstdint>
 #include <cstring>
@@ -215,6 +216,26 @@ int64_t ref_tiled_ridge(const float* P, int64_t np, int dim, float r1, float r2,
     }
     std::memcpy(S_out, dp.S.data(), dp.S.size() * sizeof(float));
     return (int64_t)dp.ns;
+}
+
+// rd::orderSamples (rd/cpu/brute_force/order.hpp:45) with the condition the
+// brute-force class passes (ridge_detection.inl:148-168); chains flattened to
+// point indices, front to back, with their start offsets.
+int64_t ref_order(const float* S, int64_t ns, int dim, float r2, int32_t* order,
+                  int32_t* chain_start)
+{
+    const float r2Sqr = r2 * r2;
+    auto chains = rd::orderSamples<float>(S, (size_t)dim, (size_t)ns,
+        [&r2Sqr](float const* p1, float const* p2, size_t d) -> bool {
+            return rd::squareEuclideanDistance(p1, p2, d) <= r2Sqr;
+        });
+    int64_t out = 0, nch = 0;
+    for (const auto& ch : chains) {
+        chain_start[nch++] = (int32_t)out;
+        for (const float* q : ch) order[out++] = (int32_t)((q - S) / dim);
+    }
+    chain_start[nch] = (int32_t)out;
+    return nch;
 }
 
 }  // extern "C"

@@ -8,11 +8,11 @@ from . import generators  # noqa: F401
 from ._lib import RDError, RunStats, lib  # noqa: F401
 from .api import (COL_MAJOR, LOOP_GRAPH, LOOP_HOST, ROW_MAJOR,  # noqa: F401
                   BatchedRidgeDetection, BruteForceRidgeDetection, TiledRidgeDetection,
-                  autotune, choose_count, pack_clouds, ridge_detection,
+                  autotune, choose_count, order_chains, pack_clouds, ridge_detection,
                   tiled_ridge_detection, tune_get, tune_reset, tune_set)
 
 __all__ = ["BruteForceRidgeDetection", "BatchedRidgeDetection", "TiledRidgeDetection",
            "ridge_detection", "tiled_ridge_detection",
-           "pack_clouds", "autotune", "choose_count", "tune_get", "tune_set", "tune_reset",
+           "pack_clouds", "order_chains", "autotune", "choose_count", "tune_get", "tune_set", "tune_reset",
            "ROW_MAJOR", "COL_MAJOR", "LOOP_GRAPH", "LOOP_HOST", "RDError",
            "RunStats", "lib", "generators"]

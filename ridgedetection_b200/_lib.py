@@ -68,6 +68,7 @@ SIGNATURES = {
     "rd_autotune": [ctypes.c_int, _vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_float, ctypes.c_int,
                     ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                     ctypes.POINTER(ctypes.c_double), _vp],
+    "rd_order_chains": [_i, _vp, _i64, _f, _vp, _vp, _pi64, _vp],
     "rd_ordered_sum": [ctypes.c_int, _vp, _vp, ctypes.c_int64, _vp, ctypes.c_int, _vp],
     "rd_bf_create": [ctypes.POINTER(_vp), _i, _i, _i, _i64, _f, _f],
     "rd_bf_set_points": [_vp, _vp, _i64, _i, _vp],

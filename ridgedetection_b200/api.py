@@ -351,3 +351,24 @@ def autotune(dim: int, n: int, ns: int, reps: int = 5, points=None,
     L.check(L.lib().rd_autotune(dim, ptr, n, ns, float(r1), reps, ctypes.byref(b),
                                 ctypes.byref(i), ctypes.byref(us), None))
     return b.value, i.value, us.value
+
+
+def order_chains(S, r2: float):
+    """Order a ridge into chains (rd::orderSamples, rd/cpu/brute_force/order.hpp:45,
+    with the brute-force class's condition: squared distance <= r2*r2).
+    S: n x dim float32 points (numpy or CUDA tensor).  Returns (order,
+    chain_start) as numpy int32 arrays: the point indices chain by chain,
+    each front to back, and the chain offsets (n_chains + 1 entries)."""
+    import torch
+    dS = S if _is_torch_cuda(S) else torch.from_numpy(np.ascontiguousarray(S, np.float32)).cuda()
+    ns = int(dS.shape[0])
+    dim = int(dS.shape[1]) if dS.dim() == 2 else 2
+    order = torch.empty(max(ns, 1), dtype=torch.int32, device=dS.device)
+    starts = torch.empty(ns + 1, dtype=torch.int32, device=dS.device)
+    nch = ctypes.c_int64(0)
+    stream = torch.cuda.current_stream(dS.device).cuda_stream
+    L.check(L.lib().rd_order_chains(dim, ctypes.c_void_p(dS.data_ptr()), ns, float(r2),
+                                    ctypes.c_void_p(order.data_ptr()),
+                                    ctypes.c_void_p(starts.data_ptr()), ctypes.byref(nch),
+                                    ctypes.c_void_p(stream)))
+    return order[:ns].cpu().numpy(), starts[: nch.value + 1].cpu().numpy()

@@ -338,6 +338,31 @@ rd_status rd_autotune(int dim, const float* d_P, int64_t n, int64_t ns, float r1
     return RD_OK;
 }
 
+rd_status rd_order_chains(int dim, const float* d_S, int64_t ns, float r2, int32_t* d_order,
+                          int32_t* d_chain_start, int64_t* n_chains, void* stream)
+{
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (!d_chain_start || !n_chains || (ns > 0 && (!d_S || !d_order)))
+        return set_err(RD_ERR_ARG, "null argument");
+    if (ns < 0 || ns > INT32_MAX / 2 - 1 || !(r2 > 0.0f)) return set_err(RD_ERR_ARG, "bad ns or r2");
+    cudaStream_t st = (cudaStream_t)stream;
+    *n_chains = 0;
+    thread_local DevBuf& alive = *new DevBuf();  // never destroyed: no CUDA calls at exit
+    thread_local DevBuf& deq = *new DevBuf();
+    thread_local DevBuf& cnt = *new DevBuf();
+    CK_CUDA(alive.ensure((size_t)ns + 16));
+    CK_CUDA(deq.ensure(sizeof(int32_t) * (size_t)(2 * ns + 1)));
+    CK_CUDA(cnt.ensure(sizeof(int32_t)));
+    const float rsq = r2 * r2;
+    CK_CUDA(launch_order_chains(dim, d_S, (int)ns, rsq, alive.as<unsigned char>(), deq.as<int32_t>(),
+                                d_order, d_chain_start, cnt.as<int32_t>(), st));
+    int32_t h = 0;
+    CK_CUDA(cudaMemcpyAsync(&h, cnt.p, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    CK_CUDA(cudaStreamSynchronize(st));
+    *n_chains = h;
+    return RD_OK;
+}
+
 rd_status rd_ordered_sum(int dim, const float* d_P, const int32_t* d_idx, int64_t n,
                          float* d_out, int method, void* stream)
 {

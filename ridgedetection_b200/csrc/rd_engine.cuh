@@ -149,6 +149,11 @@ cudaError_t prepare_tile_pass(int dim, const EngineView& v);
 cudaError_t launch_tile_pass(int dim, const EngineView& v, cudaStream_t st,
                              cudaEvent_t a0 = nullptr, cudaEvent_t a1 = nullptr);
 cudaError_t launch_decimate(int dim, const EngineView& v, cudaStream_t st);
+// chains of a ridge (rd_order.cu): alive ns bytes, deq 2*ns+1 ints of scratch;
+// order ns ints, chain_start ns+1 ints, n_chains one int (all device)
+cudaError_t launch_order_chains(int dim, const float* S, int ns, float rsq, unsigned char* alive,
+                                int32_t* deq, int32_t* order, int32_t* chain_start,
+                                int32_t* n_chains, cudaStream_t st);
 // out[d] = ordered FP32 sum of P[idx[i]*dim + d] (method 0 chain, 1 parallel exact)
 cudaError_t launch_ordered_sum(int dim, const float* P, const int32_t* idx, int n, float* out,
                                int method, cudaStream_t st);

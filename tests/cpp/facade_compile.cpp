@@ -17,6 +17,13 @@ static void use_bf()
     rd2.ridgeDetection();
 }
 
+static void use_order()
+{
+    float* dS = nullptr;
+    auto chains = orderSamples(dS, 3, 0, 0.3f);
+    (void)chains.size();
+}
+
 static void use_tiled()
 {
     std::vector<float> pts(2000, 0.f);
@@ -33,6 +40,7 @@ int main(int argc, char**)
     if (argc > 99) {
         use_bf();
         use_tiled();
+        use_order();
     }
     return 0;
 }

@@ -107,3 +107,26 @@ def test_adjoint_oracle_matches_finite_differences():
         Pm[i, d] -= h
         fd = (fwd64(Pp, S064) - fwd64(Pm, S064)) / (2 * h)
         assert abs(fd - gP[i, d]) <= 1e-8 + 1e-6 * abs(fd)
+
+
+def _order_cases():
+    from ridgedetection_b200 import generators as G
+    r = np.random.default_rng(1)
+    S1, _ = O.ridge_bf(G.sine2d(20000, seed=3), 0.3, 0.6)
+    return [("sine_ridge", S1, 0.6),
+            ("random_2d", r.random((3000, 2)).astype(np.float32), 0.03),
+            ("random_3d", r.random((2000, 3)).astype(np.float32), 0.08),
+            ("duplicates", np.repeat(r.random((50, 3)).astype(np.float32), 4, axis=0), 0.05),
+            ("one", np.zeros((1, 2), np.float32), 0.1),
+            ("empty", np.zeros((0, 2), np.float32), 0.1)]
+
+
+@pytest.mark.parametrize("case", _order_cases(), ids=lambda c: c[0])
+def test_order_restatement_matches_reference(case):
+    """rd_oracle.c rdo_order == the reference's own rd::orderSamples."""
+    if O.ref(False) is None:
+        pytest.skip("oracle/_ref not built")
+    _, S, r2 = case
+    a, b = O.order(S, r2), O.ref_order(S, r2)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    assert sorted(a[0].tolist()) == list(range(S.shape[0]))   # a permutation
