@@ -123,7 +123,6 @@ template <int DIM, DataMemoryLayout IN_MEM_LAYOUT, DataMemoryLayout OUT_MEM_LAYO
           RidgeDetectionAlgorithm ALG = RD_BRUTE_FORCE, TiledRidgeDetectionPolicy POLICY = RD_MIXED,
           TileType TILE = RD_EXTENDED_TILE, typename T = float>
 class RidgeDetection {
-    static_assert(POLICY == RD_MIXED, "only the mixed (global decimation) policy is provided");
     static_assert(sizeof(T) == 4, "float only");
 
 public:
@@ -137,6 +136,7 @@ public:
         check(rd_tiled_create(&h_, DIM, RD_ROW_MAJOR,
                               OUT_MEM_LAYOUT == COL_MAJOR ? RD_COL_MAJOR : RD_ROW_MAJOR, pointsNum));
         check(rd_tiled_set_points(h_, inputPoints, 0, 0, nullptr));
+        check(rd_tiled_set_policy(h_, POLICY == RD_LOCAL ? RD_TILED_LOCAL : RD_TILED_MIXED));
     }
     ~RidgeDetection()
     {

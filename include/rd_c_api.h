@@ -155,8 +155,11 @@ RD_API rd_status rd_bf_destroy(rd_bf* h);
  *   getTimers()                  -> rd_tiled_get_timers
  * The result is that of the reference CPU implementation
  * rd::tiled::tiledRidgeDetection<EXT_TILE_TREE_MIXED_RD> (rd/cpu/tiled/rd_tiled.hpp:1217-1374):
- * leaf tiles in pre-order, each tile's chosen points in order.  Only
- * end_phase_refinement = 0 is supported (RD_ERR_UNSUPPORTED otherwise).
+ * leaf tiles in pre-order, each tile's chosen points in order.  With
+ * end_phase_refinement = 1 that result is then refined as rd_tiled.hpp:1386-1419
+ * does: a brute-force decimation of the whole set (r2), then an evolve of the
+ * entire cloud against the survivors to convergence (r1); the refinement time
+ * is the fourth timer.
  * ------------------------------------------------------------------------- */
 typedef struct rd_tiled rd_tiled;
 RD_API rd_status rd_tiled_create(rd_tiled** out, int dim, int in_layout, int out_layout,
@@ -164,6 +167,16 @@ RD_API rd_status rd_tiled_create(rd_tiled** out, int dim, int in_layout, int out
 RD_API rd_status rd_tiled_set_points(rd_tiled* h, const float* pts, int64_t pitch,
                                      int src_on_device, void* stream);
 RD_API rd_status rd_tiled_set_loop_mode(rd_tiled* h, int mode);
+/* Tile policy, the reference's template argument RD_MIXED / RD_LOCAL
+ * (agent_tiled_ridge_detection.cuh:70-90).  RD_TILED_MIXED (default): evolve
+ * inside every leaf, decimate globally over all leaves (results as the CPU
+ * EXT_TILE_TREE_MIXED_RD).  RD_TILED_LOCAL: a complete ridge detection inside
+ * every leaf -- choose over its own points, then evolve over its own and halo
+ * points and brute-force decimation until its count stops changing
+ * (:232-331 and dispatch_ridge_detection.cuh) -- with the leaves' results in
+ * leaf pre-order; the reference appends them in completion order. */
+enum { RD_TILED_MIXED = 0, RD_TILED_LOCAL = 1 };
+RD_API rd_status rd_tiled_set_policy(rd_tiled* h, int policy);
 RD_API rd_status rd_tiled_run(rd_tiled* h, float r1, float r2, int64_t max_tile_capacity,
                               const int32_t* tiles_per_dim, int end_phase_refinement,
                               void* stream);

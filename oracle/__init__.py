@@ -76,6 +76,10 @@ def lib():
                                       ctypes.POINTER(Stats)]
         L.rdo_hausdorff.restype = ctypes.c_double
         L.rdo_hausdorff.argtypes = [_F, _i64, _F, _i64, _int]
+        L.rdo_ridge_tiled_policy.restype = _i64
+        L.rdo_ridge_tiled_policy.argtypes = [_F, _i64, _int, _flt, _flt, _i64, _I64, _int, _F,
+                                             ctypes.POINTER(ctypes.c_int64),
+                                             ctypes.POINTER(Stats)]
         L.rdo_order.restype = _i64
         L.rdo_order.argtypes = [_F, _i64, _int, _flt, _I32, _I32]
         L.rdo_evolve_adjoint.restype = _int
@@ -182,7 +186,34 @@ def ridge_bf(P, r1, r2):
     return S[:ns].copy(), st
 
 
-def ridge_tiled(P, r1, r2, max_tile_capacity, tiles_per_dim):
+def ridge_tiled_local(P, r1, r2, max_tile_capacity, tiles_per_dim, refine=False):
+    """RD_LOCAL tile policy: a full ridge detection inside every leaf."""
+    P = _f32(P)
+    S = np.zeros_like(P)
+    tpd = np.ascontiguousarray(tiles_per_dim, dtype=np.int64)
+    nl = ctypes.c_int64(0)
+    st = Stats()
+    ns = lib().rdo_ridge_tiled_policy(_fp(P), P.shape[0], P.shape[1], r1, r2, max_tile_capacity,
+                                      tpd.ctypes.data_as(_I64), 1, _fp(S), ctypes.byref(nl),
+                                      ctypes.byref(st))
+    if ns < 0:
+        raise RuntimeError("tile subdivision did not terminate")
+    S = S[:ns].copy()
+    if refine and ns > 0:
+        S = decimate(S, r2)
+        S, _ = evolve(P, S, r1)
+    return S, st, nl.value
+
+
+def ridge_tiled(P, r1, r2, max_tile_capacity, tiles_per_dim, refine=False):
+    """EXT_TILE_TREE_MIXED_RD; with refine, the end-phase refinement of
+    rd_tiled.hpp:1386-1419 (brute-force decimate, then evolve of the whole
+    cloud) composed of the restated decimate and evolve."""
+    if refine:
+        S, st, nl = ridge_tiled(P, r1, r2, max_tile_capacity, tiles_per_dim)
+        S = decimate(S, r2)
+        S, _ = evolve(P, S, r1)
+        return S, st, nl
     P = _f32(P)
     S = np.zeros_like(P)
     tpd = np.ascontiguousarray(tiles_per_dim, dtype=np.int64)
@@ -278,14 +309,16 @@ def ref_ridge_bf(P, r1, r2, threads=0, openmp=False):
     return S[:ns].copy()
 
 
-def ref_ridge_tiled(P, r1, r2, max_tile_capacity, tiles_per_dim, threads=1, openmp=False):
+def ref_ridge_tiled(P, r1, r2, max_tile_capacity, tiles_per_dim, threads=1, openmp=False,
+                    refine=False):
     L = ref(openmp)
     P = _f32(P)
     S = np.zeros_like(P)
     tpd = np.ascontiguousarray(tiles_per_dim, dtype=np.int64)
     times = np.zeros(4, np.float32)
     ns = L.ref_tiled_ridge(_fp(P), P.shape[0], P.shape[1], r1, r2, max_tile_capacity,
-                           tpd.ctypes.data_as(_I64), threads, 0, _fp(S), _fp(times))
+                           tpd.ctypes.data_as(_I64), threads, 1 if refine else 0, _fp(S),
+                           _fp(times))
     return S[:ns].copy(), times
 
 

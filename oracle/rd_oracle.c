@@ -409,6 +409,21 @@ int64_t rdo_ridge_tiled(const float* P, int64_t np, int dim, float r1, float r2,
                         int64_t max_tile_capacity, const int64_t* tiles_per_dim,
                         float* S, int64_t* n_leaves, rdo_stats* st)
 {
+    return rdo_ridge_tiled_policy(P, np, dim, r1, r2, max_tile_capacity, tiles_per_dim, 0, S,
+                                  n_leaves, st);
+}
+
+/* local = 0: EXT_TILE_TREE_MIXED_RD (rd_tiled.hpp:1217-1374), local evolve and
+ * a global decimateNoCopy.  local = 1: the RD_LOCAL policy of the GPU
+ * reference (agent_tiled_ridge_detection.cuh:232-331 over the same extended
+ * tiles; dispatch_ridge_detection.cuh doApproximate): every leaf on its own,
+ * choose over its own points, then (evolve over own + halo points; brute-force
+ * decimate) until its count stops changing; results in leaf preorder (the
+ * reference appends leaves in completion order). */
+int64_t rdo_ridge_tiled_policy(const float* P, int64_t np, int dim, float r1, float r2,
+                               int64_t max_tile_capacity, const int64_t* tiles_per_dim,
+                               int local, float* S, int64_t* n_leaves, rdo_stats* st)
+{
     if (st) memset(st, 0, sizeof(*st));
     if (np <= 0 || dim < 1 || dim > 8) return 0;
     /* rd/utils/bounding_box.hpp:126-197 (findBounds, serial) */
@@ -464,6 +479,19 @@ int64_t rdo_ridge_tiled(const float* P, int64_t np, int dim, float r1, float r2,
 
     float* gS = (float*)malloc(sizeof(float) * (size_t)(ns * dim + 1));
     int64_t old = 0;
+    if (local) {
+        for (int64_t l = 0; l < nl; ++l) {
+            int64_t oldc = 0;
+            while (oldc != nch[l]) {
+                oldc = nch[l];
+                double pairs = 0;
+                int64_t passes = rdo_evolve(pts[l], npts[l], chosen[l], nch[l], dim, r1, 0, &pairs);
+                if (st) { st->evolve_passes += passes; st->pairs += pairs; st->outer_iters++; }
+                nch[l] = rdo_decimate(chosen[l], nch[l], dim, r2);
+            }
+        }
+        old = ns;  /* skips the global loop */
+    }
     while (old != ns) {
         old = ns;
         /* evolve each leaf against its own chosen set (rd_tiled.hpp:1322-1332) */

@@ -56,6 +56,9 @@ int64_t rdo_ridge_tiled(const float* P, int64_t np, int dim, float r1, float r2,
                         float* S, int64_t* n_leaves, rdo_stats* st);
 
 double rdo_hausdorff(const float* A, int64_t na, const float* B, int64_t nb, int dim);
+int64_t rdo_ridge_tiled_policy(const float* P, int64_t np, int dim, float r1, float r2,
+                               int64_t max_tile_capacity, const int64_t* tiles_per_dim,
+                               int local, float* S, int64_t* n_leaves, rdo_stats* st);
 int64_t rdo_order(const float* S, int64_t ns, int dim, float r2, int32_t* order,
                   int32_t* chain_start);
 

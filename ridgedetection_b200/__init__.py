@@ -6,7 +6,8 @@ mirror of the reference's interface; it never falls back to a CPU path.
 """
 from . import generators  # noqa: F401
 from ._lib import RDError, RunStats, lib  # noqa: F401
-from .api import (COL_MAJOR, LOOP_GRAPH, LOOP_HOST, ROW_MAJOR,  # noqa: F401
+from .api import (COL_MAJOR, LOOP_GRAPH, LOOP_HOST, ROW_MAJOR, TILED_LOCAL,  # noqa: F401
+                  TILED_MIXED,
                   BatchedRidgeDetection, BruteForceRidgeDetection, TiledRidgeDetection,
                   autotune, choose_count, order_chains, pack_clouds, ridge_detection,
                   tiled_ridge_detection, tune_get, tune_reset, tune_set)
@@ -14,5 +15,5 @@ from .api import (COL_MAJOR, LOOP_GRAPH, LOOP_HOST, ROW_MAJOR,  # noqa: F401
 __all__ = ["BruteForceRidgeDetection", "BatchedRidgeDetection", "TiledRidgeDetection",
            "ridge_detection", "tiled_ridge_detection",
            "pack_clouds", "order_chains", "autotune", "choose_count", "tune_get", "tune_set", "tune_reset",
-           "ROW_MAJOR", "COL_MAJOR", "LOOP_GRAPH", "LOOP_HOST", "RDError",
+           "ROW_MAJOR", "TILED_MIXED", "TILED_LOCAL", "COL_MAJOR", "LOOP_GRAPH", "LOOP_HOST", "RDError",
            "RunStats", "lib", "generators"]

@@ -82,6 +82,7 @@ SIGNATURES = {
     "rd_tiled_create": [ctypes.POINTER(_vp), _i, _i, _i, _i64],
     "rd_tiled_set_points": [_vp, _vp, _i64, _i, _vp],
     "rd_tiled_set_loop_mode": [_vp, _i],
+    "rd_tiled_set_policy": [_vp, _i],
     "rd_tiled_run": [_vp, _f, _f, _i64, ctypes.POINTER(ctypes.c_int32), _i, _vp],
     "rd_tiled_get_count": [_vp, _pi64],
     "rd_tiled_get_points": [_vp, _vp, _i64, _i, _vp],

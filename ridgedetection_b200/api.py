@@ -25,6 +25,8 @@ ROW_MAJOR = L.RD_ROW_MAJOR
 COL_MAJOR = L.RD_COL_MAJOR
 LOOP_GRAPH = L.RD_LOOP_GRAPH
 LOOP_HOST = L.RD_LOOP_HOST
+TILED_MIXED = 0
+TILED_LOCAL = 1
 
 
 def _is_torch_cuda(x) -> bool:
@@ -197,6 +199,11 @@ class TiledRidgeDetection:
         L.check(self._lib.rd_tiled_get_leaf_count(self._h, ctypes.byref(n)))
         return int(n.value)
 
+    def set_policy(self, policy: int) -> None:
+        """TILED_MIXED (default: global decimation over all leaves) or
+        TILED_LOCAL (a complete ridge detection inside every leaf)."""
+        L.check(self._lib.rd_tiled_set_policy(self._h, int(policy)))
+
     def set_profiling(self, enable: bool = True) -> None:
         """Host-loop runs time every fused tile-evolve launch (stats().assign_ms)."""
         L.check(self._lib.rd_tiled_set_profiling(self._h, 1 if enable else 0))
@@ -219,12 +226,16 @@ class TiledRidgeDetection:
 
 
 def tiled_ridge_detection(P: np.ndarray, r1: float, r2: float, max_tile_capacity: int,
-                          tiles_per_dim: Sequence[int], loop_mode: int = LOOP_GRAPH):
-    """Tiled ridge of one ROW_MAJOR float32 cloud; returns (S, stats, n_leaves)."""
+                          tiles_per_dim: Sequence[int], loop_mode: int = LOOP_GRAPH,
+                          end_phase_refinement: bool = False, policy: int = TILED_MIXED):
+    """Tiled ridge of one ROW_MAJOR float32 cloud; returns (S, stats, n_leaves).
+    With end_phase_refinement the result is refined as rd_tiled.hpp:1386-1419
+    does (brute-force decimation, then an evolve of the whole cloud)."""
     P = np.ascontiguousarray(P, dtype=np.float32)
     rd = TiledRidgeDetection(P.shape[0], P.shape[1], P, loop_mode=loop_mode)
     try:
-        rd(r1, r2, max_tile_capacity, tiles_per_dim)
+        rd.set_policy(policy)
+        rd(r1, r2, max_tile_capacity, tiles_per_dim, end_phase_refinement=end_phase_refinement)
         return rd.get_chosen_points(), rd.stats(), rd.leaf_count()
     finally:
         rd.close()

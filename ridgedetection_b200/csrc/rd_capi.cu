@@ -5,6 +5,7 @@
 #include "rd_adjoint.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -527,6 +528,14 @@ rd_status rd_tiled_set_profiling(rd_tiled* h, int enable)
     return RD_OK;
 }
 
+rd_status rd_tiled_set_policy(rd_tiled* h, int policy)
+{
+    if (!h) return set_err(RD_ERR_ARG, "null handle");
+    if (policy != RD_TILED_MIXED && policy != RD_TILED_LOCAL) return set_err(RD_ERR_ARG, "bad policy");
+    h->run.local_policy = (policy == RD_TILED_LOCAL);
+    return RD_OK;
+}
+
 rd_status rd_tiled_set_loop_mode(rd_tiled* h, int mode)
 {
     if (!h) return set_err(RD_ERR_ARG, "null handle");
@@ -541,13 +550,32 @@ rd_status rd_tiled_run(rd_tiled* h, float r1, float r2, int64_t max_tile_capacit
     if (!h || !tiles_per_dim) return set_err(RD_ERR_ARG, "null argument");
     if (!(r1 > 0.0f) || !(r2 > 0.0f)) return set_err(RD_ERR_ARG, "r1 and r2 must be > 0");
     if (max_tile_capacity < 2) return set_err(RD_ERR_ARG, "max_tile_capacity must be >= 2");
-    if (end_phase_refinement)
-        return set_err(RD_ERR_UNSUPPORTED, "end-phase refinement is not built into this library");
     h->have_result = false;
     int rc = h->run.run(h->pts.as<float>(), h->np, h->dim, r1, r2, max_tile_capacity,
                         tiles_per_dim, h->mode == RD_LOOP_GRAPH, (cudaStream_t)stream);
     h->have_result = (rc == 0 || rc == RD_ERR_NOT_CONVERGED);
     if (rc) return set_err((rd_status)rc, h->run.last_error);
+    if (end_phase_refinement && h->run.ns() > 0) {
+        // rd/cpu/tiled/rd_tiled.hpp:1386-1419: a brute-force decimation of the
+        // whole result in leaf order, then an evolve of the entire cloud
+        // against the survivors, to convergence
+        const auto t0 = std::chrono::steady_clock::now();
+        float* S = h->run.result_mut();
+        int64_t left = h->run.ns();
+        if (rd_status s = rd_decimate(h->dim, S, h->run.ns(), r2, &left, stream)) {
+            h->have_result = false;
+            return s;
+        }
+        h->run.set_result_count(left);
+        int64_t passes = 0;
+        const rd_status s = rd_evolve(h->dim, h->pts.as<float>(), h->np, S, left, r1, &passes, stream);
+        h->run.add_refinement_time(
+            std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count());
+        if (s != RD_OK) {
+            h->have_result = (s == RD_ERR_NOT_CONVERGED);
+            return s;
+        }
+    }
     return RD_OK;
 }
 

@@ -498,12 +498,27 @@ int TiledRunner::run(const float* d_points, int64_t n, int dim, float r1, float 
         xidx.insert(xidx.end(), extra[k].halo.begin(), extra[k].halo.end());
     }
     const int64_t total = m + (int64_t)xidx.size();
-    for (auto& c : cl) c.group = 0;
-    std::vector<GroupDesc> gr(1);
-    std::memset(gr.data(), 0, sizeof(GroupDesc));
-    gr[0].cloud_begin = 0;
-    gr[0].n_clouds = (int32_t)cl.size();
-    gr[0].nocopy = 1;
+    std::vector<GroupDesc> gr;
+    if (local_policy) {
+        // RD_LOCAL: every leaf is its own group, decimated on its own with the
+        // brute-force semantics (agent_tiled_ridge_detection.cuh:232-331)
+        gr.resize(cl.size());
+        std::memset(gr.data(), 0, sizeof(GroupDesc) * gr.size());
+        for (size_t c = 0; c < cl.size(); ++c) {
+            cl[c].group = (int32_t)c;
+            gr[c].cloud_begin = (int32_t)c;
+            gr[c].n_clouds = 1;
+            gr[c].nocopy = 0;
+        }
+    } else {
+        // RD_MIXED: one group of all leaves, global decimateNoCopy
+        for (auto& c : cl) c.group = 0;
+        gr.resize(1);
+        std::memset(gr.data(), 0, sizeof(GroupDesc));
+        gr[0].cloud_begin = 0;
+        gr[0].n_clouds = (int32_t)cl.size();
+        gr[0].nocopy = 1;
+    }
     if (cl.empty()) {
         tm_.build_ms = tm_.whole_ms =
             std::chrono::duration<float, std::milli>(clk::now() - t0).count();

@@ -43,11 +43,18 @@ public:
     int64_t ns() const { return ns_; }
     int64_t n_leaves() const { return (int64_t)leaf_ns_.size(); }
     const float* result() const { return bOut_.as<float>(); }  // ns x dim, leaf pre-order
+    float* result_mut() { return bOut_.as<float>(); }
+    // after an in-place change of the result (end-phase refinement)
+    void set_result_count(int64_t ns) { ns_ = ns; }
+    void add_refinement_time(float ms) { tm_.refine_ms = ms; tm_.whole_ms += ms; }
     const TiledTimers& timers() const { return tm_; }
     const RunStats& stats() const { return eng_.stats(); }
     // host-loop runs time every fused tile-evolve launch (RunStats.assign_ms)
     void set_profiling(bool on) { eng_.profile_assign = on; }
     std::string last_error;
+    // false: RD_MIXED (local evolve, global decimation); true: RD_LOCAL (a full
+    // ridge detection inside every leaf)
+    bool local_policy = false;
 
 private:
     int fail(const char* what, cudaError_t e);

@@ -33,6 +33,8 @@ static void use_tiled()
     std::vector<float> out(2 * (size_t)rd.getChosenPointsNum());
     rd.getChosenPoints(out.data());
     (void)rd.getTimers();
+    tiled::RidgeDetection<2, ROW_MAJOR, ROW_MAJOR, tiled::RD_BRUTE_FORCE, tiled::RD_LOCAL> rl(1000, pts.data());
+    rl(0.2f, 0.4f, 1001, tiles, true);
 }
 
 int main(int argc, char**)

@@ -67,3 +67,41 @@ def test_tiled_spiral_10m_properties(rdb):
     assert S1.shape[0] > 100
     if S1.shape[0] <= 8000:
         assert decimation_is_stable(S1, 0.4)
+
+
+@pytest.mark.parametrize("case", [
+    ("spiral_split", 30_000, 0.2, 0.4, 1500, (3, 5)),
+    ("sine_2x2", 20_000, 0.3, 0.6, 20_001, (2, 2)),
+    ("helix_2x2x2", 20_000, 0.15, 0.3, 20_001, (2, 2, 2)),
+])
+def test_tiled_end_phase_refinement_matches_oracle(rdb, case):
+    """end_phase_refinement = 1: the tiled result, then a brute-force decimation
+    and an evolve of the whole cloud (rd/cpu/tiled/rd_tiled.hpp:1386-1419)."""
+    kind, n, r1, r2, cap, tpd = case
+    P = {"spiral_split": lambda: G.spiral2d(n, seed=42), "sine_2x2": lambda: G.sine2d(n, seed=46),
+         "helix_2x2x2": lambda: G.helix3d(n, seed=47)}[kind]()
+    S_ref, _, nl_ref = O.ridge_tiled(P, r1, r2, cap, tpd, refine=True)
+    S, st, nl = rdb.tiled_ridge_detection(P, r1, r2, cap, tpd, end_phase_refinement=True)
+    assert nl == nl_ref
+    assert bits_equal(S, S_ref)
+
+
+@pytest.mark.parametrize("case", [
+    ("spiral", 60_000, 0.2, 0.4, 60_001, (16, 16), False),
+    ("spiral_split", 30_000, 0.2, 0.4, 1500, (3, 5), False),
+    ("helix", 40_000, 0.15, 0.3, 40_001, (4, 4, 3), False),
+    ("spiral_split_refined", 30_000, 0.2, 0.4, 1500, (3, 5), True),
+])
+def test_tiled_local_policy_matches_oracle(rdb, case):
+    """RD_LOCAL: a complete ridge detection inside every leaf (the reference's
+    GPU RD_LOCAL policy; no CPU counterpart exists, the oracle restates it)."""
+    kind, n, r1, r2, cap, tpd, refine = case
+    P = {"spiral": lambda: G.spiral2d(n, seed=41), "spiral_split": lambda: G.spiral2d(n, seed=42),
+         "helix": lambda: G.helix3d(n, seed=43),
+         "spiral_split_refined": lambda: G.spiral2d(n, seed=42)}[kind]()
+    S_ref, _, nl_ref = O.ridge_tiled_local(P, r1, r2, cap, tpd, refine=refine)
+    S, st, nl = rdb.tiled_ridge_detection(P, r1, r2, cap, tpd, end_phase_refinement=refine,
+                                          policy=rdb.TILED_LOCAL)
+    assert nl == nl_ref
+    assert st.err_bits == 0
+    assert bits_equal(S, S_ref)
