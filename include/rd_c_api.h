@@ -108,6 +108,42 @@ RD_API rd_status rd_autotune(int dim, const float* d_P, int64_t n, int64_t ns, f
 RD_API rd_status rd_order_chains(int dim, const float* d_S, int64_t ns, float r2, int32_t* d_order,
                                  int32_t* d_chain_start, int64_t* n_chains, void* stream);
 
+/* Quality of a ridge (rd/utils/assessment_quality.hpp), on the device, with the
+ * reference's float arithmetic; points ROW_MAJOR on the device, results to
+ * host floats.  The reference builds its ideal patterns from unseeded random
+ * draws, so here the caller passes the ideal set.
+ *   rd_hausdorff: max(max over T of dist(t, I), max over I of dist(i, T)),
+ *     dist(p, X) = sqrt(min over X of the squared distance); -1 for nt = 0
+ *     (hausdorffDistance, :91-121).
+ *   rd_distance_stats: median (sorted[n/2]), mean (float sum in sorted order
+ *     / n), min and max of dist(s, I) over S (setDistanceStats, :123-154).
+ *   rd_segment_hausdorff: the largest distance of a T point to the x axis,
+ *     sqrt(sum over d >= 1 of t_d^2); -1 for nt = 0 (RDSegmentAssessmentQuality).
+ * Each runs on `stream` and waits for it. */
+RD_API rd_status rd_hausdorff(int dim, const float* d_T, int64_t nt, const float* d_I, int64_t ni,
+                              float* out, void* stream);
+RD_API rd_status rd_distance_stats(int dim, const float* d_S, int64_t n, const float* d_I,
+                                   int64_t ni, float* median, float* mean, float* min_dist,
+                                   float* max_dist, void* stream);
+RD_API rd_status rd_segment_hausdorff(int dim, const float* d_T, int64_t nt, float* out,
+                                      void* stream);
+
+/* Cloud files in the reference's formats (host memory, no GPU needed).
+ * Text (rd/utils/samples_set.hpp:254-294, :444-462): one point per line.
+ * rd_text_cloud_shape gives the point count -- the number of '\n' in the
+ * file -- and the dimension counted on the first line the way the reference
+ * counts it (values are extracted until end of input is hit; a value that ends
+ * the line without trailing white space is not counted).  rd_load_text_cloud
+ * then reads every non-empty line as one point into out (n x dim ROW_MAJOR;
+ * extra values ignored, missing ones 0); a count of non-empty lines other than
+ * n is an error, as in the reference.
+ * Binary (tests/test_util.hpp:505-551): n x dim raw ROW_MAJOR floats; the
+ * file may be longer than that, not shorter. */
+RD_API rd_status rd_text_cloud_shape(const char* path, int64_t* n, int* dim);
+RD_API rd_status rd_load_text_cloud(const char* path, float* out, int64_t n, int dim);
+RD_API rd_status rd_load_binary_cloud(const char* path, int64_t n, int dim, float* out);
+RD_API rd_status rd_save_binary_cloud(const char* path, const float* pts, int64_t n, int dim);
+
 /* Building block of the evolve step (no reference counterpart; the reference
  * forms the same sums inline, rd/cpu/brute_force/evolve.hpp:71-74): for each
  * coordinate d < dim, out[d] = the left-to-right FP32 sum, starting from 0 with

@@ -80,6 +80,12 @@ def lib():
         L.rdo_ridge_tiled_policy.argtypes = [_F, _i64, _int, _flt, _flt, _i64, _I64, _int, _F,
                                              ctypes.POINTER(ctypes.c_int64),
                                              ctypes.POINTER(Stats)]
+        L.rdo_hausdorff_f32.restype = _flt
+        L.rdo_hausdorff_f32.argtypes = [_F, _i64, _F, _i64, _int]
+        L.rdo_distance_stats_f32.restype = None
+        L.rdo_distance_stats_f32.argtypes = [_F, _i64, _F, _i64, _int, _F]
+        L.rdo_segment_hausdorff_f32.restype = _flt
+        L.rdo_segment_hausdorff_f32.argtypes = [_F, _i64, _int]
         L.rdo_order.restype = _i64
         L.rdo_order.argtypes = [_F, _i64, _int, _flt, _I32, _I32]
         L.rdo_evolve_adjoint.restype = _int
@@ -109,6 +115,15 @@ def ref(openmp: bool = False):
             L.ref_decimate_nocopy.argtypes = [_F, _i64, _I64, _int, _flt]
             L.ref_bf_ridge.restype = _i64
             L.ref_bf_ridge.argtypes = [_F, _i64, _int, _flt, _flt, _F, _int]
+            L.ref_load_text.restype = _i64
+            L.ref_load_text.argtypes = [ctypes.c_char_p, ctypes.c_char_p, _F, _i64,
+                                        ctypes.POINTER(ctypes.c_int)]
+            L.ref_hausdorff_f32.restype = _flt
+            L.ref_hausdorff_f32.argtypes = [_F, _i64, _F, _i64, _int]
+            L.ref_distance_stats_f32.restype = None
+            L.ref_distance_stats_f32.argtypes = [_F, _i64, _F, _i64, _int, _F]
+            L.ref_segment_hausdorff_f32.restype = _flt
+            L.ref_segment_hausdorff_f32.argtypes = [_F, _i64, _int]
             L.ref_order.restype = _i64
             L.ref_order.argtypes = [_F, _i64, _int, _flt, _I32, _I32]
             L.ref_tiled_ridge.restype = _i64
@@ -342,3 +357,38 @@ def ref_order(S, r2):
     cs = np.empty(ns + 1, np.int32)
     nch = L.ref_order(_fp(S), ns, S.shape[1], r2, o.ctypes.data_as(_I32), cs.ctypes.data_as(_I32))
     return o[:ns].copy(), cs[:nch + 1].copy()
+
+
+def ref_load_text(path, cap=1 << 22):
+    """The reference's own text cloud reader (rd::Samples<float>::loadFromFile).
+    It resolves files relative to the running executable's directory, so the
+    folder is passed relative to it.  Returns an array, or None when the
+    reference throws."""
+    L = ref(False)
+    exe_dir = os.path.dirname(os.path.realpath("/proc/self/exe"))
+    folder = os.path.relpath(os.path.dirname(os.path.abspath(path)), exe_dir) + "/"
+    out = np.zeros(cap, np.float32)
+    dim = ctypes.c_int(0)
+    n = L.ref_load_text(folder.encode(), os.path.basename(path).encode(), _fp(out), cap,
+                        ctypes.byref(dim))
+    if n < 0:
+        return None
+    return out[: n * dim.value].reshape(n, dim.value).copy()
+
+
+def quality(T, I=None, which="hausdorff", use_ref=False):
+    """assessment_quality.hpp in float: which = "hausdorff" (T vs ideal I),
+    "stats" ((median, avg, min, max) of T's distances to I) or "segment"
+    (largest distance of T to the x axis).  use_ref: the reference's own code."""
+    L = ref(False) if use_ref else lib()
+    pre = "ref_" if use_ref else "rdo_"
+    T = _f32(T)
+    dim = T.shape[1]
+    if which == "segment":
+        return getattr(L, pre + "segment_hausdorff_f32")(_fp(T), T.shape[0], dim)
+    I = _f32(I)
+    if which == "hausdorff":
+        return getattr(L, pre + "hausdorff_f32")(_fp(T), T.shape[0], _fp(I), I.shape[0], dim)
+    out = np.zeros(4, np.float32)
+    getattr(L, pre + "distance_stats_f32")(_fp(T), T.shape[0], _fp(I), I.shape[0], dim, _fp(out))
+    return tuple(float(x) for x in out)

@@ -655,3 +655,79 @@ int64_t rdo_order(const float* S, int64_t ns, int dim, float r2, int32_t* order,
     free(deq);
     return nch;
 }
+
+/* ------------------------------------------------------------------------- */
+/* rd/utils/assessment_quality.hpp in float, as the reference computes it.    */
+/* ------------------------------------------------------------------------- */
+
+/* :156-205 distance(): sqrt of the smallest squared distance from p to set B
+ * (strict < over B in order; FLT_MAX when B is empty). */
+static float q_distance(const float* p, const float* B, int64_t nb, int dim)
+{
+    float nearest = 3.402823466e+38f;
+    for (int64_t k = 0; k < nb; ++k) {
+        const float d = sqdist(p, B + k * dim, dim);
+        if (d < nearest) nearest = d;
+    }
+    return sqrtf(nearest);
+}
+
+/* :207-222 setDistance(): the largest of those over A */
+static float q_set_distance(const float* A, int64_t na, const float* B, int64_t nb, int dim)
+{
+    float mx = -3.402823466e+38f;
+    for (int64_t i = 0; i < na; ++i) {
+        const float d = q_distance(A + i * dim, B, nb, dim);
+        if (d > mx) mx = d;
+    }
+    return mx;
+}
+
+/* :91-121 hausdorffDistance(): -1 for an empty test set */
+float rdo_hausdorff_f32(const float* T, int64_t nt, const float* I, int64_t ni, int dim)
+{
+    if (nt <= 0) return -1.0f;
+    const float ab = q_set_distance(T, nt, I, ni, dim);
+    const float ba = q_set_distance(I, ni, T, nt, dim);
+    return ab > ba ? ab : ba;
+}
+
+static int cmp_float(const void* a, const void* b)
+{
+    const float x = *(const float*)a, y = *(const float*)b;
+    return (x > y) - (x < y);
+}
+
+/* :123-154 setDistanceStats(): distances of every source point to the ideal
+ * set, sorted; min, max, median = sorted[n/2], average = float sum in sorted
+ * order / n.  out = {median, avg, min, max}. */
+void rdo_distance_stats_f32(const float* S, int64_t n, const float* I, int64_t ni, int dim,
+                            float* out)
+{
+    float* d = (float*)malloc(sizeof(float) * (size_t)(n + 1));
+    for (int64_t i = 0; i < n; ++i) d[i] = q_distance(S + i * dim, I, ni, dim);
+    qsort(d, (size_t)n, sizeof(float), cmp_float);
+    float avg = 0.0f;
+    for (int64_t i = 0; i < n; ++i) avg += d[i];
+    out[0] = d[n / 2];
+    out[1] = avg / (float)n;
+    out[2] = d[0];
+    out[3] = d[n - 1];
+    free(d);
+}
+
+/* :295-375 RDSegmentAssessmentQuality: the distance of every test point to the
+ * x axis, sqrt(sum over d >= 1 of x_d^2) (0 when that sum is 0), and its
+ * largest value; -1 for an empty test set. */
+float rdo_segment_hausdorff_f32(const float* T, int64_t nt, int dim)
+{
+    if (nt <= 0) return -1.0f;
+    float mx = -3.402823466e+38f;
+    for (int64_t i = 0; i < nt; ++i) {
+        float s = 0.0f;
+        for (int k = 1; k < dim; ++k) s += T[i * dim + k] * T[i * dim + k];
+        const float d = (s > 0.0f) ? sqrtf(s) : 0.0f;
+        if (d > mx) mx = d;
+    }
+    return mx;
+}

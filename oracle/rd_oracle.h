@@ -59,6 +59,10 @@ double rdo_hausdorff(const float* A, int64_t na, const float* B, int64_t nb, int
 int64_t rdo_ridge_tiled_policy(const float* P, int64_t np, int dim, float r1, float r2,
                                int64_t max_tile_capacity, const int64_t* tiles_per_dim,
                                int local, float* S, int64_t* n_leaves, rdo_stats* st);
+float rdo_hausdorff_f32(const float* T, int64_t nt, const float* I, int64_t ni, int dim);
+void rdo_distance_stats_f32(const float* S, int64_t n, const float* I, int64_t ni, int dim,
+                            float* out);
+float rdo_segment_hausdorff_f32(const float* T, int64_t nt, int dim);
 int64_t rdo_order(const float* S, int64_t ns, int dim, float r2, int32_t* order,
                   int32_t* chain_start);
 

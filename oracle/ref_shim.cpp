@@ -30,6 +30,8 @@
 #include "rd/cpu/brute_force/decimate.hpp"
 #include "rd/cpu/tiled/rd_tiled.hpp"
 #include "rd/cpu/brute_force/order.hpp"
+#include "rd/utils/samples_set.hpp"
+#include "rd/utils/assessment_quality.hpp"
 
 #include <cstdint>
 #include <cstring>
@@ -216,6 +218,55 @@ int64_t ref_tiled_ridge(const float* P, int64_t np, int dim, float r1, float r2,
     }
     std::memcpy(S_out, dp.S.data(), dp.S.size() * sizeof(float));
     return (int64_t)dp.ns;
+}
+
+// rd::Samples<float>::loadFromFile (rd/utils/samples_set.hpp:254-294): the
+// reference's text cloud reader.  The file is found as <directory of the
+// running executable>/<folder><filename>, as the reference resolves it
+// (rd/utils/utilities.hpp:149-184).  Returns the point count, -1 on a thrown
+// error, -2 when cap is too small; *dim receives the dimension.
+int64_t ref_load_text(const char* folder, const char* filename, float* out, int64_t cap,
+                      int* dim)
+{
+    try {
+        rd::Samples<float> s;
+        s.loadFromFile(filename, folder);
+        *dim = (int)s.dim_;
+        if ((int64_t)(s.size_ * s.dim_) > cap) return -2;
+        std::memcpy(out, s.samples_, sizeof(float) * s.size_ * s.dim_);
+        return (int64_t)s.size_;
+    } catch (...) {
+        return -1;
+    }
+}
+
+// rd::RDAssessmentQuality<float> (rd/utils/assessment_quality.hpp) on a given
+// ideal pattern: the reference generates its patterns from unseeded random
+// draws, so the shim sets the protected pattern directly.
+struct ShimQuality : rd::RDAssessmentQuality<float> {
+    ShimQuality(const float* ideal, size_t n, size_t dim) : rd::RDAssessmentQuality<float>(n, dim)
+    {
+        idealPattern.assign(ideal, ideal + n * dim);
+    }
+};
+
+float ref_hausdorff_f32(const float* T, int64_t nt, const float* I, int64_t ni, int dim)
+{
+    ShimQuality q(I, (size_t)ni, (size_t)dim);
+    return q.hausdorffDistance(std::vector<float>(T, T + nt * dim));
+}
+
+void ref_distance_stats_f32(const float* S, int64_t n, const float* I, int64_t ni, int dim,
+                            float* out)
+{
+    ShimQuality q(I, (size_t)ni, (size_t)dim);
+    q.setDistanceStats(std::vector<float>(S, S + n * dim), out[0], out[1], out[2], out[3]);
+}
+
+float ref_segment_hausdorff_f32(const float* T, int64_t nt, int dim)
+{
+    rd::RDSegmentAssessmentQuality<float> q(0, (size_t)dim);
+    return q.hausdorffDistance(std::vector<float>(T, T + nt * dim));
 }
 
 // rd::orderSamples (rd/cpu/brute_force/order.hpp:45) with the condition the

@@ -68,7 +68,14 @@ SIGNATURES = {
     "rd_autotune": [ctypes.c_int, _vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_float, ctypes.c_int,
                     ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                     ctypes.POINTER(ctypes.c_double), _vp],
+    "rd_hausdorff": [_i, _vp, _i64, _vp, _i64, _pf, _vp],
+    "rd_distance_stats": [_i, _vp, _i64, _vp, _i64, _pf, _pf, _pf, _pf, _vp],
+    "rd_segment_hausdorff": [_i, _vp, _i64, _pf, _vp],
     "rd_order_chains": [_i, _vp, _i64, _f, _vp, _vp, _pi64, _vp],
+    "rd_text_cloud_shape": [ctypes.c_char_p, _pi64, ctypes.POINTER(ctypes.c_int)],
+    "rd_load_text_cloud": [ctypes.c_char_p, _vp, _i64, _i],
+    "rd_load_binary_cloud": [ctypes.c_char_p, _i64, _i, _vp],
+    "rd_save_binary_cloud": [ctypes.c_char_p, _vp, _i64, _i],
     "rd_ordered_sum": [ctypes.c_int, _vp, _vp, ctypes.c_int64, _vp, ctypes.c_int, _vp],
     "rd_bf_create": [ctypes.POINTER(_vp), _i, _i, _i, _i64, _f, _f],
     "rd_bf_set_points": [_vp, _vp, _i64, _i, _vp],

@@ -383,3 +383,78 @@ def order_chains(S, r2: float):
                                     ctypes.c_void_p(starts.data_ptr()), ctypes.byref(nch),
                                     ctypes.c_void_p(stream)))
     return order[:ns].cpu().numpy(), starts[: nch.value + 1].cpu().numpy()
+
+
+# ---------------------------------------------------------------------------
+# cloud files in the reference's formats
+# ---------------------------------------------------------------------------
+
+def load_text_cloud(path: str) -> np.ndarray:
+    """A text cloud as the reference reads it (rd/utils/samples_set.hpp:254-294):
+    n = number of newlines, dim counted on the first line (a last value with no
+    trailing white space is not counted), one point per non-empty line."""
+    n, d = ctypes.c_int64(0), ctypes.c_int(0)
+    L.check(L.lib().rd_text_cloud_shape(path.encode(), ctypes.byref(n), ctypes.byref(d)))
+    if d.value < 1:
+        raise L.RDError(L.RD_ERR_ARG, "no value on the first line")
+    out = np.empty((n.value, d.value), np.float32)
+    L.check(L.lib().rd_load_text_cloud(path.encode(), ctypes.c_void_p(out.ctypes.data),
+                                       n.value, d.value))
+    return out
+
+
+def load_binary_cloud(path: str, n: int, dim: int) -> np.ndarray:
+    """n x dim raw ROW_MAJOR float32 values (tests/test_util.hpp:505-551)."""
+    out = np.empty((n, dim), np.float32)
+    L.check(L.lib().rd_load_binary_cloud(path.encode(), n, dim, ctypes.c_void_p(out.ctypes.data)))
+    return out
+
+
+def save_binary_cloud(path: str, P) -> None:
+    """Write P (n x dim float32) as raw ROW_MAJOR floats."""
+    P = np.ascontiguousarray(P, np.float32)
+    L.check(L.lib().rd_save_binary_cloud(path.encode(), ctypes.c_void_p(P.ctypes.data),
+                                         P.shape[0], P.shape[1]))
+
+
+# ---------------------------------------------------------------------------
+# quality of a ridge (rd/utils/assessment_quality.hpp), on the device
+# ---------------------------------------------------------------------------
+
+def _dev(x):
+    import torch
+    if _is_torch_cuda(x):
+        return x.contiguous()
+    return torch.from_numpy(np.ascontiguousarray(x, np.float32)).cuda()
+
+
+def hausdorff(T, I) -> float:
+    """Symmetric Hausdorff distance of point sets T and I (float, as the
+    reference's hausdorffDistance); -1 for an empty T."""
+    dT, dI = _dev(T), _dev(I)
+    out = ctypes.c_float(0)
+    dim = int(dT.shape[1])
+    L.check(L.lib().rd_hausdorff(dim, ctypes.c_void_p(dT.data_ptr()), int(dT.shape[0]),
+                                 ctypes.c_void_p(dI.data_ptr()), int(dI.shape[0]),
+                                 ctypes.byref(out), None))
+    return out.value
+
+
+def distance_stats(S, I) -> Tuple[float, float, float, float]:
+    """(median, mean, min, max) of the distances of S's points to the set I
+    (setDistanceStats)."""
+    dS, dI = _dev(S), _dev(I)
+    v = [ctypes.c_float(0) for _ in range(4)]
+    L.check(L.lib().rd_distance_stats(int(dS.shape[1]), ctypes.c_void_p(dS.data_ptr()),
+                                      int(dS.shape[0]), ctypes.c_void_p(dI.data_ptr()),
+                                      int(dI.shape[0]), *[ctypes.byref(x) for x in v], None))
+    return tuple(x.value for x in v)
+
+
+def segment_hausdorff(T) -> float:
+    """Largest distance of T's points to the x axis (RDSegmentAssessmentQuality)."""
+    dT = _dev(T)
+    out = ctypes.c_float(0)
+    L.check(L.lib().rd_segment_hausdorff(int(dT.shape[1]), ctypes.c_void_p(dT.data_ptr()),
+                                         int(dT.shape[0]), ctypes.byref(out), None))
+    return out.value

@@ -16,6 +16,7 @@
 using namespace rdb;
 
 namespace rdb {
+rd_status report_error(rd_status s, const char* msg);
 int decimate_noalloc(int dim, float* d_S, int64_t ns, float r2, int32_t* d_ns_out, cudaStream_t st);
 extern const char* noalloc_error_message;
 }  // namespace rdb
@@ -29,6 +30,12 @@ rd_status set_err(rd_status s, const std::string& msg)
     g_err = msg;
     return s;
 }
+
+}  // namespace
+
+rd_status rdb::report_error(rd_status s, const char* msg) { return set_err(s, msg); }
+
+namespace {
 
 rd_status from_engine(int rc, const Engine& e)
 {
@@ -336,6 +343,84 @@ rd_status rd_autotune(int dim, const float* d_P, int64_t n, int64_t ns, float r1
     *block = bt.block;
     *items = bt.items;
     if (us_per_launch) *us_per_launch = best;
+    return RD_OK;
+}
+
+// ------------------------------------------------------------------------
+// quality metrics
+// ------------------------------------------------------------------------
+rd_status rd_hausdorff(int dim, const float* d_T, int64_t nt, const float* d_I, int64_t ni,
+                       float* out, void* stream)
+{
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (!out || (nt > 0 && !d_T) || (ni > 0 && !d_I)) return set_err(RD_ERR_ARG, "null argument");
+    if (nt < 0 || ni < 0 || nt > INT32_MAX || ni > INT32_MAX) return set_err(RD_ERR_ARG, "bad sizes");
+    if (nt == 0) {
+        *out = -1.0f;
+        return RD_OK;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    thread_local DevBuf& buf = *new DevBuf();  // never destroyed: no CUDA calls at exit
+    CK_CUDA(buf.ensure(sizeof(float) * (size_t)(nt + ni + 1)));
+    float* dT = buf.as<float>();
+    float* dI = dT + nt;
+    float* res = dI + ni;
+    CK_CUDA(launch_min_dist(dim, d_T, (int)nt, d_I, (int)ni, dT, st));
+    CK_CUDA(launch_min_dist(dim, d_I, (int)ni, d_T, (int)nt, dI, st));
+    CK_CUDA(launch_max2(dT, (int)nt, dI, (int)ni, res, st));
+    CK_CUDA(cudaMemcpyAsync(out, res, sizeof(float), cudaMemcpyDeviceToHost, st));
+    CK_CUDA(cudaStreamSynchronize(st));
+    return RD_OK;
+}
+
+rd_status rd_distance_stats(int dim, const float* d_S, int64_t n, const float* d_I, int64_t ni,
+                            float* median, float* mean, float* min_dist, float* max_dist,
+                            void* stream)
+{
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (!median || !mean || !min_dist || !max_dist || !d_S || (ni > 0 && !d_I))
+        return set_err(RD_ERR_ARG, "null argument");
+    if (n < 1 || ni < 0 || n > INT32_MAX / 2 || ni > INT32_MAX)
+        return set_err(RD_ERR_ARG, "need 1 <= n and sizes in range");
+    cudaStream_t st = (cudaStream_t)stream;
+    thread_local DevBuf& buf = *new DevBuf();
+    thread_local DevBuf& tmp = *new DevBuf();
+    const size_t tb = dist_stats_temp_bytes((int)n);
+    CK_CUDA(buf.ensure(sizeof(float) * (size_t)(3 * n + 8)));
+    CK_CUDA(tmp.ensure(tb + 16));
+    float* d = buf.as<float>();
+    float* sorted = d + n;
+    int32_t* iota = reinterpret_cast<int32_t*>(sorted + n);
+    float* res = reinterpret_cast<float*>(iota + n);
+    CK_CUDA(launch_min_dist(dim, d_S, (int)n, d_I, (int)ni, d, st));
+    CK_CUDA(launch_dist_stats(d, (int)n, sorted, iota, tmp.p, tb, res, st));
+    float h[4];
+    CK_CUDA(cudaMemcpyAsync(h, res, sizeof(h), cudaMemcpyDeviceToHost, st));
+    CK_CUDA(cudaStreamSynchronize(st));
+    *median = h[0];
+    *mean = h[1];
+    *min_dist = h[2];
+    *max_dist = h[3];
+    return RD_OK;
+}
+
+rd_status rd_segment_hausdorff(int dim, const float* d_T, int64_t nt, float* out, void* stream)
+{
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (!out || (nt > 0 && !d_T)) return set_err(RD_ERR_ARG, "null argument");
+    if (nt < 0 || nt > INT32_MAX) return set_err(RD_ERR_ARG, "bad size");
+    if (nt == 0) {
+        *out = -1.0f;
+        return RD_OK;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    thread_local DevBuf& buf = *new DevBuf();
+    CK_CUDA(buf.ensure(sizeof(float) * (size_t)(nt + 1)));
+    float* d = buf.as<float>();
+    CK_CUDA(launch_axis_dist(dim, d_T, (int)nt, d, st));
+    CK_CUDA(launch_max2(d, (int)nt, d, 0, d + nt, st));
+    CK_CUDA(cudaMemcpyAsync(out, d + nt, sizeof(float), cudaMemcpyDeviceToHost, st));
+    CK_CUDA(cudaStreamSynchronize(st));
     return RD_OK;
 }
 

@@ -149,6 +149,14 @@ cudaError_t prepare_tile_pass(int dim, const EngineView& v);
 cudaError_t launch_tile_pass(int dim, const EngineView& v, cudaStream_t st,
                              cudaEvent_t a0 = nullptr, cudaEvent_t a1 = nullptr);
 cudaError_t launch_decimate(int dim, const EngineView& v, cudaStream_t st);
+// quality metrics (rd_quality.cu)
+cudaError_t launch_min_dist(int dim, const float* A, int na, const float* B, int nb, float* out,
+                            cudaStream_t st);
+cudaError_t launch_axis_dist(int dim, const float* T, int n, float* out, cudaStream_t st);
+cudaError_t launch_max2(const float* a, int na, const float* b, int nb, float* out, cudaStream_t st);
+cudaError_t launch_dist_stats(float* d, int n, float* sorted, int32_t* iota, void* temp,
+                              size_t temp_bytes, float* out, cudaStream_t st);
+size_t dist_stats_temp_bytes(int n);
 // chains of a ridge (rd_order.cu): alive ns bytes, deq 2*ns+1 ints of scratch;
 // order ns ints, chain_start ns+1 ints, n_chains one int (all device)
 cudaError_t launch_order_chains(int dim, const float* S, int ns, float rsq, unsigned char* alive,

@@ -63,6 +63,22 @@ def spiral2d(n: int, seed: int = SEED_BASE, noise: float = 0.05,
     return np.ascontiguousarray(p, dtype=np.float32)
 
 
+def ideal_spiral2d(n: int, seed: int = SEED_BASE) -> np.ndarray:
+    """Noise-free points of the curve spiral2d samples, 0.5*theta*(cos, sin)
+    for theta uniform in [0, 6*pi]: an ideal pattern for the quality metrics
+    (the role of genSpiral2D with sigma = 0, rd/cpu/samples_generator.hpp:42)."""
+    th = np.random.default_rng(seed).uniform(0.0, 6.0 * math.pi, n)
+    return np.ascontiguousarray(np.stack([0.5 * th * np.cos(th), 0.5 * th * np.sin(th)], 1),
+                                dtype=np.float32)
+
+
+def ideal_helix3d(n: int, seed: int = SEED_BASE) -> np.ndarray:
+    """Noise-free points of the curve helix3d samples, (cos t, sin t, 0.15 t)
+    for t uniform in [0, 8*pi]."""
+    t = np.random.default_rng(seed).uniform(0.0, 8.0 * math.pi, n)
+    return np.ascontiguousarray(np.stack([np.cos(t), np.sin(t), 0.15 * t], 1), dtype=np.float32)
+
+
 def batch_spec(n_clouds: int = 4096, seed_base: int = SEED_BASE,
                n_min: int = 1000, n_max: int = 200_000):
     """Per-cloud (n, dim, r1, r2, seed) of the batched workload."""

@@ -130,3 +130,33 @@ def test_order_restatement_matches_reference(case):
     a, b = O.order(S, r2), O.ref_order(S, r2)
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
     assert sorted(a[0].tolist()) == list(range(S.shape[0]))   # a permutation
+
+
+def _quality_sets():
+    r = np.random.default_rng(5)
+    t = r.uniform(0, 6 * np.pi, 20000)
+    ideal = np.stack([0.5 * t * np.cos(t), 0.5 * t * np.sin(t)], 1).astype(np.float32)
+    S, _, _ = O.ridge_tiled(O_gen_spiral(), 0.2, 0.4, 100_001, (16, 16))
+    return [("ridge_vs_spiral", S, ideal),
+            ("random3d", r.normal(size=(700, 3)).astype(np.float32),
+             r.normal(size=(3000, 3)).astype(np.float32)),
+            ("single", np.ones((1, 2), np.float32), np.zeros((5, 2), np.float32))]
+
+
+def O_gen_spiral():
+    from ridgedetection_b200 import generators as G
+    return G.spiral2d(100_000, seed=6)
+
+
+@pytest.mark.parametrize("case", _quality_sets(), ids=lambda c: c[0])
+def test_quality_restatement_matches_reference(case):
+    """rd_oracle.c float Hausdorff / distance stats / segment distance == the
+    reference's own RDAssessmentQuality<float>."""
+    if O.ref(False) is None:
+        pytest.skip("oracle/_ref not built")
+    _, T, I = case
+    for which in ("hausdorff", "stats", "segment"):
+        a = O.quality(T, I, which)
+        b = O.quality(T, I, which, use_ref=True)
+        assert np.array_equal(np.float32(a), np.float32(b)), (which, a, b)
+    assert O.quality(np.zeros((0, 2), np.float32), I, "hausdorff") == -1.0
