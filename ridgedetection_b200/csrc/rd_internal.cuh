@@ -114,6 +114,49 @@ __device__ __forceinline__ float2 sqdist2_exact(const float* s, const float2* np
 
 __device__ __forceinline__ float sqr_rn(float r) { return __fmul_rn(r, r); }
 
+// Runs of equal keys of a warp, for stable grouping without match
+// instructions (the match instruction's throughput drops when a warp holds
+// many distinct keys, as in a brute-force cloud visited in random order): the 32 (key, lane) pairs are sorted by key, ties by lane
+// (a bitonic network of shuffles); lane p then holds the p-th element of that
+// order.  key < 0 means "no key" and sorts last.  Keys must be < 2^26.
+struct WarpRun {
+    int key;      // key of the element held (-1: none)
+    int src;      // its lane before the sort
+    int rank;     // its position among the elements of its key (in lane order)
+    int count;    // elements of its key in the warp
+    int head;     // lane holding the first element of its key
+};
+
+__device__ __forceinline__ WarpRun warp_runs(const int key, const int lane)
+{
+    constexpr unsigned NONE = 0x3FFFFFFu;
+    unsigned v = ((key < 0 ? NONE : (unsigned)key) << 5) | (unsigned)lane;
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const unsigned o = __shfl_xor_sync(0xffffffffu, v, j);
+            const bool up = (lane & k) == 0 || k == 32;
+            const bool lower = (lane & j) == 0;
+            v = (lower == up) ? min(v, o) : max(v, o);
+        }
+    }
+    WarpRun r;
+    const unsigned ks = v >> 5;
+    r.src = (int)(v & 31u);
+    r.key = (ks == NONE) ? -1 : (int)ks;
+    const unsigned prev = __shfl_up_sync(0xffffffffu, ks, 1);
+    const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || prev != ks);
+    const unsigned le = (lane == 31) ? 0xffffffffu : ((2u << lane) - 1u);
+    r.head = 31 - __clz(heads & le);
+    const unsigned after = heads & ~le;
+    const int end = after ? (__ffs(after) - 1) : 32;
+    r.rank = lane - r.head;
+    r.count = end - r.head;
+    return r;
+}
+
+
 // shift of one coordinate (rd/cpu/brute_force/evolve.hpp:143-177); returns 1
 // when the coordinate moved.
 __device__ __forceinline__ int shift_coord(float sum, int cnt, float& c)

@@ -550,13 +550,13 @@ __device__ void segscan_one(const EngineView& v, int c, int* s_w, int* s_carry_p
     int32_t* base = v.base + cd.key_off;
     for (int k = threadIdx.x; k < ns; k += BLOCK) {
         int run = 0;
-        for (int s0 = 0; s0 < cd.n_seg; s0 += 8) {  // 8 loads in flight per step
-            int x[8];
+        for (int s0 = 0; s0 < cd.n_seg; s0 += 16) {  // 16 loads in flight per step
+            int x[16];
 #pragma unroll
-            for (int u = 0; u < 8; ++u)
+            for (int u = 0; u < 16; ++u)
                 x[u] = (s0 + u < cd.n_seg) ? sg[(int64_t)(s0 + u) * cd.ns_cap + k] : 0;
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
+            for (int u = 0; u < 16; ++u) {
                 if (s0 + u < cd.n_seg) sg[(int64_t)(s0 + u) * cd.ns_cap + k] = run;
                 run += x[u];
             }
@@ -601,17 +601,84 @@ __device__ void segscan_one(const EngineView& v, int c, int* s_w, int* s_carry_p
 // ---------------------------------------------------------------------------
 __device__ void scatter_chunk(const EngineView& v, int c, int lc, int* s_keys, int lane);
 
-__global__ void __launch_bounds__(128) k_scatter(EngineView v)
+
+// One CTA per chunk for clouds with at most SCAT_HMAX chosen points.  The
+// chunk is split into SCAT_W contiguous warp ranges; every warp counts its
+// range's keys, an exclusive scan over the warps (per key) gives every warp
+// its own start slots, and the warps then place their ranges at the same time,
+// each in index order.  Ranges are in index order too, so the placement stays
+// stable while the dependent placement chain is SCAT_W times shorter.  Larger
+// chosen sets use scatter_chunk (one warp) in warp 0.
+constexpr int SCAT_W = 8;
+constexpr int SCAT_HMAX = 1024;
+
+__global__ void __launch_bounds__(SCAT_W * 32) k_scatter_cta(EngineView v)
 {
     extern __shared__ int s_dyn[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const ActiveList al(v, ACT_CHUNK);
-    for (int item = blockIdx.x * 4 + warp; item < al.total; item += gridDim.x * 4) {
-        __syncwarp();
+    for (int item = blockIdx.x; item < al.total; item += gridDim.x) {
+        __syncthreads();  // the previous chunk's readers are done
         int c, lc;
         al.locate(item, c, lc);
-        scatter_chunk(v, c, lc, s_dyn + warp * (v.chunk_max + v.scat_smem), lane);
+        const CloudDesc cd = v.cl[c];
+        const int ns = v.ns[c];
+        if (ns > SCAT_HMAX) {
+            if (warp == 0) scatter_chunk(v, c, lc, s_dyn, lane);
+            continue;
+        }
+        const int start = (int)(((int64_t)lc * cd.n_all) / cd.n_chunks);
+        const int end = (int)(((int64_t)(lc + 1) * cd.n_all) / cd.n_chunks);
+        const int len = end - start;
+        int* s_keys = s_dyn;                 // chunk_max
+        int* hw = s_dyn + v.chunk_max;       // SCAT_W x ns: counts, then start slots
+        const int32_t* keys = v.keys + cd.p_off + start;
+        for (int e = tid; e < len; e += SCAT_W * 32) s_keys[e] = keys[e];
+        for (int e = tid; e < SCAT_W * ns; e += SCAT_W * 32) hw[e] = 0;
+        __syncthreads();
+        const int r0 = (warp * len) / SCAT_W, r1 = ((warp + 1) * len) / SCAT_W;
+        for (int i0 = r0; i0 < r1; i0 += 32) {
+            const int i = i0 + lane;
+            const WarpRun r = warp_runs((i < r1) ? s_keys[i] : -1, lane);
+            if (r.key >= 0 && lane == r.head) atomicAdd(&hw[warp * ns + r.key], r.count);
+        }
+        __syncthreads();
+        const int seg = lc / SEG;
+        const int32_t* row = v.hist + cd.hist_off + (int64_t)lc * cd.ns_cap;
+        const int32_t* sg = v.segsum + cd.seg_off + (int64_t)seg * cd.ns_cap;
+        const int32_t* bs = v.base + cd.key_off;
+        for (int k = tid; k < ns; k += SCAT_W * 32) {
+            int run = bs[k] + sg[k] + row[k];
+#pragma unroll
+            for (int w = 0; w < SCAT_W; ++w) {
+                const int x = hw[w * ns + k];
+                hw[w * ns + k] = run;
+                run += x;
+            }
+        }
+        __syncthreads();
+        int* cur = hw + warp * ns;
+        int32_t* perm = v.perm + cd.p_off;
+        for (int i0 = r0; i0 < r1; i0 += 32) {
+            const int i = i0 + lane;
+            const WarpRun r = warp_runs((i < r1) ? s_keys[i] : -1, lane);
+            int b = 0;
+            if (r.key >= 0 && lane == r.head) {
+                b = cur[r.key];
+                cur[r.key] = b + r.count;
+            }
+            b = __shfl_sync(FULL, b, r.head);
+            if (r.key >= 0) perm[b + r.rank] = start + i0 + r.src;
+        }
     }
+}
+
+// dynamic shared memory of k_scatter_cta
+inline int scatter_cta_smem_bytes(const EngineView& v)
+{
+    const int block_path = v.chunk_max + SCAT_W * SCAT_HMAX;
+    const int warp_path = v.chunk_max + v.scat_smem;
+    return 4 * (block_path > warp_path ? block_path : warp_path);
 }
 
 __device__ void scatter_chunk(const EngineView& v, int c, int lc, int* s_keys, int lane)
@@ -628,23 +695,49 @@ __device__ void scatter_chunk(const EngineView& v, int c, int lc, int* s_keys, i
     const int end = (int)(((int64_t)(lc + 1) * cd.n_all) / cd.n_chunks);
     const int len = end - start;
     const int32_t* keys = v.keys + cd.p_off + start;
-    // stage the chunk's keys and the per-key start slots (independent loads)
-    for (int e = lane; e < len; e += 32) s_keys[e] = keys[e];
-    for (int k = lane; k < ns; k += 32) ctr[k] = bs[k] + sg[k] + row[k];
+    // stage the chunk's keys and the per-key start slots: eight independent
+    // loads per lane in flight before the first shared-memory store, so the
+    // staging costs a few load latencies instead of one per 32 elements
+    for (int e0 = 0; e0 < len; e0 += 32 * 8) {
+        int t[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int e = e0 + u * 32 + lane;
+            t[u] = (e < len) ? keys[e] : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int e = e0 + u * 32 + lane;
+            if (e < len) s_keys[e] = t[u];
+        }
+    }
+    for (int k0 = 0; k0 < ns; k0 += 32 * 4) {
+        int a[4], b2[4], r[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int k = k0 + u * 32 + lane;
+            a[u] = (k < ns) ? bs[k] : 0;
+            b2[u] = (k < ns) ? sg[k] : 0;
+            r[u] = (k < ns) ? row[k] : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int k = k0 + u * 32 + lane;
+            if (k < ns) ctr[k] = a[u] + b2[u] + r[u];
+        }
+    }
     __syncwarp();
     int32_t* perm = v.perm + cd.p_off;
     for (int off = 0; off < len; off += 32) {
         const int i = off + lane;
-        const int key = (i < len) ? s_keys[i] : -1;
-        const unsigned m = __match_any_sync(FULL, key);
-        const int leader = __ffs(m) - 1;
+        const WarpRun r = warp_runs((i < len) ? s_keys[i] : -1, lane);
         int b = 0;
-        if (key >= 0 && lane == leader) {
-            b = ctr[key];
-            ctr[key] = b + __popc(m);
+        if (r.key >= 0 && lane == r.head) {
+            b = ctr[r.key];
+            ctr[r.key] = b + r.count;
         }
-        b = __shfl_sync(FULL, b, leader);
-        if (key >= 0) perm[b + __popc(m & lanemask_lt())] = start + i;
+        b = __shfl_sync(FULL, b, r.head);
+        if (r.key >= 0) perm[b + r.rank] = start + off + r.src;
         __syncwarp();
     }
 }
@@ -654,10 +747,13 @@ __device__ void scatter_chunk(const EngineView& v, int c, int lc, int* s_keys, i
 // coordinate d of the key's members in index order with rounded adds,
 // exactly as rd/cpu/brute_force/evolve.hpp:71-74 accumulates, then applies the
 // movement test of evolve.hpp:143-177.  Members are gathered through the
-// permutation written by k_scatter, BP at a time, the next block in flight
+// permutation written by k_scatter_cta, BP at a time, the next block in flight
 // while the current one is folded.
 // ---------------------------------------------------------------------------
 constexpr int SUM_BP = 128;  // members staged per step of the ordered fold
+// k_sum_shift stages 256 members per step: folding a block (about 256 dependent
+// adds) then outlasts the gather of the next one from L2
+constexpr int SUM_BP_WIDE = 256;
 // points (keys) per lane loaded together by the fused tile kernel's
 // assignment (placement) loop
 constexpr int TILE_PPL = 8;
@@ -671,8 +767,8 @@ __device__ void sum_shift_one(const EngineView& v, int c, int k, float* buf, int
 template <int DIM>
 __global__ void __launch_bounds__(256) k_sum_shift(EngineView v)
 {
-    __shared__ float s_buf[8][SUM_BP * DIM];
-    __shared__ int s_idx[8][SUM_BP];
+    __shared__ float s_buf[8][SUM_BP_WIDE * DIM];
+    __shared__ int s_idx[8][SUM_BP_WIDE];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const ActiveList al(v, ACT_SLOT);
     for (int t = blockIdx.x * 8 + warp; t < al.total; t += gridDim.x * 8) {
@@ -685,11 +781,10 @@ __global__ void __launch_bounds__(256) k_sum_shift(EngineView v)
 
 // Sequential FP32 fold, in list order, of the points P[perm[0..n)] (one warp;
 // the sum of coordinate d is returned in lane d < DIM).
-template <int DIM>
+template <int DIM, int BP = SUM_BP>
 __device__ float fold_members(const int32_t* __restrict__ perm, const int n,
                               const float* __restrict__ P, float* buf, int* sidx, const int lane)
 {
-    constexpr int BP = SUM_BP;
     constexpr int R = BP * DIM / 32;    // floats per lane per step
     float nxt[R];
     // Two-stage pipeline: member indices of block b+2 and coordinates of
@@ -754,7 +849,7 @@ __device__ void sum_shift_one(const EngineView& v, int c, int k, float* buf, int
     if (n == 0) return;
     const int32_t* mp = v.perm + cd.p_off + v.base[cd.key_off + k];
     const float* Pc = v.P + cd.p_off * DIM;
-    const float sum = fold_members<DIM>(mp, n, Pc, buf, sidx, lane);
+    const float sum = fold_members<DIM, SUM_BP_WIDE>(mp, n, Pc, buf, sidx, lane);
     int moved = 0;
     if (lane < DIM) {
         float* s = v.S + (cd.s_off + k) * DIM + lane;
@@ -870,6 +965,8 @@ __global__ void __launch_bounds__(BLOCK) k_tile_evolve(EngineView v)
                         }
                         keys[i] = key;
                     }
+                    // a tile's warp step holds few distinct keys: the match
+                    // instruction is cheap there (warp_runs suits many keys)
                     const unsigned mm = __match_any_sync(FULL, key);
                     if (key >= 0 && lane == __ffs(mm) - 1) atomicAdd(&whist[key], __popc(mm));
                 }
@@ -921,7 +1018,6 @@ __global__ void __launch_bounds__(BLOCK) k_tile_evolve(EngineView v)
                 }
 #pragma unroll
                 for (int h = 0; h < TILE_PPL; ++h) {
-                    const int i = i0 + h * 32 + lane;
                     const int key = kq[h];
                     const unsigned m = __match_any_sync(FULL, key);
                     const int leader = __ffs(m) - 1;
@@ -931,7 +1027,7 @@ __global__ void __launch_bounds__(BLOCK) k_tile_evolve(EngineView v)
                         cur[key] = b + __popc(m);
                     }
                     b = __shfl_sync(FULL, b, leader);
-                    if (key >= 0) perm[b + __popc(m & lanemask_lt())] = i;
+                    if (key >= 0) perm[b + __popc(m & lanemask_lt())] = i0 + h * 32 + lane;
                 }
             }
             __syncthreads();
@@ -1520,8 +1616,8 @@ cudaError_t prepare_pass_dim(const EngineView& v, const TuneParams& tp)
     e = cudaFuncSetAttribute(k_decimate<DIM, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              dec_smem_bytes(v));
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                4 * (v.chunk_max + v.scat_smem) * 4);
+    return cudaFuncSetAttribute(k_scatter_cta, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                scatter_cta_smem_bytes(v));
 }
 
 template <int DIM>
@@ -1547,8 +1643,7 @@ cudaError_t launch_pass_dim(const EngineView& v, const TuneParams& tp, int assig
     if (v.n_segs > 0) k_colscan<<<std::min(v.n_segs, sms * 8), 256, 0, st>>>(v);
     k_segscan<1024><<<std::min(v.n_clouds, sms * 2), 1024, 0, st>>>(v);
     if (v.n_chunks > 0)
-        k_scatter<<<std::min((v.n_chunks + 3) / 4, sms * 8), 128,
-                    4 * (v.chunk_max + v.scat_smem) * 4, st>>>(v);
+        k_scatter_cta<<<std::min(v.n_chunks, sms * 8), SCAT_W * 32, scatter_cta_smem_bytes(v), st>>>(v);
     if (v.n_slots > 0) k_sum_shift<DIM><<<std::min((v.n_slots + 7) / 8, sms * 8), 256, 0, st>>>(v);
     k_control<<<std::min((v.n_clouds + 255) / 256, sms), 256, 0, st>>>(v);
     k_decimate<DIM, 512><<<std::min(v.n_groups, sms * 2), 512, dec_smem_bytes(v), st>>>(v);
@@ -1761,8 +1856,7 @@ cudaError_t launch_evolve_step_dim(const EngineView& v, const TuneParams& tp, in
     if (v.n_segs > 0) k_colscan<<<std::min(v.n_segs, sms * 8), 256, 0, st>>>(v);
     k_segscan<1024><<<std::min(v.n_clouds, sms * 2), 1024, 0, st>>>(v);
     if (v.n_chunks > 0)
-        k_scatter<<<std::min((v.n_chunks + 3) / 4, sms * 8), 128,
-                    4 * (v.chunk_max + v.scat_smem) * 4, st>>>(v);
+        k_scatter_cta<<<std::min(v.n_chunks, sms * 8), SCAT_W * 32, scatter_cta_smem_bytes(v), st>>>(v);
     if (v.n_slots > 0) k_sum_shift<DIM><<<std::min((v.n_slots + 7) / 8, sms * 8), 256, 0, st>>>(v);
     return cudaGetLastError();
 }
