@@ -142,7 +142,6 @@ int Engine::setup(int dim, const std::vector<CloudDesc>& clouds,
             chunk_max_ = std::max<int>(chunk_max_, (int)((cd.n_all + nch - 1) / nch));
         for (int k = 0; k < cd.n_chunks; ++k) h_chunk_cloud_.push_back((int32_t)c);
         chunk += cd.n_chunks;
-        cd.n_seg = (cd.n_chunks + SEG - 1) / SEG;
     }
     n_chunks_ = (int32_t)chunk;
     const size_t nc = h_cl_.size();
@@ -161,7 +160,7 @@ int Engine::setup(int dim, const std::vector<CloudDesc>& clouds,
     RD_CK(bPairs_.ensure(8 * (nc + 1)));
     RD_CK(bCtr_.ensure(4 * CTR_COUNT));
     RD_CK(bActCloud_.ensure(4 * (nc + 1)));
-    RD_CK(bActPre_.ensure(4 * 3 * (nc + 1)));
+    RD_CK(bActPre_.ensure(4 * ACT_KINDS * (nc + 1)));
     RD_CK(bGroupConv_.ensure(4 * (h_gr_.size() + 1)));
     RD_CK(bReady_.ensure(4 * (h_gr_.size() + 1)));
     RD_CK(bDbig_.ensure(4 * 4));
@@ -177,13 +176,11 @@ EngineView Engine::view() const
     v.gr = bGr_.as<GroupDesc>();
     v.chunk_cloud = bChunkCloud_.as<int32_t>();
     v.slot_cloud = bSlotCloud_.as<int32_t>();
-    v.seg_list = bSegList_.as<int2>();
     v.P = bP_.as<float>();
     v.S = bS_.as<float>();
     v.keys = bKeys_.as<int32_t>();
     v.perm = bGrouped_.as<int32_t>();
     v.hist = bHist_.as<int32_t>();
-    v.segsum = bSegsum_.as<int32_t>();
     v.cnt = bCnt_.as<int32_t>();
     v.base = bBase_.as<int32_t>();
     v.next = bNext_.as<int32_t>();
@@ -220,7 +217,8 @@ EngineView Engine::view() const
     v.n_groups = (int32_t)h_gr_.size();
     v.n_chunks = n_chunks_;
     v.n_slots = n_slots_;
-    v.n_segs = n_segs_;
+    v.n_kblk = n_kblk_;
+    v.n_kblk_warp = n_kblk_warp_;
     v.chunk_pts = chunk_pts_;
     v.chunk_max = chunk_max_;
     v.hist_smem = hist_smem_;
@@ -246,26 +244,23 @@ int Engine::finish_setup_after_choose(cudaStream_t st)
     h_ns_.resize(nc);
     RD_CK(cudaMemcpyAsync(h_ns_.data(), bNs_.p, 4 * nc, cudaMemcpyDeviceToHost, st));
     RD_CK(cudaStreamSynchronize(st));
-    int64_t hist = 0, seg = 0, key = 0;
+    int64_t hist = 0, key = 0, kblk = 0, kblk_warp = 0;
     int max_ns = 0;
     h_slot_cloud_.clear();
-    h_seg_list_.clear();
     for (size_t c = 0; c < nc; ++c) {
         CloudDesc& cd = h_cl_[c];
         cd.ns_cap = h_ns_[c];
         max_ns = std::max(max_ns, cd.ns_cap);
         cd.hist_off = hist;
         hist += (int64_t)cd.n_chunks * cd.ns_cap;
-        cd.seg_off = seg;
-        seg += (int64_t)cd.n_seg * cd.ns_cap;
         cd.key_off = key;
         key += cd.ns_cap;
+        (cd.n_chunks > SCAN_ROWS_WARP ? kblk : kblk_warp) += (cd.ns_cap + KBLK - 1) / KBLK;
         for (int k = 0; k < cd.ns_cap; ++k) h_slot_cloud_.push_back((int32_t)c);
-        if (cd.ns_cap > 0)
-            for (int s = 0; s < cd.n_seg; ++s) h_seg_list_.push_back(make_int2((int)c, s));
     }
     n_slots_ = (int32_t)key;
-    n_segs_ = (int32_t)h_seg_list_.size();
+    n_kblk_ = (int32_t)kblk;
+    n_kblk_warp_ = (int32_t)kblk_warp;
     // group decimation scratch
     h_dec_hoff_.resize(h_gr_.size());
     h_dec_hbits_.resize(h_gr_.size());
@@ -289,11 +284,9 @@ int Engine::finish_setup_after_choose(cudaStream_t st)
     RD_CK(upload(bCl_, h_cl_, st));
     RD_CK(upload(bGr_, h_gr_, st));
     RD_CK(upload(bSlotCloud_, h_slot_cloud_, st));
-    RD_CK(upload(bSegList_, h_seg_list_, st));
     RD_CK(upload(bDecHoff_, h_dec_hoff_, st));
     RD_CK(upload(bDecHbits_, h_dec_hbits_, st));
     RD_CK(bHist_.ensure(4 * (size_t)(hist + 1)));
-    RD_CK(bSegsum_.ensure(4 * (size_t)(seg + 1)));
     RD_CK(bCnt_.ensure(4 * (size_t)(key + 1)));
     RD_CK(bBase_.ensure(4 * (size_t)(key + 1)));
     RD_CK(bDx_.ensure(4 * (size_t)(sscr * dim_ + 1)));

@@ -4,7 +4,7 @@
 // share the point dimension DIM:
 //   choose      one CTA per cloud, greedy r1-separated subset in input order
 //               over a hashed uniform grid (exact test, grid only prunes);
-//   evolve      passes of  assign -> column scan -> segment scan -> stable
+//   evolve      passes of  assign -> chunk scan -> key bases -> stable
 //               scatter -> ordered sum + shift -> control, over all clouds still
 //               evolving; the per-chosen coordinate sums are formed in cloud-point
 //               index order, exactly as the reference's serial loop forms them;
@@ -40,6 +40,13 @@ constexpr int DEC_SMEM_MAX_POINTS = 32752;
 // fused per-tile evolve: chosen points per tile it can hold
 constexpr int TILE_NS_MAX = 1024;
 
+// kinds of work list over the evolving clouds (rebuilt by the control step
+// after every iteration): assignment chunks; blocks of KBLK chosen points of
+// clouds with more than SCAN_ROWS_WARP chunks (CTA-wide histogram scan) and of
+// the other clouds (one warp per block); chosen slots
+enum : int { ACT_CHUNK = 0, ACT_KBLK = 1, ACT_KBLK_WARP = 2, ACT_SLOT = 3, ACT_KINDS = 4 };
+constexpr int SCAN_ROWS_WARP = 64;
+
 enum : int {
     CTR_WORK = 0,      // assignment work ticket
     CTR_ACTIVE = 1,    // unfinished clouds after the last control step
@@ -55,13 +62,11 @@ struct EngineView {
     const GroupDesc* gr;
     const int32_t* chunk_cloud;  // chunk -> cloud
     const int32_t* slot_cloud;   // chosen slot -> cloud
-    const int2* seg_list;        // (cloud, segment) pairs
     float* P;                    // packed evolve points, ROW_MAJOR
     float* S;                    // chosen points, ROW_MAJOR, capacity n_own per cloud
     int32_t* keys;               // per point slot: assigned chosen index or -1
     int32_t* perm;               // per point slot: point indices grouped by key, index order
-    int32_t* hist;               // per cloud: n_chunks x ns_cap key histogram
-    int32_t* segsum;             // per cloud: n_seg x ns_cap segment sums
+    int32_t* hist;               // per cloud: n_chunks x ns_cap key histogram (then its prefix over chunks)
     int32_t* cnt;                // per chosen slot: members in the last pass
     int32_t* base;               // per chosen slot: first slot of its segment of perm
     int32_t* hash;               // choose hash heads
@@ -76,7 +81,7 @@ struct EngineView {
     unsigned long long* pairs;   // per cloud: sum over passes of n_all * ns
     int32_t* ctr;                // CTR_* counters
     int32_t* act_cloud;          // evolving clouds, in cloud order (n_clouds)
-    int32_t* act_pre;            // 3 x (n_clouds+1) exclusive prefixes of their work items
+    int32_t* act_pre;            // ACT_KINDS x (n_clouds+1) exclusive prefixes of their work items
     int32_t* group_conv;         // per group: members converged in this round
     int32_t* ready;              // groups ready for decimation (n_groups)
     // decimation scratch, per group (offsets in GroupDesc / dec_hoff)
@@ -99,7 +104,8 @@ struct EngineView {
     int32_t n_groups;
     int32_t n_chunks;
     int32_t n_slots;
-    int32_t n_segs;
+    int32_t n_kblk;              // blocks of KBLK chosen slots, clouds of > SCAN_ROWS_WARP chunks
+    int32_t n_kblk_warp;         // the same over the other clouds
     int32_t chunk_pts;           // max points per assignment chunk (BLOCK*ITEMS)
     int32_t chunk_max;           // largest chunk actually used (scatter staging)
     int32_t hist_smem;           // ints of dynamic smem for the assign histogram

@@ -110,10 +110,9 @@ private:
     std::vector<CloudDesc> h_cl_;
     std::vector<GroupDesc> h_gr_;
     std::vector<int32_t> h_chunk_cloud_, h_slot_cloud_, h_ns_, h_err_;
-    std::vector<int2> h_seg_list_;
     std::vector<int64_t> h_dec_hoff_;
     std::vector<int32_t> h_dec_hbits_;
-    int32_t n_chunks_ = 0, n_slots_ = 0, n_segs_ = 0;
+    int32_t n_chunks_ = 0, n_slots_ = 0, n_kblk_ = 0, n_kblk_warp_ = 0;
     int chunk_pts_ = 1024;
     int chunk_max_ = 0;
     int sms_ = 148;
@@ -121,8 +120,8 @@ private:
     int assign_grid_ = 0;
     RunStats stats_;
 
-    DevBuf bCl_, bGr_, bChunkCloud_, bSlotCloud_, bSegList_;
-    DevBuf bP_, bS_, bKeys_, bGrouped_, bHist_, bSegsum_, bCnt_, bBase_, bNext_, bHash_, bSurv_;
+    DevBuf bCl_, bGr_, bChunkCloud_, bSlotCloud_;
+    DevBuf bP_, bS_, bKeys_, bGrouped_, bHist_, bCnt_, bBase_, bNext_, bHash_, bSurv_;
     DevBuf bNs_, bPhase_, bCont_, bPasses_, bTotPasses_, bOuter_, bErr_, bPairs_, bCtr_;
     DevBuf bActCloud_, bActPre_, bGroupConv_, bReady_, bDnbOff_, bDnb_, bDbig_, bDcpre_;
     int dec_smem_max_ = 0;

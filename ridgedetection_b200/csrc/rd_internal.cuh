@@ -54,9 +54,7 @@ struct CloudDesc {
     int32_t n_chunks;
     int32_t group;
     int64_t hist_off;    // start of this cloud's chunk x key histogram (set after choose)
-    int32_t n_seg;       // ceil(n_chunks / SEG)
     int32_t ns_cap;      // chosen count right after choose (hist row length)
-    int64_t seg_off;     // start of this cloud's segment x key sums
     int64_t key_off;     // start of this cloud's per-chosen arrays (cnt/base)
     int64_t hash_off;    // start of this cloud's choose hash heads
     int32_t hash_bits;   // log2 of the number of hash buckets
@@ -71,7 +69,7 @@ struct GroupDesc {
     int64_t s_scratch;   // first scratch slot of the group's decimation
 };
 
-constexpr int SEG = 16;  // histogram rows per segment in the column scan
+constexpr int KBLK = 32;  // chosen points per histogram-scan block (one per lane)
 
 // ---------------------------------------------------------------------------
 // exact FP32 helpers

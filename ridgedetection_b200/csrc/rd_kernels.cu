@@ -19,9 +19,8 @@ namespace {
 
 // Work lists over the clouds still evolving, rebuilt by k_loopcond after every
 // iteration: act_cloud[a] is the a-th evolving cloud and act_pre[kind] the
-// exclusive prefix of its work items (chunks, histogram segments or chosen
-// slots), so kernels launched over fixed grids touch only active work.
-enum : int { ACT_CHUNK = 0, ACT_SEG = 1, ACT_SLOT = 2, ACT_KINDS = 3 };
+// exclusive prefix of its work items (ACT_* in rd_engine.cuh), so kernels
+// launched over fixed grids touch only active work.
 
 struct ActiveList {
     const int32_t* pre;
@@ -489,104 +488,138 @@ __global__ void __launch_bounds__(BLOCK) k_assign(EngineView v)
 }
 
 // ---------------------------------------------------------------------------
-// column scan: per (cloud, segment of SEG chunk rows) and key, in-place
-// exclusive prefix down the rows and the segment total.
+// Chunk scan: for every chosen point k of a cloud, the exclusive prefix over
+// the cloud's chunks of the chunk x key histogram (in place: afterwards row lc
+// holds, for each key, the members in earlier chunks) and the member count
+// cnt[k].  Work item = block of KBLK keys, one key per lane.
+//   k_chunkscan_cta   clouds with more than SCAN_ROWS_WARP chunk rows: one CTA
+//                     per item; the CS_W warps take contiguous row ranges, sum
+//                     them, exchange the warp totals, and rescan their rows
+//                     writing the prefixes;
+//   k_chunkscan_warp  the other clouds: one warp per item, a single pass.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_colscan(EngineView v)
+constexpr int CS_W = 16;   // warps of the CTA-wide scan
+constexpr int CSW_W = 8;   // items (warps) per CTA of the warp-wide scan
+constexpr int CS_LOADS = 16;  // histogram loads in flight per lane
+
+__global__ void __launch_bounds__(CS_W * 32) k_chunkscan_cta(EngineView v)
 {
-    const ActiveList al(v, ACT_SEG);
+    __shared__ int s_part[CS_W][32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const ActiveList al(v, ACT_KBLK);
     for (int item = blockIdx.x; item < al.total; item += gridDim.x) {
-    int c, seg;
-    al.locate(item, c, seg);
-    const CloudDesc cd = v.cl[c];
-    const int ns = v.ns[c];
-    const int r0 = seg * SEG;
-    const int rows = min(SEG, cd.n_chunks - r0);
-    int32_t* h = v.hist + cd.hist_off + (int64_t)r0 * cd.ns_cap;
-    int32_t* out = v.segsum + cd.seg_off + (int64_t)seg * cd.ns_cap;
-    for (int k = threadIdx.x; k < ns; k += blockDim.x) {
-        int x[SEG];  // all loads in flight before the dependent prefix
+        int c, kb;
+        al.locate(item, c, kb);
+        const CloudDesc cd = v.cl[c];
+        const int k = kb * KBLK + lane;
+        const bool ok = k < v.ns[c];
+        const int rows = cd.n_chunks;
+        const int rw0 = (warp * rows) / CS_W, rw1 = ((warp + 1) * rows) / CS_W;
+        int32_t* h = v.hist + cd.hist_off + k;
+        int sum = 0;
+        for (int r0 = rw0; r0 < rw1; r0 += CS_LOADS) {
+            int x[CS_LOADS];
 #pragma unroll
-        for (int r = 0; r < SEG; ++r) x[r] = (r < rows) ? h[(int64_t)r * cd.ns_cap + k] : 0;
-        int run = 0;
+            for (int u = 0; u < CS_LOADS; ++u)
+                x[u] = (ok && r0 + u < rw1) ? h[(int64_t)(r0 + u) * cd.ns_cap] : 0;
 #pragma unroll
-        for (int r = 0; r < SEG; ++r) {
-            if (r < rows) h[(int64_t)r * cd.ns_cap + k] = run;
-            run += x[r];
+            for (int u = 0; u < CS_LOADS; ++u) sum += x[u];
         }
-        out[k] = run;
-    }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// segment scan + key bases: one CTA per cloud.  Exclusive prefix of the
-// segment totals per key (in place), member count per key, and the exclusive
-// prefix of the counts over keys (first grouped slot of each key).
-// ---------------------------------------------------------------------------
-template <int BLOCK>
-__device__ void segscan_one(const EngineView& v, int c, int* s_w, int* s_carry_p);
-
-template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_segscan(EngineView v)
-{
-    __shared__ int s_w[BLOCK / 32];
-    __shared__ int s_carry;
-    const int nact = v.ctr[CTR_NACT];
-    for (int a = blockIdx.x; a < nact; a += gridDim.x) {
-        __syncthreads();  // previous cloud's readers of s_w / s_carry are done
-        segscan_one<BLOCK>(v, v.act_cloud[a], s_w, &s_carry);
-    }
-}
-
-template <int BLOCK>
-__device__ void segscan_one(const EngineView& v, int c, int* s_w, int* s_carry_p)
-{
-    int& s_carry = *s_carry_p;
-    const CloudDesc cd = v.cl[c];
-    const int ns = v.ns[c];
-    int32_t* sg = v.segsum + cd.seg_off;
-    int32_t* cnt = v.cnt + cd.key_off;
-    int32_t* base = v.base + cd.key_off;
-    for (int k = threadIdx.x; k < ns; k += BLOCK) {
-        int run = 0;
-        for (int s0 = 0; s0 < cd.n_seg; s0 += 16) {  // 16 loads in flight per step
-            int x[16];
+        s_part[warp][lane] = sum;
+        __syncthreads();
+        int run = 0, tot = 0;
 #pragma unroll
-            for (int u = 0; u < 16; ++u)
-                x[u] = (s0 + u < cd.n_seg) ? sg[(int64_t)(s0 + u) * cd.ns_cap + k] : 0;
+        for (int w = 0; w < CS_W; ++w) {
+            const int y = s_part[w][lane];
+            run += (w < warp) ? y : 0;
+            tot += y;
+        }
+        for (int r0 = rw0; r0 < rw1; r0 += CS_LOADS) {
+            int x[CS_LOADS];
 #pragma unroll
-            for (int u = 0; u < 16; ++u) {
-                if (s0 + u < cd.n_seg) sg[(int64_t)(s0 + u) * cd.ns_cap + k] = run;
+            for (int u = 0; u < CS_LOADS; ++u)
+                x[u] = (ok && r0 + u < rw1) ? h[(int64_t)(r0 + u) * cd.ns_cap] : 0;
+#pragma unroll
+            for (int u = 0; u < CS_LOADS; ++u) {
+                if (ok && r0 + u < rw1) h[(int64_t)(r0 + u) * cd.ns_cap] = run;
                 run += x[u];
             }
         }
-        cnt[k] = run;
+        if (warp == 0 && ok) v.cnt[cd.key_off + k] = tot;
+        __syncthreads();  // s_part is reused by the next item
     }
-    __syncthreads();
-    if (threadIdx.x == 0) s_carry = 0;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int k0 = 0; k0 < ns; k0 += BLOCK) {
-        __syncthreads();
-        const int k = k0 + threadIdx.x;
-        const int x = (k < ns) ? cnt[k] : 0;
-        int incl = x;
+}
+
+__global__ void __launch_bounds__(CSW_W * 32) k_chunkscan_warp(EngineView v)
+{
+    const int lane = threadIdx.x & 31;
+    const ActiveList al(v, ACT_KBLK_WARP);
+    const int stride = gridDim.x * CSW_W;
+    for (int item = blockIdx.x * CSW_W + (threadIdx.x >> 5); item < al.total; item += stride) {
+        int c, kb;
+        al.locate(item, c, kb);
+        const CloudDesc cd = v.cl[c];
+        const int k = kb * KBLK + lane;
+        const bool ok = k < v.ns[c];
+        const int rows = cd.n_chunks;
+        int32_t* h = v.hist + cd.hist_off + k;
+        int run = 0;
+        for (int r0 = 0; r0 < rows; r0 += CS_LOADS) {
+            int x[CS_LOADS];
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(FULL, incl, o);
-            if (lane >= o) incl += y;
+            for (int u = 0; u < CS_LOADS; ++u)
+                x[u] = (ok && r0 + u < rows) ? h[(int64_t)(r0 + u) * cd.ns_cap] : 0;
+#pragma unroll
+            for (int u = 0; u < CS_LOADS; ++u) {
+                if (ok && r0 + u < rows) h[(int64_t)(r0 + u) * cd.ns_cap] = run;
+                run += x[u];
+            }
         }
-        if (lane == 31) s_w[warp] = incl;
-        __syncthreads();
-        int wpre = 0, tot = 0;
-        for (int w = 0; w < BLOCK / 32; ++w) {
-            wpre += (w < warp) ? s_w[w] : 0;
-            tot += s_w[w];
+        if (ok) v.cnt[cd.key_off + k] = run;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Key bases: one CTA per evolving cloud, exclusive prefix of the member
+// counts over its keys (first grouped slot of each key).
+// ---------------------------------------------------------------------------
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_keybase(EngineView v)
+{
+    __shared__ int s_w[BLOCK / 32];
+    __shared__ int s_carry;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nact = v.ctr[CTR_NACT];
+    for (int a = blockIdx.x; a < nact; a += gridDim.x) {
+        __syncthreads();  // the previous cloud's readers of s_w / s_carry are done
+        const int c = v.act_cloud[a];
+        const CloudDesc cd = v.cl[c];
+        const int ns = v.ns[c];
+        const int32_t* cnt = v.cnt + cd.key_off;
+        int32_t* base = v.base + cd.key_off;
+        if (threadIdx.x == 0) s_carry = 0;
+        for (int k0 = 0; k0 < ns; k0 += BLOCK) {
+            __syncthreads();
+            const int k = k0 + threadIdx.x;
+            const int x = (k < ns) ? cnt[k] : 0;
+            int incl = x;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += y;
+            }
+            if (lane == 31) s_w[warp] = incl;
+            __syncthreads();
+            int wpre = 0, tot = 0;
+            for (int w = 0; w < BLOCK / 32; ++w) {
+                wpre += (w < warp) ? s_w[w] : 0;
+                tot += s_w[w];
+            }
+            const int carry = s_carry;
+            if (k < ns) base[k] = carry + wpre + incl - x;
+            __syncthreads();
+            if (threadIdx.x == 0) s_carry = carry + tot;
         }
-        const int carry = s_carry;
-        if (k < ns) base[k] = carry + wpre + incl - x;
-        __syncthreads();
-        if (threadIdx.x == 0) s_carry = carry + tot;
     }
 }
 
@@ -643,12 +676,10 @@ __global__ void __launch_bounds__(SCAT_W * 32) k_scatter_cta(EngineView v)
             if (r.key >= 0 && lane == r.head) atomicAdd(&hw[warp * ns + r.key], r.count);
         }
         __syncthreads();
-        const int seg = lc / SEG;
         const int32_t* row = v.hist + cd.hist_off + (int64_t)lc * cd.ns_cap;
-        const int32_t* sg = v.segsum + cd.seg_off + (int64_t)seg * cd.ns_cap;
         const int32_t* bs = v.base + cd.key_off;
         for (int k = tid; k < ns; k += SCAT_W * 32) {
-            int run = bs[k] + sg[k] + row[k];
+            int run = bs[k] + row[k];
 #pragma unroll
             for (int w = 0; w < SCAT_W; ++w) {
                 const int x = hw[w * ns + k];
@@ -685,9 +716,7 @@ __device__ void scatter_chunk(const EngineView& v, int c, int lc, int* s_keys, i
 {
     const CloudDesc cd = v.cl[c];
     const int ns = v.ns[c];
-    const int seg = lc / SEG;
     int32_t* row = v.hist + cd.hist_off + (int64_t)lc * cd.ns_cap;
-    const int32_t* sg = v.segsum + cd.seg_off + (int64_t)seg * cd.ns_cap;
     const int32_t* bs = v.base + cd.key_off;
     const bool in_smem = ns <= v.scat_smem;
     int32_t* ctr = in_smem ? (s_keys + v.chunk_max) : row;
@@ -712,18 +741,17 @@ __device__ void scatter_chunk(const EngineView& v, int c, int lc, int* s_keys, i
         }
     }
     for (int k0 = 0; k0 < ns; k0 += 32 * 4) {
-        int a[4], b2[4], r[4];
+        int a[4], r[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int k = k0 + u * 32 + lane;
             a[u] = (k < ns) ? bs[k] : 0;
-            b2[u] = (k < ns) ? sg[k] : 0;
             r[u] = (k < ns) ? row[k] : 0;
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int k = k0 + u * 32 + lane;
-            if (k < ns) ctr[k] = a[u] + b2[u] + r[u];
+            if (k < ns) ctr[k] = a[u] + r[u];
         }
     }
     __syncwarp();
@@ -1486,31 +1514,34 @@ __global__ void __launch_bounds__(1024) k_loopcond(EngineView v, cudaGraphCondit
                                                    int use_handle, int count_iter)
 {
     __shared__ int s_act;
-    __shared__ int s_w[32][4];
-    __shared__ int s_carry[4];
+    __shared__ int s_w[32][ACT_KINDS + 1];
+    __shared__ int s_carry[ACT_KINDS + 1];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) {
         s_act = 0;
-        s_carry[0] = s_carry[1] = s_carry[2] = s_carry[3] = 0;
+        for (int q = 0; q <= ACT_KINDS; ++q) s_carry[q] = 0;
     }
     __syncthreads();
     int act = 0;
     for (int c = tid; c < v.n_clouds; c += blockDim.x) act += (v.phase[c] != PH_DONE);
     if (act) atomicAdd(&s_act, act);
     // work lists of the next iteration: evolving clouds, prefixes of their
-    // chunks, histogram segments and chosen slots
+    // chunks, chosen-point blocks and chosen slots
     const int nc = v.n_clouds;
     for (int c0 = 0; c0 < nc; c0 += blockDim.x) {
         const int c = c0 + tid;
         const bool ev = (c < nc) && v.phase[c] == PH_EVOLVE;
-        int x[4];
+        int x[ACT_KINDS + 1];
         x[0] = ev ? 1 : 0;
-        x[1] = ev ? v.cl[c].n_chunks : 0;
-        x[2] = ev ? v.cl[c].n_seg : 0;
-        x[3] = ev ? v.ns[c] : 0;
-        int incl[4];
+        const int rows = ev ? v.cl[c].n_chunks : 0;
+        const int nkb = ev ? (v.ns[c] + KBLK - 1) / KBLK : 0;
+        x[1 + ACT_CHUNK] = rows;
+        x[1 + ACT_KBLK] = rows > SCAN_ROWS_WARP ? nkb : 0;
+        x[1 + ACT_KBLK_WARP] = rows > SCAN_ROWS_WARP ? 0 : nkb;
+        x[1 + ACT_SLOT] = ev ? v.ns[c] : 0;
+        int incl[ACT_KINDS + 1];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q <= ACT_KINDS; ++q) {
             incl[q] = x[q];
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -1520,9 +1551,9 @@ __global__ void __launch_bounds__(1024) k_loopcond(EngineView v, cudaGraphCondit
             if (lane == 31) s_w[warp][q] = incl[q];
         }
         __syncthreads();
-        int excl[4], tot[4];
+        int excl[ACT_KINDS + 1], tot[ACT_KINDS + 1];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q <= ACT_KINDS; ++q) {
             int pre = 0, t = 0;
             for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
                 pre += (w < warp) ? s_w[w][q] : 0;
@@ -1533,22 +1564,19 @@ __global__ void __launch_bounds__(1024) k_loopcond(EngineView v, cudaGraphCondit
         }
         if (ev) {
             v.act_cloud[excl[0]] = c;
-            v.act_pre[ACT_CHUNK * (nc + 1) + excl[0]] = excl[1];
-            v.act_pre[ACT_SEG * (nc + 1) + excl[0]] = excl[2];
-            v.act_pre[ACT_SLOT * (nc + 1) + excl[0]] = excl[3];
+#pragma unroll
+            for (int q = 0; q < ACT_KINDS; ++q) v.act_pre[q * (nc + 1) + excl[0]] = excl[1 + q];
         }
         __syncthreads();
         if (tid == 0) {
 #pragma unroll
-            for (int q = 0; q < 4; ++q) s_carry[q] += tot[q];
+            for (int q = 0; q <= ACT_KINDS; ++q) s_carry[q] += tot[q];
         }
         __syncthreads();
     }
     if (tid == 0) {
         const int nact = s_carry[0];
-        v.act_pre[ACT_CHUNK * (nc + 1) + nact] = s_carry[1];
-        v.act_pre[ACT_SEG * (nc + 1) + nact] = s_carry[2];
-        v.act_pre[ACT_SLOT * (nc + 1) + nact] = s_carry[3];
+        for (int q = 0; q < ACT_KINDS; ++q) v.act_pre[q * (nc + 1) + nact] = s_carry[1 + q];
         v.ctr[CTR_NACT] = nact;
         v.ctr[CTR_WORK] = 0;
         v.ctr[CTR_NREADY] = 0;
@@ -1640,8 +1668,10 @@ cudaError_t launch_pass_dim(const EngineView& v, const TuneParams& tp, int assig
     if (a1) cudaEventRecord(a1, st);
     // fixed grids; every kernel walks only the current work lists
     const int sms = v.n_sms;
-    if (v.n_segs > 0) k_colscan<<<std::min(v.n_segs, sms * 8), 256, 0, st>>>(v);
-    k_segscan<1024><<<std::min(v.n_clouds, sms * 2), 1024, 0, st>>>(v);
+    if (v.n_kblk > 0) k_chunkscan_cta<<<std::min(v.n_kblk, sms * 4), CS_W * 32, 0, st>>>(v);
+    if (v.n_kblk_warp > 0)
+        k_chunkscan_warp<<<std::min((v.n_kblk_warp + CSW_W - 1) / CSW_W, sms * 8), CSW_W * 32, 0, st>>>(v);
+    k_keybase<1024><<<std::min(v.n_clouds, sms * 2), 1024, 0, st>>>(v);
     if (v.n_chunks > 0)
         k_scatter_cta<<<std::min(v.n_chunks, sms * 8), SCAT_W * 32, scatter_cta_smem_bytes(v), st>>>(v);
     if (v.n_slots > 0) k_sum_shift<DIM><<<std::min((v.n_slots + 7) / 8, sms * 8), 256, 0, st>>>(v);
@@ -1853,8 +1883,10 @@ cudaError_t launch_evolve_step_dim(const EngineView& v, const TuneParams& tp, in
     RD_ASSIGN_CASE(128, 16)
     { return cudaErrorInvalidValue; }
 #undef RD_ASSIGN_CASE
-    if (v.n_segs > 0) k_colscan<<<std::min(v.n_segs, sms * 8), 256, 0, st>>>(v);
-    k_segscan<1024><<<std::min(v.n_clouds, sms * 2), 1024, 0, st>>>(v);
+    if (v.n_kblk > 0) k_chunkscan_cta<<<std::min(v.n_kblk, sms * 4), CS_W * 32, 0, st>>>(v);
+    if (v.n_kblk_warp > 0)
+        k_chunkscan_warp<<<std::min((v.n_kblk_warp + CSW_W - 1) / CSW_W, sms * 8), CSW_W * 32, 0, st>>>(v);
+    k_keybase<1024><<<std::min(v.n_clouds, sms * 2), 1024, 0, st>>>(v);
     if (v.n_chunks > 0)
         k_scatter_cta<<<std::min(v.n_chunks, sms * 8), SCAT_W * 32, scatter_cta_smem_bytes(v), st>>>(v);
     if (v.n_slots > 0) k_sum_shift<DIM><<<std::min((v.n_slots + 7) / 8, sms * 8), 256, 0, st>>>(v);
