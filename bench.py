@@ -54,6 +54,8 @@ def parse_args():
                              "spiral2d_1m_tiled"])
     ap.add_argument("--clouds", type=int, default=4096, help="batch workload: number of clouds")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--assign-cull", default="on", choices=["on", "off"],
+                    help="exact chunk-box culling of the brute-force assignment (off = all-pairs kernel)")
     ap.add_argument("--shape", default=None,
                     help="BLOCK,ITEMS of the assignment kernel instead of the autotuner's pick "
                          "(a profiler distorts the tuner's timings)")
@@ -82,6 +84,19 @@ def run_profile(args):
     """Solves with the host-driven loop for profilers (see --profile-run)."""
     import torch
     import ridgedetection_b200 as rdb
+    if args.workload == "batch":
+        from ridgedetection_b200 import generators as G
+        spec = G.batch_spec(args.clouds)
+        clouds = [(G.batch_cloud(n, dim, seed), r1, r2) for (n, dim, r1, r2, seed) in spec]
+        packed, descs = rdb.pack_clouds(clouds)
+        dpk = torch.from_numpy(packed).cuda()
+        b = rdb.BatchedRidgeDetection(loop_mode=rdb.LOOP_HOST)
+        for _ in range(args.warmup + args.steps):
+            b.run(dpk, descs)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_run": "batch", "clouds": args.clouds,
+                          "solves": args.warmup + args.steps}))
+        return
     P, r1, r2 = workload(args.workload)
     n, dim = P.shape
     dP = torch.from_numpy(P).cuda()
@@ -654,6 +669,9 @@ def run_b200_batch(args, world, rank, local):
 def main():
     args = parse_args()
     world, rank, local = dist_setup(args)
+    if args.impl != "reference":
+        import ridgedetection_b200 as rdb
+        rdb.set_assign_cull(args.assign_cull == "on")
     if args.profile_run:
         run_profile(args)
         return

@@ -85,6 +85,16 @@ RD_API rd_status rd_probe_fp32_peak(double* tflops, void* stream);
 RD_API rd_status rd_tune_set(int dim, int64_t n, int block, int items);
 RD_API rd_status rd_tune_get(int dim, int64_t n, int* block, int* items);
 RD_API rd_status rd_tune_reset(void);
+/* Exact culling of the brute-force assignment (no reference counterpart; it
+ * replaces nothing and changes no result).  rd/cpu/brute_force/evolve.hpp:43-66
+ * compares every cloud point with every chosen point but keeps the nearest
+ * only when it lies within r1.  With culling on (the default), each chunk of
+ * spatially sorted points compares only the chosen points whose distance to
+ * the chunk's bounding box can be within r1 (with a rounding margin), giving
+ * the same assignment bit for bit.  Off = the all-pairs kernel.  Process-wide,
+ * read when a run starts. */
+RD_API rd_status rd_set_assign_cull(int enable);
+RD_API rd_status rd_get_assign_cull(int* enable);
 /* Times every supported shape on the cloud d_P (device, n x dim ROW_MAJOR;
  * NULL = n synthetic points uniform in the unit cube) with its first ns points
  * as the chosen set and assignment radius r1: the assignment kernel is timed

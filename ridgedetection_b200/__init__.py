@@ -11,10 +11,11 @@ from .api import (COL_MAJOR, LOOP_GRAPH, LOOP_HOST, ROW_MAJOR, TILED_LOCAL,  # n
                   BatchedRidgeDetection, BruteForceRidgeDetection, TiledRidgeDetection,
                   autotune, choose_count, load_binary_cloud, load_text_cloud, order_chains,
                   pack_clouds, save_binary_cloud, hausdorff, distance_stats, segment_hausdorff, ridge_detection,
-                  tiled_ridge_detection, tune_get, tune_reset, tune_set)
+                  tiled_ridge_detection, tune_get, tune_reset, tune_set, set_assign_cull,
+                  get_assign_cull)
 
 __all__ = ["BruteForceRidgeDetection", "BatchedRidgeDetection", "TiledRidgeDetection",
            "ridge_detection", "tiled_ridge_detection",
-           "pack_clouds", "order_chains", "hausdorff", "distance_stats", "segment_hausdorff", "load_text_cloud", "load_binary_cloud", "save_binary_cloud", "autotune", "choose_count", "tune_get", "tune_set", "tune_reset",
+           "pack_clouds", "order_chains", "hausdorff", "distance_stats", "segment_hausdorff", "load_text_cloud", "load_binary_cloud", "save_binary_cloud", "autotune", "choose_count", "tune_get", "tune_set", "tune_reset", "set_assign_cull", "get_assign_cull",
            "ROW_MAJOR", "TILED_MIXED", "TILED_LOCAL", "COL_MAJOR", "LOOP_GRAPH", "LOOP_HOST", "RDError",
            "RunStats", "lib", "generators"]

@@ -65,6 +65,8 @@ SIGNATURES = {
     "rd_tune_set": [ctypes.c_int, ctypes.c_int64, ctypes.c_int, ctypes.c_int],
     "rd_tune_get": [ctypes.c_int, ctypes.c_int64, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
     "rd_tune_reset": [],
+    "rd_set_assign_cull": [ctypes.c_int],
+    "rd_get_assign_cull": [ctypes.POINTER(ctypes.c_int)],
     "rd_autotune": [ctypes.c_int, _vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_float, ctypes.c_int,
                     ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                     ctypes.POINTER(ctypes.c_double), _vp],

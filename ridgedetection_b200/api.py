@@ -330,6 +330,20 @@ def tune_reset() -> None:
     L.check(L.lib().rd_tune_reset())
 
 
+def set_assign_cull(enable: bool) -> None:
+    """Switch the exact chunk-box culling of the brute-force assignment
+    (process-wide, on by default).  Results are the same either way; off runs
+    the all-pairs assignment kernel."""
+    L.check(L.lib().rd_set_assign_cull(1 if enable else 0))
+
+
+def get_assign_cull() -> bool:
+    """Whether runs started now use the culled assignment."""
+    e = ctypes.c_int(0)
+    L.check(L.lib().rd_get_assign_cull(ctypes.byref(e)))
+    return bool(e.value)
+
+
 def choose_count(P, r1: float) -> int:
     """Number of points the greedy r1-ball choose keeps for the cloud P (a
     float32 CUDA tensor or numpy array, ROW_MAJOR n x dim)."""

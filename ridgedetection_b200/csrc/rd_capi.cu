@@ -287,6 +287,19 @@ rd_status rd_tune_reset(void)
     return RD_OK;
 }
 
+rd_status rd_set_assign_cull(int enable)
+{
+    set_assign_cull(enable != 0);
+    return RD_OK;
+}
+
+rd_status rd_get_assign_cull(int* enable)
+{
+    if (!enable) return set_err(RD_ERR_ARG, "null argument");
+    *enable = assign_cull_enabled() ? 1 : 0;
+    return RD_OK;
+}
+
 rd_status rd_autotune(int dim, const float* d_P, int64_t n, int64_t ns, float r1, int reps,
                       int* block, int* items, double* us_per_launch, void* stream)
 {

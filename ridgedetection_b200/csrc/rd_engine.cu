@@ -2,6 +2,7 @@
 #include "rd_engine_host.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -48,6 +49,10 @@ const std::vector<TuneParams>& tune_candidates()
     return c;
 }
 
+
+static std::atomic<int> g_assign_cull{1};
+void set_assign_cull(bool on) { g_assign_cull.store(on ? 1 : 0); }
+bool assign_cull_enabled() { return g_assign_cull.load() != 0; }
 
 cudaError_t DevBuf::ensure(size_t want)
 {
@@ -145,6 +150,15 @@ int Engine::setup(int dim, const std::vector<CloudDesc>& clouds,
     }
     n_chunks_ = (int32_t)chunk;
     const size_t nc = h_cl_.size();
+    // the spatial order sorts by (cloud, cell): clouds must tile [0, total)
+    // in cloud order
+    spatial_ok_ = total_points < (int64_t(1) << 31) - 1;
+    int64_t next_off = 0;
+    for (const CloudDesc& cd : h_cl_) {
+        spatial_ok_ = spatial_ok_ && cd.p_off == next_off;
+        next_off += cd.n_all;
+    }
+    spatial_ok_ = spatial_ok_ && next_off == total_points;
     RD_CK(bP_.ensure(sizeof(float) * (size_t)(total_points * dim + 4)));
     RD_CK(bS_.ensure(sizeof(float) * (size_t)(s_off * dim + 4)));
     RD_CK(bNext_.ensure(sizeof(int32_t) * (size_t)(s_off + 1)));
@@ -226,6 +240,9 @@ EngineView Engine::view() const
     v.max_passes = max_passes;
     v.max_outer = max_outer;
     v.max_iters = max_iters;
+    v.Ps = bPs_.as<float>();
+    v.sorder = bSorder_.as<int32_t>();
+    v.cull = cull_ ? 1 : 0;
     v.n_sms = sms_;
     v.flags = flags_;
     return v;
@@ -412,6 +429,16 @@ int Engine::run(cudaStream_t st, bool use_graph, int mode)
     for (const CloudDesc& cd : h_cl_) max_ns = std::max(max_ns, cd.ns_cap);
     fused_ = fuse_tiles && h_gr_.size() == 1 && h_cl_.size() > 1 && max_ns <= TILE_NS_MAX &&
              flags_ == 0;
+    cull_ = cull_assign && assign_cull_enabled() && !fused_ && spatial_ok_ && total_points_ > 0;
+    if (cull_) {
+        const size_t scratch = spatial_prep_scratch_bytes(total_points_);
+        RD_CK(bPs_.ensure(sizeof(float) * (size_t)(total_points_ * dim_ + 4)));
+        RD_CK(bSorder_.ensure(sizeof(int32_t) * (size_t)(total_points_ + 1)));
+        RD_CK(bSpatialTmp_.ensure(scratch));
+        const EngineView vs = view();
+        RD_CK(launch_spatial_prep(dim_, vs, total_points_, bSpatialTmp_.p, scratch, bPs_.as<float>(),
+                                  bSorder_.as<int32_t>(), st));
+    }
     const EngineView v = view();
     RD_CK(prepare_pass(dim_, v, tune));
     if (fused_) RD_CK(prepare_tile_pass(dim_, v));
@@ -461,6 +488,7 @@ int Engine::adjoint_setup(cudaStream_t st)
     }
     stats_ = RunStats();
     flags_ = ENG_ALWAYS_MOVE;
+    cull_ = false;
     RD_CK(upload(bCl_, h_cl_, st));
     RD_CK(upload(bGr_, h_gr_, st));
     EngineView v0 = view();

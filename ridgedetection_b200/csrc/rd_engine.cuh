@@ -115,6 +115,10 @@ struct EngineView {
     int32_t max_iters;
     int32_t n_sms;
     int32_t flags;               // ENG_* run-mode bits
+    // exact chunk-box culling of the assignment (see k_assign_cull)
+    const float* Ps;             // evolve points in spatial order inside each cloud
+    const int32_t* sorder;       // spatial position -> packed point slot
+    int32_t cull;                // passes assign with k_assign_cull + k_keyhist
 };
 
 // dynamic shared memory of the decimation kernel: two int16 counts and an
@@ -171,6 +175,14 @@ cudaError_t launch_order_chains(int dim, const float* S, int ns, float rsq, unsi
 // out[d] = ordered FP32 sum of P[idx[i]*dim + d] (method 0 chain, 1 parallel exact)
 cudaError_t launch_ordered_sum(int dim, const float* P, const int32_t* idx, int n, float* out,
                                int method, cudaStream_t st);
+// Spatial order of every cloud's points for the culled assignment: cells of
+// edge r1/4, Morton order of the cells (cloud first), slot order inside a
+// cell; Ps/sorder receive the reordered points and their slots.  Needs
+// contiguous clouds in cloud order and n_points < 2^31; scratch of
+// spatial_prep_scratch_bytes(n).
+size_t spatial_prep_scratch_bytes(int64_t n_points);
+cudaError_t launch_spatial_prep(int dim, const EngineView& v, int64_t n_points, void* scratch,
+                                size_t scratch_bytes, float* Ps, int32_t* sorder, cudaStream_t st);
 // the five kernels of one evolve pass without control/decimation (adjoint forward)
 cudaError_t launch_evolve_step(int dim, const EngineView& v, const TuneParams& tp, int assign_grid,
                                cudaStream_t st);

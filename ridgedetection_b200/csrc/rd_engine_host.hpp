@@ -41,6 +41,10 @@ void tune_store(int dim, int64_t n, const TuneParams& tp);
 void tune_clear();
 // supported launch shapes, in a fixed order
 const std::vector<TuneParams>& tune_candidates();
+// Process-wide switch of the exact chunk-box culling of the assignment (on by
+// default); read by every engine run.  Thread-safe.
+void set_assign_cull(bool on);
+bool assign_cull_enabled();
 
 class Engine {
 public:
@@ -95,6 +99,7 @@ public:
     bool tune_locked = false;     // keep `tune`; otherwise setup() takes tune_lookup()
     bool profile_assign = false;  // host loop only: time every assign launch with events
     bool fuse_tiles = true;       // tiled runs: per-tile evolve kernel (see run())
+    bool cull_assign = true;      // lockstep passes: exact chunk-box culling of the assignment
     std::string last_error;
 
 private:
@@ -127,6 +132,9 @@ private:
     int dec_smem_max_ = 0;
     int dec_nb_pp_ = DEC_NB_MIN_PER_POINT;
     bool fused_ = false;
+    bool cull_ = false;           // this run assigns with culling
+    bool spatial_ok_ = false;     // the batch layout allows the spatial order
+    DevBuf bPs_, bSorder_, bSpatialTmp_;
     DevBuf bDx_, bDcell_, bDalive_, bDc1_, bDc2_, bDbstart_, bDitems_, bDecHoff_, bDecHbits_;
 
     cudaStream_t cap_stream_ = nullptr;

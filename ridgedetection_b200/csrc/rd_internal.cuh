@@ -112,6 +112,20 @@ __device__ __forceinline__ float2 sqdist2_exact(const float* s, const float2* np
 
 __device__ __forceinline__ float sqr_rn(float r) { return __fmul_rn(r, r); }
 
+// Cells of the spatial order used by the culled assignment: cell coordinate
+// floor(x * inv) with inv = 4 / r1 (edge r1/4), wrapped to 32 bits;
+// non-finite or huge coordinates land in cell 0.  The order only changes how
+// tight the culling boxes are, never a result.
+__device__ __forceinline__ float spatial_cell_inv(float r1) { return 4.0f / r1; }
+
+__device__ __forceinline__ uint32_t spatial_cell(float x, float inv)
+{
+    const float f = floorf(x * inv);
+    if (!(f > -1.0e15f && f < 1.0e15f)) return 0u;
+    return (uint32_t)(uint64_t)(int64_t)f;
+}
+
+
 // Runs of equal keys of a warp, for stable grouping without match
 // instructions (the match instruction's throughput drops when a warp holds
 // many distinct keys, as in a brute-force cloud visited in random order): the 32 (key, lane) pairs are sorted by key, ties by lane

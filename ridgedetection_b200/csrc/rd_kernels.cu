@@ -488,6 +488,186 @@ __global__ void __launch_bounds__(BLOCK) k_assign(EngineView v)
 }
 
 // ---------------------------------------------------------------------------
+// Culled assignment: the same keys as k_assign, over chunks of the spatial
+// order (Ps, built once per run by launch_spatial_prep) instead of the slot
+// order.  Each warp takes 128 consecutive points of that order (4 per lane)
+// and their bounding box; a chosen point s takes part in the warp's argmin
+// only when the squared gap between s and the box, g2, is at most
+// thr = r1^2 (1 + 2^-10) (rounded up).  Exactness: the computed g2 exceeds the
+// exact squared gap G by at most a relative 2^-20 (a few roundings of
+// non-negative terms), and every computed distance from s to a point of the
+// box is at least G (1 - 2^-20); so g2 > thr makes every such distance > r1^2.
+// A skipped chosen point can then neither be the nearest one within r1 nor tie
+// with it, and the minimum over the remaining points, visited in index order
+// with strict '<', is the reference's (rd/cpu/brute_force/evolve.hpp:54-66).
+// The bound needs r1^2 in the normal range; any other r1 disables the skip.
+// NaN gaps never skip.  The chosen points are staged in shared memory in
+// batches of AC_TS.  Keys are written back to the points' slots; k_keyhist
+// then builds the per-chunk histograms in slot order.
+// ---------------------------------------------------------------------------
+constexpr int AC_BLOCK = 256;  // threads of k_assign_cull
+constexpr int AC_ITEMS = 4;    // points per lane per step (a warp: 128 consecutive points)
+constexpr int AC_TS = 1024;    // chosen points per shared-memory batch
+
+// squared gap between s and the box [lo, hi] (0 inside; NaN-free for NaN s)
+template <int DIM>
+__device__ __forceinline__ float box_gap2(const float* s, const float* lo, const float* hi)
+{
+    float g2 = 0.0f;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        const float gap = fmaxf(fmaxf(__fsub_rn(lo[d], s[d]), __fsub_rn(s[d], hi[d])), 0.0f);
+        g2 = __fadd_rn(g2, __fmul_rn(gap, gap));
+    }
+    return g2;
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(AC_BLOCK) k_assign_cull(EngineView v)
+{
+    constexpr int DP = PadDim<DIM>::v;
+    constexpr int WPTS = 32 * AC_ITEMS;
+    __shared__ __align__(16) float sS[AC_TS * DP];
+    __shared__ int s_item;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+    const ActiveList al(v, ACT_CHUNK);
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(&v.ctr[CTR_WORK], 1);
+        __syncthreads();
+        const int item = s_item;
+        __syncthreads();
+        if (item >= al.total) break;
+        int c, lc;
+        al.locate(item, c, lc);
+        const CloudDesc cd = v.cl[c];
+        const int start = (int)(((int64_t)lc * cd.n_all) / cd.n_chunks);
+        const int end = (int)(((int64_t)(lc + 1) * cd.n_all) / cd.n_chunks);
+        const int ns = v.ns[c];
+        const float* Ps = v.Ps + cd.p_off * DIM;
+        const float* gS = v.S + cd.s_off * DIM;
+        const float rsq = sqr_rn(cd.r1);
+        const bool may_skip = rsq >= 1.0e-30f && rsq <= 1.0e30f;
+        const float thr = __fmul_ru(rsq, 1.0009765625f);
+        for (int b0 = start; b0 < end; b0 += AC_BLOCK * AC_ITEMS) {
+            // this warp's points: b0 + warp*128 + j*32 + lane, and their box
+            float p[AC_ITEMS][DIM];
+            float2 np2[AC_ITEMS / 2][DIM];
+            float best[AC_ITEMS];
+            int bi[AC_ITEMS];
+            float blo[DIM], bhi[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                blo[d] = INFINITY;
+                bhi[d] = -INFINITY;
+            }
+#pragma unroll
+            for (int j = 0; j < AC_ITEMS; ++j) {
+                const int i = b0 + warp * WPTS + j * 32 + lane;
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) {
+                    p[j][d] = (i < end) ? Ps[(int64_t)i * DIM + d] : 0.0f;
+                    if (i < end) {
+                        blo[d] = fminf(blo[d], p[j][d]);
+                        bhi[d] = fmaxf(bhi[d], p[j][d]);
+                    }
+                }
+                best[j] = FLT_MAX;
+                bi[j] = -1;
+            }
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    blo[d] = fminf(blo[d], __shfl_xor_sync(FULL, blo[d], o));
+                    bhi[d] = fmaxf(bhi[d], __shfl_xor_sync(FULL, bhi[d], o));
+                }
+            }
+#pragma unroll
+            for (int jj = 0; jj < AC_ITEMS / 2; ++jj)
+#pragma unroll
+                for (int d = 0; d < DIM; ++d)
+                    np2[jj][d] = make_float2(-p[2 * jj][d], -p[2 * jj + 1][d]);
+            for (int t0 = 0; t0 < ns; t0 += AC_TS) {
+                const int tl = min(AC_TS, ns - t0);
+                __syncthreads();  // the previous batch is no longer read
+                for (int e = tid; e < tl; e += AC_BLOCK)
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) sS[e * DP + d] = gS[(int64_t)(t0 + e) * DIM + d];
+                __syncthreads();
+                for (int q0 = 0; q0 < tl; q0 += 32) {
+                    const int q = q0 + lane;
+                    bool keep = false;
+                    if (q < tl) {
+                        float s[DIM];
+                        load_chosen<DIM>(sS, q, s);
+                        keep = !(may_skip && box_gap2<DIM>(s, blo, bhi) > thr);
+                    }
+                    unsigned bal = __ballot_sync(FULL, keep);
+                    while (bal) {  // kept chosen points in index order, warp-uniform
+                        const int b = __ffs(bal) - 1;
+                        bal &= bal - 1;
+                        float s[DIM];
+                        load_chosen<DIM>(sS, q0 + b, s);
+                        const int kk = t0 + q0 + b;
+#pragma unroll
+                        for (int jj = 0; jj < AC_ITEMS / 2; ++jj) {
+                            const float2 dd = sqdist2_exact<DIM>(s, np2[jj]);
+                            if (dd.x < best[2 * jj]) { best[2 * jj] = dd.x; bi[2 * jj] = kk; }
+                            if (dd.y < best[2 * jj + 1]) { best[2 * jj + 1] = dd.y; bi[2 * jj + 1] = kk; }
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < AC_ITEMS; ++j) {
+                const int i = b0 + warp * WPTS + j * 32 + lane;
+                if (i < end) v.keys[v.sorder[cd.p_off + i]] = (best[j] <= rsq) ? bi[j] : -1;
+            }
+        }
+    }
+}
+
+// per-chunk key histograms in slot order after k_assign_cull (the rows
+// k_assign writes itself)
+constexpr int KH_BLOCK = 256;
+
+__global__ void __launch_bounds__(KH_BLOCK) k_keyhist(EngineView v)
+{
+    extern __shared__ int s_hist[];
+    const int tid = threadIdx.x;
+    const ActiveList al(v, ACT_CHUNK);
+    for (int item = blockIdx.x; item < al.total; item += gridDim.x) {
+        int c, lc;
+        al.locate(item, c, lc);
+        const CloudDesc cd = v.cl[c];
+        const int ns = v.ns[c];
+        const int start = (int)(((int64_t)lc * cd.n_all) / cd.n_chunks);
+        const int end = (int)(((int64_t)(lc + 1) * cd.n_all) / cd.n_chunks);
+        const int32_t* keys = v.keys + cd.p_off;
+        int32_t* row = v.hist + cd.hist_off + (int64_t)lc * cd.ns_cap;
+        if (ns <= v.hist_smem) {
+            for (int k = tid; k < ns; k += KH_BLOCK) s_hist[k] = 0;
+            __syncthreads();
+            for (int i = start + tid; i < end; i += KH_BLOCK) {
+                const int k = keys[i];
+                if (k >= 0) atomicAdd(&s_hist[k], 1);
+            }
+            __syncthreads();
+            for (int k = tid; k < ns; k += KH_BLOCK) row[k] = s_hist[k];
+        } else {
+            for (int k = tid; k < ns; k += KH_BLOCK) row[k] = 0;
+            __syncthreads();
+            for (int i = start + tid; i < end; i += KH_BLOCK) {
+                const int k = keys[i];
+                if (k >= 0) atomicAdd(&row[k], 1);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Chunk scan: for every chosen point k of a cloud, the exclusive prefix over
 // the cloud's chunks of the chunk x key histogram (in place: afterwards row lc
 // holds, for each key, the members in earlier chunks) and the member count
@@ -1644,6 +1824,8 @@ cudaError_t prepare_pass_dim(const EngineView& v, const TuneParams& tp)
     e = cudaFuncSetAttribute(k_decimate<DIM, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              dec_smem_bytes(v));
     if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_keyhist, cudaFuncAttributeMaxDynamicSharedMemorySize, hist_bytes);
+    if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_scatter_cta, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 scatter_cta_smem_bytes(v));
 }
@@ -1653,7 +1835,11 @@ cudaError_t launch_pass_dim(const EngineView& v, const TuneParams& tp, int assig
                             cudaStream_t st, cudaEvent_t a0, cudaEvent_t a1)
 {
     const int hist_bytes = v.hist_smem * 4;
+    const int sms = v.n_sms;
     if (a0) cudaEventRecord(a0, st);
+    if (v.cull) {
+        k_assign_cull<DIM><<<std::max(1, std::min(v.n_chunks, sms * 8)), AC_BLOCK, 0, st>>>(v);
+    } else {
 #define RD_ASSIGN_CASE(B, I)                                                                  \
     if (tp.block == B && tp.items == I) {                                                     \
         k_assign<DIM, B, I><<<assign_grid, B, hist_bytes, st>>>(v);                           \
@@ -1665,9 +1851,11 @@ cudaError_t launch_pass_dim(const EngineView& v, const TuneParams& tp, int assig
     RD_ASSIGN_CASE(128, 16)
     { return cudaErrorInvalidValue; }
 #undef RD_ASSIGN_CASE
+    }
     if (a1) cudaEventRecord(a1, st);
+    if (v.cull && v.n_chunks > 0)
+        k_keyhist<<<std::min(v.n_chunks, sms * 4), KH_BLOCK, hist_bytes, st>>>(v);
     // fixed grids; every kernel walks only the current work lists
-    const int sms = v.n_sms;
     if (v.n_kblk > 0) k_chunkscan_cta<<<std::min(v.n_kblk, sms * 4), CS_W * 32, 0, st>>>(v);
     if (v.n_kblk_warp > 0)
         k_chunkscan_warp<<<std::min((v.n_kblk_warp + CSW_W - 1) / CSW_W, sms * 8), CSW_W * 32, 0, st>>>(v);
