@@ -36,11 +36,17 @@ sys.path.insert(0, ROOT)
 
 METRIC = "evolve pairs/s"
 UNIT = "pairs/s"
-# DRAM traffic of one k_assign launch on the helix3d_1m workload from one ncu
-# capture (dram__bytes_read.sum + dram__bytes_write.sum = 12,039,936 + 0 bytes,
-# profiles/k_assign_helix3d_1m.md); the algorithmic bytes are the 1,000,000
-# points x 12 B read once.  Applies to helix3d_1m only.
-ASSIGN_TRAFFIC_BYTES = {"helix3d_1m": 12_039_936}
+# DRAM traffic of one assignment launch on the helix3d_1m workload, from one
+# ncu capture each (dram__bytes_read.sum + dram__bytes_write.sum):
+#   k_assign_cull (culled, the default): 16,034,816 + 0 bytes
+#     (profiles/k_assign_cull_helix3d_1m.md) against 20 B of algorithmic
+#     traffic per point (12 B sorted point + 4 B slot read, 4 B key written,
+#     the keys staying in L2);
+#   k_assign (all pairs): 12,039,936 + 0 bytes (profiles/k_assign_helix3d_1m.md),
+#     the 1,000,000 points x 12 B read once.
+# Applies to helix3d_1m only.
+ASSIGN_TRAFFIC_BYTES = {"helix3d_1m": 16_034_816}
+ALL_PAIRS_TRAFFIC_BYTES = {"helix3d_1m": 12_039_936}
 
 
 def parse_args():
@@ -337,21 +343,55 @@ def run_b200_bf(args, world, rank, local):
     e2e_val = world * pairs_step / (float(e2e_t.item()) * 1e-3)
     ns_final = rd.ns_
 
-    # ---- dominant kernel: assign, timed per launch in a host-loop solve ----
+    # ---- dominant kernel: assign, timed per launch in host-loop solves: the
+    # bench's own kernel, then the all-pairs kernel for the FP32 roofline ----
     rd.set_loop_mode(rdb.LOOP_HOST)
     lib = L.lib()
-    L.check(lib.rd_bf_set_profiling(rd._h, 1))
-    rd.ridge_detection()
-    pst = rd.stats()
-    L.check(lib.rd_bf_set_profiling(rd._h, 0))
+    culled = rdb.get_assign_cull()
+
+    def profiled_solve():
+        L.check(lib.rd_bf_set_profiling(rd._h, 1))
+        rd.ridge_detection()
+        s = rd.stats()
+        L.check(lib.rd_bf_set_profiling(rd._h, 0))
+        return s
+
+    pst = profiled_solve()
+    rdb.set_assign_cull(False)
+    ast = profiled_solve()
+    rdb.set_assign_cull(culled)
     rd.set_loop_mode(rdb.LOOP_GRAPH)
     flops_per_pair = 3 * dim
     assign_ms_avg = pst.assign_ms / max(1, pst.assign_launches)
-    flops_per_launch = pst.pairs * flops_per_pair / max(1, pst.assign_launches)
-    achieved_tflops = flops_per_launch / (assign_ms_avg * 1e-3) / 1e12
+    ap_ms_avg = ast.assign_ms / max(1, ast.assign_launches)
+    ap_flops_per_launch = ast.pairs * flops_per_pair / max(1, ast.assign_launches)
+    ap_tflops = ap_flops_per_launch / (ap_ms_avg * 1e-3) / 1e12
     peak = ctypes.c_double(0)
     L.check(lib.rd_probe_fp32_peak(ctypes.byref(peak), ctypes.c_void_p(stream.cuda_stream)))
     nominal = 148 * 128 * 2 * 1.965e9 / 1e12
+    hbm_peak, hbm_src = measured_hbm_gbs()
+    # culled kernel: per point a sorted point and its slot read, its key written
+    cull_bytes = n * (4 * dim + 4 + 4)
+    cull_gbs = cull_bytes / (assign_ms_avg * 1e-3) / 1e9
+    all_pairs = {"kernel": "k_assign", "bound": "fp32", "achieved": ap_tflops,
+                 "peak": peak.value, "unit": "TFLOP/s", "frac": ap_tflops / peak.value,
+                 "peak_source": "measured FMA-chain probe (rd_probe_fp32_peak); "
+                                f"nominal {nominal:.1f} TFLOP/s at 1965 MHz",
+                 "flops_per_pair": flops_per_pair, "ms_per_launch": ap_ms_avg,
+                 "launches": ast.assign_launches,
+                 # the exact distance takes 9 separately rounded FP32
+                 # operations per pair (no FMA may be used), so the pipe's
+                 # ceiling in these units is half the FMA FLOP rate
+                 "frac_of_nonfused_peak": ap_tflops / (peak.value / 2),
+                 "traffic": ALL_PAIRS_TRAFFIC_BYTES.get(args.workload)}
+    if culled:
+        roofline = {"bound": "hbm", "kernel": "k_assign_cull", "achieved": cull_gbs,
+                    "peak": hbm_peak, "unit": "GB/s", "frac": cull_gbs / hbm_peak,
+                    "peak_source": hbm_src, "bytes_per_launch": cull_bytes,
+                    "ms_per_launch": assign_ms_avg, "launches": pst.assign_launches,
+                    "traffic": ASSIGN_TRAFFIC_BYTES.get(args.workload)}
+    else:
+        roofline = dict(all_pairs)
 
     if world > 1:
         torch.distributed.barrier()
@@ -376,27 +416,20 @@ def run_b200_bf(args, world, rank, local):
                                f"r1={r1}, r2={r2}",
                    "l2": "flushed (256 MiB write) between timed steps",
                    "loop": "CUDA graph WHILE node", "parallelism": f"replicas x{world}",
+                   "assign": "culled (exact chunk-box culling)" if culled else "all pairs",
                    "assign_shape": {"block": tb, "items": ti, "source": "rd_autotune",
                                     "tuned_us_per_launch": tus}},
         "solves_per_s": world * 1e3 / ms_max,
         "pairs_per_step": pairs_step, "loop_iters_per_step": iters_step,
         "ns_final": ns_final,
-        "roofline": {"bound": "fp32", "kernel": "k_assign", "achieved": achieved_tflops,
-                     "peak": peak.value, "unit": "TFLOP/s",
-                     "frac": achieved_tflops / peak.value,
-                     "peak_source": "measured FMA-chain probe (rd_probe_fp32_peak); "
-                                    f"nominal {nominal:.1f} TFLOP/s at 1965 MHz",
-                     "flops_per_pair": flops_per_pair,
-                     "assign_ms_per_launch": assign_ms_avg,
-                     "assign_launches": pst.assign_launches,
-                     # the exact distance takes 9 separately rounded FP32
-                     # operations per pair (no FMA may be used), so the pipe's
-                     # ceiling in these units is half the FMA FLOP rate
-                     "frac_of_nonfused_peak": achieved_tflops / (peak.value / 2),
-                     "traffic": ASSIGN_TRAFFIC_BYTES.get(args.workload)},
+        "roofline": roofline,
+        "all_pairs": all_pairs,
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(P.nbytes),
                 "d2h_bytes_per_step": int(ns_final * dim * 4)},
-        "gpu_launches": args.steps * (2 + 8 * iters_step),
+        # per loop iteration: assign, key histogram (culled), chunk scan, key
+        # bases, scatter, sum+shift, control, decimate, loop condition; per
+        # solve about 32 more (reset, choose rounds, spatial order)
+        "gpu_launches": args.steps * ((9 if culled else 8) * iters_step + 32),
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
@@ -659,7 +692,10 @@ def run_b200_batch(args, world, rank, local):
             "pairs_per_step_rank0": stb.pairs, "loop_iters_rank0": stb.loop_iters,
             "e2e": {"value": n_all / (ms_e2e * 1e-3), "unit": "solves/s",
                     "h2d_bytes_per_step": int(packed.nbytes), "d2h_bytes_per_step": d2h},
-            "gpu_launches": args.steps * (2 + 8 * stb.loop_iters),
+            # per loop iteration: assign, key histogram (culled), two chunk
+            # scans, key bases, scatter, sum+shift, control, decimate, loop
+            # condition; per run about 32 more (reset, choose, spatial order)
+            "gpu_launches": args.steps * ((10 if rdb.get_assign_cull() else 9) * stb.loop_iters + 32),
             "clocks": clocks,
         }))
     if world > 1:

@@ -184,6 +184,17 @@ private:
 
 }  // namespace tiled
 
+// Exact culling of the brute-force assignment (process-wide, on by default):
+// the same keys as the all-pairs comparison of rd/cpu/brute_force/evolve.hpp:43-66,
+// skipping chosen points that provably lie beyond r1.  Read when a run starts.
+inline void setAssignCull(bool enable) { check(rd_set_assign_cull(enable ? 1 : 0)); }
+inline bool assignCull()
+{
+    int e = 0;
+    check(rd_get_assign_cull(&e));
+    return e != 0;
+}
+
 // rd::orderSamples (rd/cpu/brute_force/order.hpp:45) with the brute-force
 // class's condition (squared distance <= r2*r2), on the device: chains of
 // point indices of the ns x DIM ROW_MAJOR device points dS, each chain front

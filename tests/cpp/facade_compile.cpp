@@ -22,6 +22,7 @@ static void use_order()
     float* dS = nullptr;
     auto chains = orderSamples(dS, 3, 0, 0.3f);
     (void)chains.size();
+    setAssignCull(assignCull());
 }
 
 static void use_tiled()

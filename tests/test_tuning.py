@@ -40,3 +40,15 @@ def test_bad_dim_and_size_rejected():
         rdb.tune_set(2, 0, 128, 8)
     with pytest.raises(rdb.RDError):
         rdb.tune_get(5, 1000)
+
+
+def test_assign_cull_switch_roundtrip():
+    """The culling switch is process-wide host state: no GPU needed."""
+    import ridgedetection_b200 as rdb
+    assert rdb.get_assign_cull()
+    try:
+        rdb.set_assign_cull(False)
+        assert not rdb.get_assign_cull()
+    finally:
+        rdb.set_assign_cull(True)
+    assert rdb.get_assign_cull()
