@@ -197,6 +197,7 @@ EngineView Engine::view() const
     v.hist = bHist_.as<int32_t>();
     v.cnt = bCnt_.as<int32_t>();
     v.base = bBase_.as<int32_t>();
+    v.big = bBig_.as<int32_t>();
     v.next = bNext_.as<int32_t>();
     v.hash = bHash_.as<int32_t>();
     v.ns = bNs_.as<int32_t>();
@@ -306,6 +307,7 @@ int Engine::finish_setup_after_choose(cudaStream_t st)
     RD_CK(bHist_.ensure(4 * (size_t)(hist + 1)));
     RD_CK(bCnt_.ensure(4 * (size_t)(key + 1)));
     RD_CK(bBase_.ensure(4 * (size_t)(key + 1)));
+    RD_CK(bBig_.ensure(4 * (size_t)(key + 1)));
     RD_CK(bDx_.ensure(4 * (size_t)(sscr * dim_ + 1)));
     RD_CK(bDcell_.ensure(4 * (size_t)(sscr * dim_ + 1)));
     RD_CK(bDalive_.ensure(4 * (size_t)(sscr + 1)));

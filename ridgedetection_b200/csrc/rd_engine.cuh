@@ -54,6 +54,7 @@ enum : int {
     CTR_ERR = 3,       // OR of global error bits
     CTR_NACT = 4,      // evolving clouds in the current work lists
     CTR_NREADY = 5,    // groups ready for decimation in this iteration
+    CTR_NBIG = 6,      // keys in the big-key list of the current pass
     CTR_COUNT = 8,
 };
 
@@ -69,6 +70,7 @@ struct EngineView {
     int32_t* hist;               // per cloud: n_chunks x ns_cap key histogram (then its prefix over chunks)
     int32_t* cnt;                // per chosen slot: members in the last pass
     int32_t* base;               // per chosen slot: first slot of its segment of perm
+    int32_t* big;                // chosen slots with SUM_BIG_MIN+ members in this pass
     int32_t* hash;               // choose hash heads
     int32_t* next;               // per chosen slot: choose hash chain
     int32_t* ns;                 // per cloud: current chosen count

@@ -126,7 +126,7 @@ private:
     RunStats stats_;
 
     DevBuf bCl_, bGr_, bChunkCloud_, bSlotCloud_;
-    DevBuf bP_, bS_, bKeys_, bGrouped_, bHist_, bCnt_, bBase_, bNext_, bHash_, bSurv_;
+    DevBuf bP_, bS_, bKeys_, bGrouped_, bHist_, bCnt_, bBase_, bBig_, bNext_, bHash_, bSurv_;
     DevBuf bNs_, bPhase_, bCont_, bPasses_, bTotPasses_, bOuter_, bErr_, bPairs_, bCtr_;
     DevBuf bActCloud_, bActPre_, bGroupConv_, bReady_, bDnbOff_, bDnb_, bDbig_, bDcpre_;
     int dec_smem_max_ = 0;

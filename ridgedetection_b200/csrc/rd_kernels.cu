@@ -17,6 +17,10 @@ namespace rdb {
 
 namespace {
 
+// members from which a key is folded by a whole CTA of k_sum_shift (seven
+// warps gather, one warp runs the add chain) instead of by one warp
+constexpr int SUM_BIG_MIN = 2048;
+
 // Work lists over the clouds still evolving, rebuilt by k_loopcond after every
 // iteration: act_cloud[a] is the a-th evolving cloud and act_pre[kind] the
 // exclusive prefix of its work items (ACT_* in rd_engine.cuh), so kernels
@@ -761,7 +765,8 @@ __global__ void __launch_bounds__(CSW_W * 32) k_chunkscan_warp(EngineView v)
 
 // ---------------------------------------------------------------------------
 // Key bases: one CTA per evolving cloud, exclusive prefix of the member
-// counts over its keys (first grouped slot of each key).
+// counts over its keys (first grouped slot of each key); keys of SUM_BIG_MIN
+// or more members are listed for the CTA-wide folds of k_sum_shift.
 // ---------------------------------------------------------------------------
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_keybase(EngineView v)
@@ -797,6 +802,7 @@ __global__ void __launch_bounds__(BLOCK) k_keybase(EngineView v)
             }
             const int carry = s_carry;
             if (k < ns) base[k] = carry + wpre + incl - x;
+            if (x >= SUM_BIG_MIN) v.big[atomicAdd(&v.ctr[CTR_NBIG], 1)] = (int)(cd.key_off + k);
             __syncthreads();
             if (threadIdx.x == 0) s_carry = carry + tot;
         }
@@ -968,22 +974,38 @@ constexpr int TILE_PPL = 8;
 // members from which the fused tile kernel folds a key with the whole CTA
 // (exact parallel evaluation, rd_fold.cuh) instead of one warp's add chain
 constexpr int FOLD_CTA_MIN = 4096;
+// members per shared-memory buffer of a CTA-folded key (two buffers)
+constexpr int SB_CHUNK = 1024;
 
 template <int DIM>
 __device__ void sum_shift_one(const EngineView& v, int c, int k, float* buf, int* sidx, int lane);
 
 template <int DIM>
-__global__ void __launch_bounds__(256) k_sum_shift(EngineView v)
+__device__ void sum_shift_big_one(const EngineView& v, int slot, float (*s_x)[SB_CHUNK * DIM]);
+
+// grid = big_ctas CTAs for the listed big keys (one key at a time each), then
+// the CTAs whose warps take one smaller key each
+template <int DIM>
+__global__ void __launch_bounds__(256) k_sum_shift(EngineView v, int big_ctas)
 {
-    __shared__ float s_buf[8][SUM_BP_WIDE * DIM];
-    __shared__ int s_idx[8][SUM_BP_WIDE];
+    __shared__ __align__(16) unsigned char s_raw[8 * SUM_BP_WIDE * (DIM + 1) * 4];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if ((int)blockIdx.x < big_ctas) {
+        static_assert(2 * SB_CHUNK * DIM <= 8 * SUM_BP_WIDE * (DIM + 1), "big-key buffers");
+        float (*s_x)[SB_CHUNK * DIM] = reinterpret_cast<float (*)[SB_CHUNK * DIM]>(s_raw);
+        const int nbig = v.ctr[CTR_NBIG];
+        for (int i = blockIdx.x; i < nbig; i += big_ctas) sum_shift_big_one<DIM>(v, v.big[i], s_x);
+        return;
+    }
+    float* s_buf = reinterpret_cast<float*>(s_raw) + warp * SUM_BP_WIDE * DIM;
+    int* s_idx = reinterpret_cast<int*>(s_raw + 8 * SUM_BP_WIDE * DIM * 4) + warp * SUM_BP_WIDE;
     const ActiveList al(v, ACT_SLOT);
-    for (int t = blockIdx.x * 8 + warp; t < al.total; t += gridDim.x * 8) {
+    const int b = (int)blockIdx.x - big_ctas, nb = (int)gridDim.x - big_ctas;
+    for (int t = b * 8 + warp; t < al.total; t += nb * 8) {
         __syncwarp();
         int c, k;
         al.locate(t, c, k);
-        sum_shift_one<DIM>(v, c, k, s_buf[warp], s_idx[warp], lane);
+        sum_shift_one<DIM>(v, c, k, s_buf, s_idx, lane);
     }
 }
 
@@ -1049,15 +1071,13 @@ __device__ float fold_members(const int32_t* __restrict__ perm, const int n,
     return sum;
 }
 
+// The shift of chosen point k of cloud c from its members' sum (lane d < DIM
+// holds coordinate d): evolve.hpp:143-177, or the plain mean for the
+// adjoint's forward step.  Called by one whole warp.
 template <int DIM>
-__device__ void sum_shift_one(const EngineView& v, int c, int k, float* buf, int* sidx, int lane)
+__device__ void apply_shift(const EngineView& v, int c, const CloudDesc& cd, int k, int n, float sum,
+                            int lane)
 {
-    const CloudDesc cd = v.cl[c];
-    const int n = v.cnt[cd.key_off + k];
-    if (n == 0) return;
-    const int32_t* mp = v.perm + cd.p_off + v.base[cd.key_off + k];
-    const float* Pc = v.P + cd.p_off * DIM;
-    const float sum = fold_members<DIM, SUM_BP_WIDE>(mp, n, Pc, buf, sidx, lane);
     int moved = 0;
     if (lane < DIM) {
         float* s = v.S + (cd.s_off + k) * DIM + lane;
@@ -1070,6 +1090,83 @@ __device__ void sum_shift_one(const EngineView& v, int c, int k, float* buf, int
         }
     }
     if (__any_sync(FULL, moved) && lane == 0) v.cont[c] = 1;
+}
+
+template <int DIM>
+__device__ void sum_shift_one(const EngineView& v, int c, int k, float* buf, int* sidx, int lane)
+{
+    const CloudDesc cd = v.cl[c];
+    const int n = v.cnt[cd.key_off + k];
+    if (n == 0 || n >= SUM_BIG_MIN) return;  // big keys: k_sum_shift_big
+    const int32_t* mp = v.perm + cd.p_off + v.base[cd.key_off + k];
+    const float* Pc = v.P + cd.p_off * DIM;
+    const float sum = fold_members<DIM, SUM_BP_WIDE>(mp, n, Pc, buf, sidx, lane);
+    apply_shift<DIM>(v, c, cd, k, n, sum, lane);
+}
+
+// ---------------------------------------------------------------------------
+// The same ordered sum + shift for one key of SUM_BIG_MIN or more members
+// (global chosen slot `slot`), by a whole CTA: warps 1..7 gather the members'
+// coordinates (in member order) into one of two shared buffers while warp 0
+// folds the other with the same chain of rounded adds (lane d: coordinate
+// d), so the gathers of a large cluster no longer stall its add chain.
+// ---------------------------------------------------------------------------
+template <int DIM>
+__device__ void sum_shift_big_one(const EngineView& v, int slot, float (*s_x)[SB_CHUNK * DIM])
+{
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int c = v.slot_cloud[slot];
+    const CloudDesc cd = v.cl[c];
+    const int k = (int)(slot - cd.key_off);
+    const int n = v.cnt[slot];
+    const int32_t* mp = v.perm + cd.p_off + v.base[slot];
+    const float* Pc = v.P + cd.p_off * DIM;
+    const int nchunk = (n + SB_CHUNK - 1) / SB_CHUNK;
+    auto gather = [&](int ch, float* dst) {  // warps 1..7
+        const int off = ch * SB_CHUNK;
+        const int m = min(SB_CHUNK, n - off);
+        for (int j0 = tid - 32; j0 < m; j0 += 224 * 4) {
+            int ix[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int j = j0 + u * 224;
+                ix[u] = (j < m) ? mp[off + j] : 0;
+            }
+            float x[4][DIM];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int d = 0; d < DIM; ++d)
+                    x[u][d] = (j0 + u * 224 < m) ? Pc[(int64_t)ix[u] * DIM + d] : 0.0f;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int j = j0 + u * 224;
+                if (j < m)
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) dst[j * DIM + d] = x[u][d];
+            }
+        }
+    };
+    __syncthreads();  // the previous key's buffers are no longer read
+    if (warp > 0) gather(0, s_x[0]);
+    __syncthreads();
+    float sum = 0.0f;
+    for (int ch = 0; ch < nchunk; ++ch) {
+        if (warp > 0) {
+            if (ch + 1 < nchunk) gather(ch + 1, s_x[(ch + 1) & 1]);
+        } else if (lane < DIM) {
+            const float* x = s_x[ch & 1];
+            const int m = min(SB_CHUNK, n - ch * SB_CHUNK);
+            if (m == SB_CHUNK) {
+#pragma unroll 32
+                for (int j = 0; j < SB_CHUNK; ++j) sum = __fadd_rn(sum, x[j * DIM + lane]);
+            } else {
+                for (int j = 0; j < m; ++j) sum = __fadd_rn(sum, x[j * DIM + lane]);
+            }
+        }
+        __syncthreads();
+    }
+    if (warp == 0) apply_shift<DIM>(v, c, cd, k, n, sum, lane);
 }
 
 // ---------------------------------------------------------------------------
@@ -1760,6 +1857,7 @@ __global__ void __launch_bounds__(1024) k_loopcond(EngineView v, cudaGraphCondit
         v.ctr[CTR_NACT] = nact;
         v.ctr[CTR_WORK] = 0;
         v.ctr[CTR_NREADY] = 0;
+        v.ctr[CTR_NBIG] = 0;
         const int it = v.ctr[CTR_ITERS] + (count_iter ? 1 : 0);
         v.ctr[CTR_ITERS] = it;
         int a = s_act;
@@ -1862,7 +1960,12 @@ cudaError_t launch_pass_dim(const EngineView& v, const TuneParams& tp, int assig
     k_keybase<1024><<<std::min(v.n_clouds, sms * 2), 1024, 0, st>>>(v);
     if (v.n_chunks > 0)
         k_scatter_cta<<<std::min(v.n_chunks, sms * 8), SCAT_W * 32, scatter_cta_smem_bytes(v), st>>>(v);
-    if (v.n_slots > 0) k_sum_shift<DIM><<<std::min((v.n_slots + 7) / 8, sms * 8), 256, 0, st>>>(v);
+    if (v.n_slots > 0) {
+        // at most (points / SUM_BIG_MIN) keys can be big
+        const int big_ctas = (int)std::min<int64_t>(
+            ((int64_t)v.n_chunks * v.chunk_pts + SUM_BIG_MIN - 1) / SUM_BIG_MIN, sms);
+        k_sum_shift<DIM><<<big_ctas + std::min((v.n_slots + 7) / 8, sms * 8), 256, 0, st>>>(v, big_ctas);
+    }
     k_control<<<std::min((v.n_clouds + 255) / 256, sms), 256, 0, st>>>(v);
     k_decimate<DIM, 512><<<std::min(v.n_groups, sms * 2), 512, dec_smem_bytes(v), st>>>(v);
     return cudaGetLastError();
@@ -2077,7 +2180,12 @@ cudaError_t launch_evolve_step_dim(const EngineView& v, const TuneParams& tp, in
     k_keybase<1024><<<std::min(v.n_clouds, sms * 2), 1024, 0, st>>>(v);
     if (v.n_chunks > 0)
         k_scatter_cta<<<std::min(v.n_chunks, sms * 8), SCAT_W * 32, scatter_cta_smem_bytes(v), st>>>(v);
-    if (v.n_slots > 0) k_sum_shift<DIM><<<std::min((v.n_slots + 7) / 8, sms * 8), 256, 0, st>>>(v);
+    if (v.n_slots > 0) {
+        // at most (points / SUM_BIG_MIN) keys can be big
+        const int big_ctas = (int)std::min<int64_t>(
+            ((int64_t)v.n_chunks * v.chunk_pts + SUM_BIG_MIN - 1) / SUM_BIG_MIN, sms);
+        k_sum_shift<DIM><<<big_ctas + std::min((v.n_slots + 7) / 8, sms * 8), 256, 0, st>>>(v, big_ctas);
+    }
     return cudaGetLastError();
 }
 
