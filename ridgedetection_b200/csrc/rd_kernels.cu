@@ -18,8 +18,12 @@ namespace rdb {
 namespace {
 
 // members from which a key is folded by a whole CTA of k_sum_shift (seven
-// warps gather, one warp runs the add chain) instead of by one warp
+// warps gather, one warp runs the add chain) instead of by one warp -- while
+// the pass has at most two such keys per big-key CTA.  A CTA folds a key
+// about 2.5x sooner than a warp but takes 8 warps, so with many big keys (a
+// batch of large clouds) the per-warp folds finish first.
 constexpr int SUM_BIG_MIN = 2048;
+constexpr int SUM_BIG_PER_CTA = 2;
 
 // Work lists over the clouds still evolving, rebuilt by k_loopcond after every
 // iteration: act_cloud[a] is the a-th evolving cloud and act_pre[kind] the
@@ -978,7 +982,8 @@ constexpr int FOLD_CTA_MIN = 4096;
 constexpr int SB_CHUNK = 1024;
 
 template <int DIM>
-__device__ void sum_shift_one(const EngineView& v, int c, int k, float* buf, int* sidx, int lane);
+__device__ void sum_shift_one(const EngineView& v, int c, int k, float* buf, int* sidx, int lane,
+                              bool cta_big);
 
 template <int DIM>
 __device__ void sum_shift_big_one(const EngineView& v, int slot, float (*s_x)[SB_CHUNK * DIM]);
@@ -990,11 +995,13 @@ __global__ void __launch_bounds__(256) k_sum_shift(EngineView v, int big_ctas)
 {
     __shared__ __align__(16) unsigned char s_raw[8 * SUM_BP_WIDE * (DIM + 1) * 4];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nbig = v.ctr[CTR_NBIG];
+    const bool cta_big = nbig <= SUM_BIG_PER_CTA * big_ctas;  // else every key goes to a warp
     if ((int)blockIdx.x < big_ctas) {
         static_assert(2 * SB_CHUNK * DIM <= 8 * SUM_BP_WIDE * (DIM + 1), "big-key buffers");
         float (*s_x)[SB_CHUNK * DIM] = reinterpret_cast<float (*)[SB_CHUNK * DIM]>(s_raw);
-        const int nbig = v.ctr[CTR_NBIG];
-        for (int i = blockIdx.x; i < nbig; i += big_ctas) sum_shift_big_one<DIM>(v, v.big[i], s_x);
+        if (cta_big)
+            for (int i = blockIdx.x; i < nbig; i += big_ctas) sum_shift_big_one<DIM>(v, v.big[i], s_x);
         return;
     }
     float* s_buf = reinterpret_cast<float*>(s_raw) + warp * SUM_BP_WIDE * DIM;
@@ -1005,7 +1012,7 @@ __global__ void __launch_bounds__(256) k_sum_shift(EngineView v, int big_ctas)
         __syncwarp();
         int c, k;
         al.locate(t, c, k);
-        sum_shift_one<DIM>(v, c, k, s_buf, s_idx, lane);
+        sum_shift_one<DIM>(v, c, k, s_buf, s_idx, lane, cta_big);
     }
 }
 
@@ -1093,11 +1100,12 @@ __device__ void apply_shift(const EngineView& v, int c, const CloudDesc& cd, int
 }
 
 template <int DIM>
-__device__ void sum_shift_one(const EngineView& v, int c, int k, float* buf, int* sidx, int lane)
+__device__ void sum_shift_one(const EngineView& v, int c, int k, float* buf, int* sidx, int lane,
+                              bool cta_big)
 {
     const CloudDesc cd = v.cl[c];
     const int n = v.cnt[cd.key_off + k];
-    if (n == 0 || n >= SUM_BIG_MIN) return;  // big keys: k_sum_shift_big
+    if (n == 0 || (cta_big && n >= SUM_BIG_MIN)) return;  // big keys: the CTA path
     const int32_t* mp = v.perm + cd.p_off + v.base[cd.key_off + k];
     const float* Pc = v.P + cd.p_off * DIM;
     const float sum = fold_members<DIM, SUM_BP_WIDE>(mp, n, Pc, buf, sidx, lane);
