@@ -1,7 +1,7 @@
 """Host-side multi-rank logic on CPU: LPT sharding and the gather of per-cloud
 results over torch.distributed (gloo, world_size 2).  The per-rank solver here
-is the CPU checker, so no GPU is involved; on the GPU box the same code runs
-with BatchedRidgeDetection over NCCL."""
+is the CPU oracle, so no GPU is involved; with GPUs the same code runs with
+BatchedRidgeDetection over NCCL."""
 import os
 import socket
 
