@@ -285,19 +285,31 @@ RD_API rd_status rd_evolve(int dim, const float* d_P, int64_t np, float* d_S, in
                            float r1, int64_t* passes_out, void* stream);
 RD_API rd_status rd_decimate(int dim, float* d_S, int64_t ns, float r2, int64_t* ns_out,
                              void* stream);
+/* One evolve pass, the body of the reference's evolve loop
+ * (rd/cpu/brute_force/evolve.hpp:313-338: calculateClosestSphereCenter then
+ * shiftTowardMassCenter; GPU dispatch_evolve.cuh, one iteration of its
+ * contFlag loop): every cloud point is assigned to its nearest chosen point
+ * within r1, and each chosen point whose cluster mean moved beyond the
+ * reference's threshold takes that mean.  *moved_out (host) = 1 when some
+ * chosen point moved (the reference's contFlag), else 0.  d_S is updated in
+ * place.  Blocks until the result is in place. */
+RD_API rd_status rd_evolve_pass(int dim, const float* d_P, int64_t np, float* d_S, int64_t ns,
+                                float r1, int32_t* moved_out, void* stream);
 
 /* ---------------------------------------------------------------------------
  * rd_decimate_noalloc: the decimation of rd_decimate without any device
  * allocation.  It has no counterpart in the reference.  It exists for callers
- * that cannot call cudaMalloc: code running while a CUDA graph is captured,
- * hosts that forbid allocation after start-up, plugins whose device memory
- * belongs to a framework that gives them no workspace.
+ * that cannot call cudaMalloc: hosts that forbid device allocation once they
+ * have started (real-time or embedded loops, where an allocation can block or
+ * fail under memory pressure) and plugins whose device memory belongs to a
+ * framework that gives them no workspace.
  *   - Scratch is one fixed __device__ array of RD_DECIMATE_NOALLOC_SCRATCH_BYTES
- *     inside the library; every GPU that loads the library holds it until the
- *     process exits.  ns above RD_DECIMATE_NOALLOC_MAX_POINTS is rejected with
- *     RD_ERR_CAPACITY (use rd_decimate instead).
- *   - The first call on a device looks up the array's device address (with that
- *     device current); make that first call before any stream capture.
+ *     (1.5 MiB) inside the library; every GPU that loads the library holds it
+ *     until the process exits.  ns above RD_DECIMATE_NOALLOC_MAX_POINTS is
+ *     rejected with RD_ERR_CAPACITY (use rd_decimate instead).
+ *   - The first call on a device (and the first after a device reset) looks up
+ *     the array's device address with that device current; make that first
+ *     call before any stream capture.
  *   - All calls share the array: calls whose kernels overlap on the GPU race.
  *     Serialize them (one stream, or events).
  *   - d_S (ns points, packed ROW_MAJOR, device) is decimated in place; the

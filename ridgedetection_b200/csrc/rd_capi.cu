@@ -18,7 +18,6 @@ using namespace rdb;
 namespace rdb {
 rd_status report_error(rd_status s, const char* msg);
 int decimate_noalloc(int dim, float* d_S, int64_t ns, float r2, int32_t* d_ns_out, cudaStream_t st);
-extern const char* noalloc_error_message;
 }  // namespace rdb
 
 namespace {
@@ -789,6 +788,32 @@ rd_status rd_evolve(int dim, const float* d_P, int64_t np, float* d_S, int64_t n
     return from_engine(rc, e);
 }
 
+rd_status rd_evolve_pass(int dim, const float* d_P, int64_t np, float* d_S, int64_t ns, float r1,
+                         int32_t* moved_out, void* stream)
+{
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (!d_P || !d_S || !moved_out) return set_err(RD_ERR_ARG, "null argument");
+    if (np < 0 || np > INT32_MAX - 1024 || ns < 0 || ns > INT32_MAX - 1024 || !(r1 > 0.0f))
+        return set_err(RD_ERR_ARG, "bad sizes or r1");
+    *moved_out = 0;
+    if (ns == 0) return RD_OK;
+    thread_local Engine& e = *new Engine();  // never destroyed: no CUDA calls at exit
+    cudaStream_t st = (cudaStream_t)stream;
+    if (rd_status s = one_cloud_engine(e, dim, np, std::max(np, ns), r1, r1)) return s;
+    if (np) CK_CUDA(cudaMemcpyAsync(e.points(), d_P, sizeof(float) * np * dim, cudaMemcpyDeviceToDevice, st));
+    CK_CUDA(cudaMemcpyAsync(e.chosen_mut(), d_S, sizeof(float) * ns * dim, cudaMemcpyDeviceToDevice, st));
+    e.given_ns.assign(1, (int32_t)ns);
+    // one pass: the pass limit ends the run after it; the limit being hit
+    // means the pass moved a chosen point (contFlag set)
+    e.max_passes = 1;
+    const int rc = e.run(st, false, Engine::RUN_EVOLVE_ONLY);
+    if (rc && rc != RD_ERR_NOT_CONVERGED) return from_engine(rc, e);
+    CK_CUDA(cudaMemcpyAsync(d_S, e.chosen(), sizeof(float) * ns * dim, cudaMemcpyDeviceToDevice, st));
+    CK_CUDA(cudaStreamSynchronize(st));
+    *moved_out = (rc == RD_ERR_NOT_CONVERGED) ? 1 : 0;
+    return RD_OK;
+}
+
 rd_status rd_decimate(int dim, float* d_S, int64_t ns, float r2, int64_t* ns_out, void* stream)
 {
     if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
@@ -812,9 +837,8 @@ rd_status rd_decimate(int dim, float* d_S, int64_t ns, float r2, int64_t* ns_out
 rd_status rd_decimate_noalloc(int dim, float* d_S, int64_t ns, float r2, int32_t* d_ns_out,
                               void* stream)
 {
-    const int rc = rdb::decimate_noalloc(dim, d_S, ns, r2, d_ns_out, (cudaStream_t)stream);
-    if (rc) return set_err((rd_status)rc, rdb::noalloc_error_message ? rdb::noalloc_error_message : "");
-    return RD_OK;
+    // errors are recorded in the calling thread's message by decimate_noalloc
+    return (rd_status)rdb::decimate_noalloc(dim, d_S, ns, r2, d_ns_out, (cudaStream_t)stream);
 }
 
 // ------------------------------------------------------------------------

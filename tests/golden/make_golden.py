@@ -3,10 +3,10 @@
 The reference has no golden vectors of its own (its generators are unseeded and
 the data files it names are not in its repository), so the fixtures are made by
 running the reference's CPU implementation, compiled from its sources by
-`make -C oracle ref` into oracle/_ref/librdref.so (serial build), on seeded
-inputs.  Each fixture stores the input cloud and the reference's outputs; the
-tests then check the plain-C restatement (oracle/rd_oracle.c) and the GPU path
-against them bit for bit.
+`make -C oracle ref REF=<checkout>/ridge_detection` into oracle/_ref/librdref.so
+(serial build), on seeded inputs.  Each fixture stores the input cloud and the
+reference's outputs; the tests then check the plain-C restatement
+(oracle/rd_oracle.c) and the GPU path against them bit for bit.
 
 Run from the repository root:  python tests/golden/make_golden.py
 """
@@ -60,7 +60,8 @@ TILED = {
 
 def main():
     if O.ref() is None:
-        raise SystemExit("oracle/_ref/librdref.so missing: run `make -C oracle ref` first")
+        raise SystemExit("oracle/_ref/librdref.so missing: run "
+                         "`make -C oracle ref REF=<checkout>/ridge_detection` first")
     for name, (gen, r1, r2) in CASES.items():
         P = gen()
         S_choose = O.ref_choose(P, r1)

@@ -1,6 +1,6 @@
 """rd_decimate_noalloc: the decimation for callers that cannot allocate device
-memory (code under CUDA-graph capture, hosts that forbid allocation after
-start-up, plugins without a workspace).  Its scratch is a fixed array inside
+memory (hosts that forbid device allocation once they have started, plugins
+whose framework gives them no workspace).  Its scratch is a fixed array inside
 the library; it must give exactly what the allocating rd_decimate gives, call
 after call, since every call reuses (and must re-clear) that array.
 
