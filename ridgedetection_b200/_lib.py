@@ -103,6 +103,7 @@ SIGNATURES = {
     "rd_choose": [_i, _vp, _i64, _f, _vp, _pi64, _vp],
     "rd_evolve": [_i, _vp, _i64, _vp, _i64, _f, _pi64, _vp],
     "rd_decimate": [_i, _vp, _i64, _f, _pi64, _vp],
+    "rd_evolve_pass": [_i, _vp, _i64, _vp, _i64, _f, ctypes.POINTER(ctypes.c_int32), _vp],
     "rd_decimate_noalloc": [_i, _vp, _i64, _f, _vp, _vp],
     "rd_evolve_adjoint": [_i, _vp, _i64, _vp, _i64, _f, _i, _i, _vp, _vp, _vp, _vp, _i, _vp],
     "rd_batch_create": [ctypes.POINTER(_vp)],
