@@ -7,6 +7,14 @@ One step = one full ridge solve (choose, then evolve/decimate to convergence)
 through the library's C ABI.  The metric is evolve pairs/s: the sum over all
 evolve passes of (cloud points x chosen points), divided by the solve time.
 
+At N=1 the same line also carries two sub-objects, each timed by the same
+rules (warm-up, L2 flush, CUDA events, clocks, e2e, CPU baseline):
+  "tiled"    the tiled 2D spiral, N = 10,000,000, 64 x 64 tiles (full solves),
+             with the HBM roofline of the fused per-tile evolve kernel;
+  "batched"  4,096 clouds (1k..200k points) solved by one batched graph run,
+             against the plain per-cloud loop over the same clouds.
+--sub none leaves them out.
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
                   [--workload helix3d_1m|sine2d_20k|batch]
 
@@ -38,12 +46,11 @@ METRIC = "evolve pairs/s"
 UNIT = "pairs/s"
 # DRAM traffic of one assignment launch on the helix3d_1m workload, from one
 # ncu capture each (dram__bytes_read.sum + dram__bytes_write.sum):
-#   k_assign_cull (culled, the default): 16,034,816 + 0 bytes
-#     (profiles/k_assign_cull_helix3d_1m.md) against 20 B of algorithmic
-#     traffic per point (12 B sorted point + 4 B slot read, 4 B key written,
-#     the keys staying in L2);
-#   k_assign (all pairs): 12,039,936 + 0 bytes (profiles/k_assign_helix3d_1m.md),
-#     the 1,000,000 points x 12 B read once.
+#   k_assign_cull (culled, the default): 16,034,816 + 0 bytes against 20 B of
+#     algorithmic traffic per point (12 B sorted point + 4 B slot read, 4 B key
+#     written, the keys staying in L2);
+#   k_assign (all pairs): 12,039,936 + 0 bytes, the 1,000,000 points x 12 B
+#     read once.
 # Applies to helix3d_1m only.
 ASSIGN_TRAFFIC_BYTES = {"helix3d_1m": 16_034_816}
 ALL_PAIRS_TRAFFIC_BYTES = {"helix3d_1m": 12_039_936}
@@ -60,6 +67,9 @@ def parse_args():
                              "spiral2d_1m_tiled"])
     ap.add_argument("--clouds", type=int, default=4096, help="batch workload: number of clouds")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sub", default="tiled,batch",
+                    help="default workload at N=1: comma list of sub-workloads measured into "
+                         "the same JSON line (tiled, batch) or 'none'")
     ap.add_argument("--assign-cull", default="on", choices=["on", "off"],
                     help="exact chunk-box culling of the brute-force assignment (off = all-pairs kernel)")
     ap.add_argument("--shape", default=None,
@@ -220,17 +230,19 @@ def run_reference_arm(args, world, rank):
                           "unavailable": "oracle/_ref/librdref_omp.so was not built"}))
         return
     if args.workload.endswith("_tiled"):
-        vals = []
+        vals, secs = [], []
         cb = None
         for _ in range(args.warmup + args.steps):
             cb = cpu_baseline_tiled(r1, r2)
             vals.append(cb["value"])
+            secs.append(cb["seconds"])
         val = statistics.mean(vals[args.warmup:])
         cb["value"] = val
         print(json.dumps({
             "impl": "reference", "metric": "tiled ridge points/s", "value": val,
             "unit": "points/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * 1_000_000 / val, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": 1e3 * statistics.mean(secs[args.warmup:]), "higher_is_better": True,
+            "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": args.workload, "cores": cb["cores"]},
             "cpu_baseline": cb,
@@ -396,6 +408,16 @@ def run_b200_bf(args, world, rank, local):
     if world > 1:
         torch.distributed.barrier()
     rd.close()
+    del dP, hP, hout, l2_flush
+    subs = {}
+    if world == 1 and args.workload == "helix3d_1m" and args.sub != "none":
+        wanted = set(args.sub.split(","))
+        if "tiled" in wanted:
+            subs["tiled"] = run_b200_tiled(args, world, rank, local, embedded=True)
+            torch.cuda.empty_cache()
+        if "batch" in wanted:
+            subs["batched"] = run_b200_batch(args, world, rank, local, embedded=True)
+            torch.cuda.empty_cache()
     if rank != 0:
         if world > 1:
             torch.distributed.destroy_process_group()
@@ -433,6 +455,7 @@ def run_b200_bf(args, world, rank, local):
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
+    line.update(subs)
     print(json.dumps(line))
     if world > 1:
         torch.distributed.destroy_process_group()
@@ -461,23 +484,27 @@ def cpu_baseline_tiled(r1, r2, n_sample=1_000_000):
     oracle.ref_ridge_tiled(Ps, r1, r2, n_sample + 1, (64, 64), threads=threads, openmp=True)
     dt = time.perf_counter() - t
     return {"value": n_sample / dt, "unit": "points/s", "cores": threads, "kind": "reference",
+            "seconds": dt,
             "sample": f"one OpenMP tiled solve (EXT_TILE_TREE_MIXED_RD) of a {n_sample}-point "
                       f"spiral from the same generator, 64x64 tiles, {dt:.1f} s"}
 
 
-def run_b200_tiled(args, world, rank, local):
+def run_b200_tiled(args, world, rank, local, embedded=False):
     """Tiled 10M-point spiral: full solves (device tile build, fused per-tile
-    evolve, global decimation) through the C ABI, replicas across ranks."""
+    evolve, global decimation) through the C ABI, replicas across ranks.
+    embedded: measured as a sub-object of the default line (returned, not
+    printed; the caller owns the process group)."""
     import torch
     import ridgedetection_b200 as rdb
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    if world > 1:
+    if world > 1 and not embedded:
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
-    P, r1, r2 = workload(args.workload)
+    wl = "spiral2d_10m_tiled" if embedded else args.workload
+    P, r1, r2 = workload(wl)
     n, dim = P.shape
     tiles = (64, 64)
     stream = torch.cuda.current_stream()
@@ -557,9 +584,9 @@ def run_b200_tiled(args, world, rank, local):
         torch.distributed.barrier()
     rd.close()
     if rank != 0:
-        if world > 1:
+        if world > 1 and not embedded:
             torch.distributed.destroy_process_group()
-        return
+        return None
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         try:
@@ -572,7 +599,7 @@ def run_b200_tiled(args, world, rank, local):
         "unit": "points/s", "n_gpus": world, "steps": args.steps,
         "warmup": max(3, args.warmup), "ms_per_step": ms_max, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{args.workload}: tiled (extended tiles, mixed) full solve, "
+        "config": {"workload": f"{wl}: tiled (extended tiles, mixed) full solve, "
                                f"N={n}, dim={dim}, r1={r1}, r2={r2}, 64x64 tiles, "
                                f"max tile capacity N+1",
                    "l2": "flushed (256 MiB write) between timed steps",
@@ -592,14 +619,62 @@ def run_b200_tiled(args, world, rank, local):
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
+    if embedded:
+        return line
     print(json.dumps(line))
     if world > 1:
         torch.distributed.destroy_process_group()
+    return None
 
 
-def run_b200_batch(args, world, rank, local):
+def _ref_solve_cloud(item):
+    """One cloud of the batch through the reference's serial brute-force
+    solve (a worker of cpu_baseline_batch's spawn pool)."""
+    import oracle
+    from ridgedetection_b200 import generators as G
+    n, dim, r1, r2, seed = item
+    P = G.batch_cloud(n, dim, seed)
+    t = time.perf_counter()
+    oracle.ref_ridge_bf(P, r1, r2)
+    return time.perf_counter() - t
+
+
+def cpu_baseline_batch(spec, count=32):
+    """The reference has no batched path; its per-cloud CPU solve
+    (rd::RidgeDetection<float>, serial build) runs over a bounded sample of the
+    batch -- every (len(spec)/count)-th cloud in order of size, so the sample
+    spans the size range -- with one cloud per host core at a time (a spawn
+    process pool), and the batch's solves/s is extrapolated from it."""
+    import multiprocessing as mp
+    import oracle
+    if oracle.ref() is None:
+        return None
+    order = sorted(range(len(spec)), key=lambda c: (spec[c][0], c))
+    step = max(1, len(spec) // count)
+    pick = [spec[order[len(order) - 1 - k * step]] for k in range(min(count, len(spec)))]
+    threads = os.cpu_count() or 1
+    t = time.perf_counter()
+    with mp.get_context("spawn").Pool(threads) as pool:
+        secs = pool.map(_ref_solve_cloud, pick, chunksize=1)
+    dt = time.perf_counter() - t
+    # the whole batch keeps every core busy (thousands of clouds over a few
+    # dozen cores), so its rate is the sample's clouds per core-second times
+    # the cores; the sample's own wall time is set by its largest cloud
+    core_s = sum(secs)
+    return {"value": len(pick) * threads / core_s, "unit": "solves/s", "cores": threads,
+            "kind": "reference",
+            "sample": f"{len(pick)} of the {len(spec)} clouds (every {step}th by size, "
+                      f"{min(p[0] for p in pick)}..{max(p[0] for p in pick)} points), each "
+                      f"solved by the reference's serial CPU ridge detection, {threads} at a "
+                      f"time in a process pool: {core_s:.1f} core-s ({dt:.1f} s wall); "
+                      f"solves/s = clouds x cores / core-s"}
+
+
+def run_b200_batch(args, world, rank, local, embedded=False):
     """Batched workload: graph-driven batched solve vs the plain per-cloud loop.
-    Clouds are sharded over ranks by size (LPT, no collective on the data path)."""
+    Clouds are sharded over ranks by size (LPT, no collective on the data path).
+    embedded: measured as a sub-object of the default line (returned, not
+    printed; the caller owns the process group)."""
     import torch
     import ridgedetection_b200 as rdb
     from ridgedetection_b200 import generators as G
@@ -607,7 +682,7 @@ def run_b200_batch(args, world, rank, local):
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    if world > 1:
+    if world > 1 and not embedded:
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
@@ -676,9 +751,17 @@ def run_b200_batch(args, world, rank, local):
     p1.record(stream)
     p1.synchronize()
     ms_plain = max_over_ranks(p0.elapsed_time(p1))
+    line = None
     if rank == 0:
         n_all = len(spec)
-        print(json.dumps({
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                cpu = cpu_baseline_batch(spec)
+            except Exception as e:  # the baseline is reported, never the target
+                cpu = {"value": None, "unit": "solves/s", "cores": os.cpu_count(),
+                       "kind": "reference", "sample": f"failed: {e}"}
+        line = {
             "metric": "ridge solves/s", "value": n_all / (ms_batch * 1e-3),
             "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": ms_batch, "higher_is_better": True,
@@ -688,6 +771,7 @@ def run_b200_batch(args, world, rank, local):
                        "l2": "flushed (256 MiB write) between timed steps",
                        "loop": "CUDA graph WHILE node", "parallelism": f"LPT cloud shards x{world}"},
             "plain_loop_solves_per_s": n_all / (ms_plain * 1e-3),
+            "plain_loop_ms": ms_plain,
             "batched_over_plain": ms_plain / ms_batch,
             "pairs_per_step_rank0": stb.pairs, "loop_iters_rank0": stb.loop_iters,
             "e2e": {"value": n_all / (ms_e2e * 1e-3), "unit": "solves/s",
@@ -697,9 +781,14 @@ def run_b200_batch(args, world, rank, local):
             # condition; per run about 32 more (reset, choose, spatial order)
             "gpu_launches": args.steps * ((10 if rdb.get_assign_cull() else 9) * stb.loop_iters + 32),
             "clocks": clocks,
-        }))
-    if world > 1:
+            "cpu_baseline": cpu,
+        }
+        if not embedded:
+            print(json.dumps(line))
+    b.close()
+    if world > 1 and not embedded:
         torch.distributed.destroy_process_group()
+    return line
 
 
 def main():

@@ -24,6 +24,7 @@
 #ifndef RD_C_API_H
 #define RD_C_API_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #if defined(__GNUC__)
@@ -295,6 +296,51 @@ RD_API rd_status rd_decimate(int dim, float* d_S, int64_t ns, float r2, int64_t*
  * place.  Blocks until the result is in place. */
 RD_API rd_status rd_evolve_pass(int dim, const float* d_P, int64_t np, float* d_S, int64_t ns,
                                 float r1, int32_t* moved_out, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Device-level steps at the reference's full shape: per-array layouts and
+ * strides, the neighbour overload of evolve, and CUB-style temporary storage.
+ *   rd_choose_ws    DeviceChoose::choose<DIM,IN,OUT>(d_P, d_S, np, d_ns, r,
+ *                   pStride, sStride, stream)  (rd/gpu/device/device_choose.cuh)
+ *   rd_evolve_ws    DeviceEvolve::evolve<DIM,IN,OUT>(d_P, d_S, d_cordSums,
+ *                   d_cnt, np, ns, r, inPtsStride, chosenPtsStride,
+ *                   cordSumsStride, stream)  (rd/gpu/device/device_evolve.cuh:35-62)
+ *                   and its neighbour overload (d_N, nn, neighbourPtsStride;
+ *                   :70-97): the chosen points evolve over the input points
+ *                   followed by the neighbour points, in that index order
+ *   rd_decimate_ws  DeviceDecimate::decimate<DIM,OUT>(d_S, d_ns, r, stride,
+ *                   stream)  (rd/gpu/device/device_decimate.cuh)
+ * Every array has its own layout (RD_ROW_MAJOR / RD_COL_MAJOR) and pitch in
+ * floats (0 = packed; for rd_choose_ws's COL_MAJOR output, 0 = np, its
+ * capacity).  All point arrays are on the device.
+ * Temporary storage, as CUB's algorithms take it: call with d_temp = NULL to
+ * get the bytes needed in *temp_bytes (nothing runs), then call again with
+ * d_temp pointing to at least that many bytes of device memory, 256-byte
+ * aligned.  The second call takes all its scratch from d_temp (the reference's
+ * d_cordSums / d_spherePointCount are part of it); a d_temp smaller than the
+ * query gives RD_ERR_CAPACITY.  The query depends on the sizes, the dimension
+ * and the launch-shape table, not on the data.
+ * rd_evolve_ws: max_passes = 0 evolves to convergence (RD_ERR_NOT_CONVERGED if
+ * the library's limit of 65,536 passes is reached); max_passes = k > 0 stops
+ * after at most k passes (k = 1 is one pass of the reference's loop).
+ * *passes_out (optional) = passes run; *moved_out (optional) = 1 when the
+ * last pass moved a chosen point (the reference's contFlag), else 0.
+ * rd_decimate_ws compacts the survivors, in order, to the front of d_S.
+ * Each call blocks until its result is in place.
+ * ------------------------------------------------------------------------- */
+RD_API rd_status rd_choose_ws(int dim, const float* d_P, int64_t np, int p_layout,
+                              int64_t p_pitch, float r1, float* d_S, int s_layout,
+                              int64_t s_pitch, int64_t* ns_out, void* d_temp,
+                              size_t* temp_bytes, void* stream);
+RD_API rd_status rd_evolve_ws(int dim, const float* d_P, int64_t np, int p_layout,
+                              int64_t p_pitch, const float* d_N, int64_t nn, int n_layout,
+                              int64_t n_pitch, float* d_S, int64_t ns, int s_layout,
+                              int64_t s_pitch, float r1, int64_t max_passes,
+                              int64_t* passes_out, int32_t* moved_out, void* d_temp,
+                              size_t* temp_bytes, void* stream);
+RD_API rd_status rd_decimate_ws(int dim, float* d_S, int64_t ns, int s_layout, int64_t s_pitch,
+                                float r2, int64_t* ns_out, void* d_temp, size_t* temp_bytes,
+                                void* stream);
 
 /* ---------------------------------------------------------------------------
  * rd_decimate_noalloc: the decimation of rd_decimate without any device

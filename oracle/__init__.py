@@ -88,6 +88,12 @@ def lib():
         L.rdo_segment_hausdorff_f32.argtypes = [_F, _i64, _int]
         L.rdo_order.restype = _i64
         L.rdo_order.argtypes = [_F, _i64, _int, _flt, _I32, _I32]
+        L.rdo_forward64.restype = _int
+        L.rdo_forward64.argtypes = [_D, _i64, _D, _i64, _int, ctypes.c_double, _int, _D, _I32,
+                                    _I32]
+        L.rdo_fd64.restype = _int
+        L.rdo_fd64.argtypes = [_D, _i64, _D, _I32, _I32, _i64, _int, ctypes.c_double, _int, _D,
+                               _i64, _int, _i64, ctypes.c_double, _D]
         L.rdo_evolve_adjoint.restype = _int
         L.rdo_evolve_adjoint.argtypes = [_F, _i64, _F, _i64, _int, _flt, _int, _D, _D, _D, _F]
         _lib = L
@@ -264,6 +270,41 @@ def evolve_adjoint(P, S0, r1, iters, W):
 # --------------------------------------------------------------------------
 # reference wrappers (None when oracle/_ref was not built)
 # --------------------------------------------------------------------------
+
+class Forward64:
+    """FP64 run of the evolve adjoint's forward map with every assignment
+    recomputed (rd_fd64.c), kept for central differences of its loss."""
+
+    def __init__(self, P, S0, r1, iters):
+        self.P = np.ascontiguousarray(P, dtype=np.float64)
+        S0 = np.ascontiguousarray(S0, dtype=np.float64)
+        self.np, self.dim = self.P.shape
+        self.ns = S0.shape[0]
+        self.r1, self.iters = float(r1), int(iters)
+        self.S_all = np.zeros((iters + 1, self.ns, self.dim), np.float64)
+        self.keys = np.zeros((iters, self.np), np.int32)
+        self.cnt = np.zeros((iters, self.ns), np.int32)
+        rc = lib().rdo_forward64(self.P.ctypes.data_as(_D), self.np, S0.ctypes.data_as(_D),
+                                 self.ns, self.dim, self.r1, self.iters,
+                                 self.S_all.ctypes.data_as(_D), self.keys.ctypes.data_as(_I32),
+                                 self.cnt.ctypes.data_as(_I32))
+        if rc:
+            raise MemoryError("rdo_forward64 failed")
+
+    def central_difference(self, W, i, d, h, s0_row=-1):
+        """(L(P + h e_id) - L(P - h e_id)) / 2h, L = sum W . S^iters, or None when
+        the perturbation changes an assignment.  s0_row: the chosen point that
+        starts as a copy of cloud point i (moves with it), or -1."""
+        W = np.ascontiguousarray(W, dtype=np.float64)
+        out = ctypes.c_double(0.0)
+        rc = lib().rdo_fd64(self.P.ctypes.data_as(_D), self.np, self.S_all.ctypes.data_as(_D),
+                            self.keys.ctypes.data_as(_I32), self.cnt.ctypes.data_as(_I32),
+                            self.ns, self.dim, self.r1, self.iters, W.ctypes.data_as(_D),
+                            int(i), int(d), int(s0_row), float(h), ctypes.byref(out))
+        if rc == 2:
+            raise ValueError("rdo_fd64: bad arguments or allocation failure")
+        return None if rc else out.value
+
 
 def ref_choose(P, r1):
     L = ref()

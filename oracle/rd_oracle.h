@@ -73,6 +73,16 @@ int rdo_evolve_adjoint(const float* P, int64_t np, const float* S0, int64_t ns, 
                        float r1, int iters, const double* W, double* grad_P,
                        double* grad_S0, float* S_final);
 
+/* FP64 forward of the evolve adjoint's map with recomputed assignments, and
+ * central differences of its loss (rd_fd64.c).  S_all: (iters+1) x ns x dim,
+ * keys: iters x np, cnt: iters x ns.  rdo_fd64 returns 0 with *fd set, 1 when
+ * the +-h runs change an assignment (a boundary coordinate), 2 on bad input. */
+int rdo_forward64(const double* P, int64_t np, const double* S0, int64_t ns, int dim,
+                  double r1, int iters, double* S_all, int32_t* keys, int32_t* cnt);
+int rdo_fd64(const double* P, int64_t np, const double* S_all, const int32_t* keys,
+             const int32_t* cnt, int64_t ns, int dim, double r1, int iters, const double* W,
+             int64_t i, int d, int64_t s0_row, double h, double* fd);
+
 #ifdef __cplusplus
 }
 #endif

@@ -104,6 +104,13 @@ SIGNATURES = {
     "rd_evolve": [_i, _vp, _i64, _vp, _i64, _f, _pi64, _vp],
     "rd_decimate": [_i, _vp, _i64, _f, _pi64, _vp],
     "rd_evolve_pass": [_i, _vp, _i64, _vp, _i64, _f, ctypes.POINTER(ctypes.c_int32), _vp],
+    "rd_choose_ws": [_i, _vp, _i64, _i, _i64, _f, _vp, _i, _i64, _pi64, _vp,
+                     ctypes.POINTER(ctypes.c_size_t), _vp],
+    "rd_evolve_ws": [_i, _vp, _i64, _i, _i64, _vp, _i64, _i, _i64, _vp, _i64, _i, _i64, _f, _i64,
+                     _pi64, ctypes.POINTER(ctypes.c_int32), _vp, ctypes.POINTER(ctypes.c_size_t),
+                     _vp],
+    "rd_decimate_ws": [_i, _vp, _i64, _i, _i64, _f, _pi64, _vp, ctypes.POINTER(ctypes.c_size_t),
+                       _vp],
     "rd_decimate_noalloc": [_i, _vp, _i64, _f, _vp, _vp],
     "rd_evolve_adjoint": [_i, _vp, _i64, _vp, _i64, _f, _i, _i, _vp, _vp, _vp, _vp, _i, _vp],
     "rd_batch_create": [ctypes.POINTER(_vp)],

@@ -834,6 +834,204 @@ rd_status rd_decimate(int dim, float* d_S, int64_t ns, float r2, int64_t* ns_out
     return RD_OK;
 }
 
+// ------------------------------------------------------------------------
+// device-level steps with layouts, strides, the neighbour overload and
+// CUB-style caller scratch
+// ------------------------------------------------------------------------
+}  // extern "C"
+
+namespace {
+
+rd_status check_layout(int layout, int64_t pitch, int64_t n, int dim, const char* what)
+{
+    if (layout == RD_ROW_MAJOR) {
+        if (pitch != 0 && pitch < dim)
+            return set_err(RD_ERR_ARG, std::string(what) + ": ROW_MAJOR pitch < dim");
+        return RD_OK;
+    }
+    if (layout == RD_COL_MAJOR) {
+        if (pitch != 0 && pitch < n)
+            return set_err(RD_ERR_ARG, std::string(what) + ": COL_MAJOR pitch < point count");
+        return RD_OK;
+    }
+    return set_err(RD_ERR_ARG, std::string(what) + ": unknown layout");
+}
+
+constexpr size_t WS_ALIGN = 256;
+
+// Runs `plan` under a measuring arena and reports the bytes it added up.
+template <class Plan>
+rd_status ws_query(Engine& e, Plan plan, size_t* temp_bytes)
+{
+    DevArena m;
+    {
+        ArenaScope scope(&m);
+        if (rd_status s = plan(e)) return s;
+    }
+    *temp_bytes = (m.used + WS_ALIGN - 1) / WS_ALIGN * WS_ALIGN;
+    return RD_OK;
+}
+
+rd_status ws_check(void* d_temp, size_t* temp_bytes)
+{
+    if (!temp_bytes) return set_err(RD_ERR_ARG, "temp_bytes must not be null");
+    if (d_temp && (reinterpret_cast<uintptr_t>(d_temp) % WS_ALIGN) != 0)
+        return set_err(RD_ERR_ARG, "d_temp must be 256-byte aligned");
+    return RD_OK;
+}
+
+// one_cloud_engine has already recorded its message; a run's status comes
+// with the engine's message; either way a request that did not fit the
+// caller's scratch is reported as such
+rd_status ws_fail(int rc, Engine& e, const DevArena& a)
+{
+    if (a.exhausted)
+        return set_err(RD_ERR_CAPACITY, "temporary storage too small for this call (query "
+                                        "temp_bytes with d_temp = NULL for the same arguments)");
+    return from_engine(rc, e);
+}
+
+}  // namespace
+
+extern "C" {
+
+rd_status rd_choose_ws(int dim, const float* d_P, int64_t np, int p_layout, int64_t p_pitch,
+                       float r1, float* d_S, int s_layout, int64_t s_pitch, int64_t* ns_out,
+                       void* d_temp, size_t* temp_bytes, void* stream)
+{
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (rd_status s = ws_check(d_temp, temp_bytes)) return s;
+    if (np < 0 || np > INT32_MAX - 1024 || !(r1 > 0.0f)) return set_err(RD_ERR_ARG, "bad np or r1");
+    if (rd_status s = check_layout(p_layout, p_pitch, np, dim, "points")) return s;
+    if (rd_status s = check_layout(s_layout, s_pitch, np, dim, "chosen points")) return s;
+    if (!d_temp) {
+        if (np == 0) { *temp_bytes = WS_ALIGN; return RD_OK; }
+        Engine q;
+        return ws_query(q, [&](Engine& e) -> rd_status {
+            if (rd_status s = one_cloud_engine(e, dim, np, np, r1, r1)) return s;
+            return from_engine(e.plan_workspace(Engine::RUN_CHOOSE_ONLY), e);
+        }, temp_bytes);
+    }
+    if (!d_P || !d_S || !ns_out) return set_err(RD_ERR_ARG, "null argument");
+    *ns_out = 0;
+    if (np == 0) return RD_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    thread_local Engine& e = *new Engine();  // never destroyed: no CUDA calls at exit
+    DevArena a;
+    a.base = static_cast<char*>(d_temp);
+    a.cap = *temp_bytes;
+    ArenaScope scope(&a);
+    DevBuf none;
+    if (rd_status s = one_cloud_engine(e, dim, np, np, r1, r1)) return ws_fail(s, e, a);
+    if (rd_status s = load_points(d_P, p_layout, p_pitch, np, dim, 1, e.points(), none, st)) return s;
+    if (int rc = e.run(st, false, Engine::RUN_CHOOSE_ONLY)) return ws_fail(rc, e, a);
+    const int64_t ns = e.ns()[0];
+    // a COL_MAJOR output with pitch 0 has the input's capacity (np) as its pitch
+    const int64_t sp = (s_layout == RD_COL_MAJOR && s_pitch == 0) ? np : s_pitch;
+    if (rd_status s = store_points(e.chosen(), ns, dim, s_layout, sp, d_S, 1, none, st)) return s;
+    CK_CUDA(cudaStreamSynchronize(st));
+    *ns_out = ns;
+    return RD_OK;
+}
+
+rd_status rd_evolve_ws(int dim, const float* d_P, int64_t np, int p_layout, int64_t p_pitch,
+                       const float* d_N, int64_t nn, int n_layout, int64_t n_pitch, float* d_S,
+                       int64_t ns, int s_layout, int64_t s_pitch, float r1, int64_t max_passes,
+                       int64_t* passes_out, int32_t* moved_out, void* d_temp, size_t* temp_bytes,
+                       void* stream)
+{
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (rd_status s = ws_check(d_temp, temp_bytes)) return s;
+    if (np < 0 || nn < 0 || np + nn > INT32_MAX - 1024 || ns < 0 || ns > INT32_MAX - 1024 ||
+        max_passes < 0 || !(r1 > 0.0f))
+        return set_err(RD_ERR_ARG, "bad sizes, pass limit or r1");
+    if (rd_status s = check_layout(p_layout, p_pitch, np, dim, "points")) return s;
+    if (rd_status s = check_layout(n_layout, n_pitch, nn, dim, "neighbour points")) return s;
+    if (rd_status s = check_layout(s_layout, s_pitch, ns, dim, "chosen points")) return s;
+    const int64_t total = np + nn;
+    const int64_t cap = std::max(total, ns);
+    if (!d_temp) {
+        if (ns == 0) { *temp_bytes = WS_ALIGN; return RD_OK; }
+        Engine q;
+        return ws_query(q, [&](Engine& e) -> rd_status {
+            if (rd_status s = one_cloud_engine(e, dim, total, cap, r1, r1)) return s;
+            e.given_ns.assign(1, (int32_t)ns);
+            return from_engine(e.plan_workspace(Engine::RUN_EVOLVE_ONLY), e);
+        }, temp_bytes);
+    }
+    if ((np && !d_P) || (nn && !d_N) || !d_S) return set_err(RD_ERR_ARG, "null argument");
+    if (passes_out) *passes_out = 0;
+    if (moved_out) *moved_out = 0;
+    if (ns == 0) return RD_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    thread_local Engine& e = *new Engine();  // never destroyed: no CUDA calls at exit
+    DevArena a;
+    a.base = static_cast<char*>(d_temp);
+    a.cap = *temp_bytes;
+    ArenaScope scope(&a);
+    DevBuf none;
+    if (rd_status s = one_cloud_engine(e, dim, total, cap, r1, r1)) return ws_fail(s, e, a);
+    // the evolve points: the input points, then the neighbour points
+    // (DeviceEvolve::evolve's neighbour overload, device_evolve.cuh:70-97)
+    if (rd_status s = load_points(d_P, p_layout, p_pitch, np, dim, 1, e.points(), none, st)) return s;
+    if (rd_status s = load_points(d_N, n_layout, n_pitch, nn, dim, 1, e.points() + np * dim, none, st))
+        return s;
+    if (rd_status s = load_points(d_S, s_layout, s_pitch, ns, dim, 1, e.chosen_mut(), none, st))
+        return s;
+    e.given_ns.assign(1, (int32_t)ns);
+    e.max_passes = max_passes > 0 ? (int)std::min<int64_t>(max_passes, 1 << 16) : (1 << 16);
+    const int rc = e.run(st, max_passes != 1, Engine::RUN_EVOLVE_ONLY);
+    if (rc && rc != RD_ERR_NOT_CONVERGED) return ws_fail(rc, e, a);
+    if (rd_status s = store_points(e.chosen(), ns, dim, s_layout, s_pitch, d_S, 1, none, st)) return s;
+    CK_CUDA(cudaStreamSynchronize(st));
+    if (passes_out) *passes_out = e.stats().total_passes;
+    // the pass limit ends a run whose last pass still moved a chosen point
+    if (moved_out) *moved_out = (rc == RD_ERR_NOT_CONVERGED) ? 1 : 0;
+    if (rc == RD_ERR_NOT_CONVERGED && max_passes == 0) return from_engine(rc, e);
+    return RD_OK;
+}
+
+rd_status rd_decimate_ws(int dim, float* d_S, int64_t ns, int s_layout, int64_t s_pitch, float r2,
+                         int64_t* ns_out, void* d_temp, size_t* temp_bytes, void* stream)
+{
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (rd_status s = ws_check(d_temp, temp_bytes)) return s;
+    if (ns < 0 || ns > INT32_MAX - 1024 || !(r2 > 0.0f)) return set_err(RD_ERR_ARG, "bad ns or r2");
+    if (rd_status s = check_layout(s_layout, s_pitch, ns, dim, "chosen points")) return s;
+    if (!d_temp) {
+        if (ns == 0) { *temp_bytes = WS_ALIGN; return RD_OK; }
+        Engine q;
+        return ws_query(q, [&](Engine& e) -> rd_status {
+            if (rd_status s = one_cloud_engine(e, dim, 0, ns, r2, r2)) return s;
+            e.given_ns.assign(1, (int32_t)ns);
+            return from_engine(e.plan_workspace(Engine::RUN_DECIMATE_ONLY), e);
+        }, temp_bytes);
+    }
+    if (!d_S || !ns_out) return set_err(RD_ERR_ARG, "null argument");
+    *ns_out = ns;
+    if (ns == 0) return RD_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    thread_local Engine& e = *new Engine();  // never destroyed: no CUDA calls at exit
+    DevArena a;
+    a.base = static_cast<char*>(d_temp);
+    a.cap = *temp_bytes;
+    ArenaScope scope(&a);
+    DevBuf none;
+    if (rd_status s = one_cloud_engine(e, dim, 0, ns, r2, r2)) return ws_fail(s, e, a);
+    if (rd_status s = load_points(d_S, s_layout, s_pitch, ns, dim, 1, e.chosen_mut(), none, st))
+        return s;
+    e.given_ns.assign(1, (int32_t)ns);
+    if (int rc = e.run(st, false, Engine::RUN_DECIMATE_ONLY)) return ws_fail(rc, e, a);
+    const int64_t left = e.ns()[0];
+    // survivors keep their order and go to the front; a COL_MAJOR array keeps
+    // its pitch (the reference's decimate compacts in place the same way)
+    const int64_t sp = (s_layout == RD_COL_MAJOR && s_pitch == 0) ? ns : s_pitch;
+    if (rd_status s = store_points(e.chosen(), left, dim, s_layout, sp, d_S, 1, none, st)) return s;
+    CK_CUDA(cudaStreamSynchronize(st));
+    *ns_out = left;
+    return RD_OK;
+}
+
 rd_status rd_decimate_noalloc(int dim, float* d_S, int64_t ns, float r2, int32_t* d_ns_out,
                               void* stream)
 {

@@ -54,10 +54,42 @@ static std::atomic<int> g_assign_cull{1};
 void set_assign_cull(bool on) { g_assign_cull.store(on ? 1 : 0); }
 bool assign_cull_enabled() { return g_assign_cull.load() != 0; }
 
+namespace {
+thread_local DevArena* t_arena = nullptr;
+std::atomic<uint64_t> g_arena_gen{1};
+constexpr size_t ARENA_ALIGN = 256;
+}  // namespace
+
+DevArena* current_arena() { return t_arena; }
+
+ArenaScope::ArenaScope(DevArena* a) : prev(t_arena)
+{
+    a->gen = g_arena_gen.fetch_add(1);
+    t_arena = a;
+}
+
+ArenaScope::~ArenaScope() { t_arena = prev; }
+
 cudaError_t DevBuf::ensure(size_t want)
 {
     if (want == 0) want = 16;
-    if (want <= bytes) return cudaSuccess;
+    if (DevArena* a = t_arena) {
+        if (borrowed && gen == a->gen && want <= bytes) return cudaSuccess;
+        release();
+        const size_t off = (a->used + ARENA_ALIGN - 1) / ARENA_ALIGN * ARENA_ALIGN;
+        if (!a->measuring() && (off > a->cap || want > a->cap - off)) {
+            a->exhausted = true;
+            return cudaErrorMemoryAllocation;
+        }
+        // a measuring arena hands out distinct, aligned placeholders
+        p = a->measuring() ? reinterpret_cast<void*>(uintptr_t(ARENA_ALIGN) + off) : a->base + off;
+        a->used = off + want;
+        bytes = want;
+        borrowed = true;
+        gen = a->gen;
+        return cudaSuccess;
+    }
+    if (want <= bytes && !borrowed) return cudaSuccess;
     release();
     cudaError_t e = cudaMalloc(&p, want);
     if (e != cudaSuccess) {
@@ -71,9 +103,10 @@ cudaError_t DevBuf::ensure(size_t want)
 
 void DevBuf::release()
 {
-    if (p) cudaFree(p);
+    if (p && !borrowed) cudaFree(p);
     p = nullptr;
     bytes = 0;
+    borrowed = false;
 }
 
 Engine::Engine() {}
@@ -102,6 +135,7 @@ static cudaError_t upload(DevBuf& b, const std::vector<T>& h, cudaStream_t st)
 {
     cudaError_t e = b.ensure(sizeof(T) * (h.size() + 1));
     if (e != cudaSuccess || h.empty()) return e;
+    if (DevArena* a = current_arena(); a && a->measuring()) return cudaSuccess;
     return cudaMemcpyAsync(b.p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, st);
 }
 
@@ -260,8 +294,13 @@ int Engine::finish_setup_after_choose(cudaStream_t st)
 {
     const size_t nc = h_cl_.size();
     h_ns_.resize(nc);
-    RD_CK(cudaMemcpyAsync(h_ns_.data(), bNs_.p, 4 * nc, cudaMemcpyDeviceToHost, st));
-    RD_CK(cudaStreamSynchronize(st));
+    if (DevArena* a = current_arena(); a && a->measuring()) {
+        // size planning: the counts the caller will give
+        for (size_t c = 0; c < nc; ++c) h_ns_[c] = c < given_ns.size() ? given_ns[c] : h_cl_[c].n_own;
+    } else {
+        RD_CK(cudaMemcpyAsync(h_ns_.data(), bNs_.p, 4 * nc, cudaMemcpyDeviceToHost, st));
+        RD_CK(cudaStreamSynchronize(st));
+    }
     int64_t hist = 0, key = 0, kblk = 0, kblk_warp = 0;
     int max_ns = 0;
     h_slot_cloud_.clear();
@@ -476,6 +515,38 @@ int Engine::run(cudaStream_t st, bool use_graph, int mode)
         if (a1) cudaEventDestroy(a1);
     }
     return collect(st);
+}
+
+int Engine::plan_workspace(int mode)
+{
+    DevArena* a = current_arena();
+    if (!a || !a->measuring()) {
+        last_error = "workspace planning needs a measuring arena";
+        return 1;
+    }
+    // the buffers run() takes, in its order, for a single-cloud device step
+    RD_CK(upload(bCl_, h_cl_, nullptr));
+    RD_CK(upload(bGr_, h_gr_, nullptr));
+    RD_CK(upload(bChunkCloud_, h_chunk_cloud_, nullptr));
+    if (mode == RUN_EVOLVE_ONLY || mode == RUN_DECIMATE_ONLY) {
+        if (int rc = finish_setup_after_choose(nullptr)) return rc;
+        if (mode == RUN_EVOLVE_ONLY && cull_assign && assign_cull_enabled() && spatial_ok_ &&
+            total_points_ > 0) {
+            RD_CK(bPs_.ensure(sizeof(float) * (size_t)(total_points_ * dim_ + 4)));
+            RD_CK(bSorder_.ensure(sizeof(int32_t) * (size_t)(total_points_ + 1)));
+            RD_CK(bSpatialTmp_.ensure(spatial_prep_scratch_bytes(total_points_)));
+        }
+        return 0;
+    }
+    if (mode == RUN_CHOOSE_ONLY) {
+        if (h_cl_.size() == 1 && h_cl_[0].n_own >= (1 << 16)) {
+            RD_CK(bHash_.ensure(4 * (size_t)choose_hash_buckets()));
+            RD_CK(bSurv_.ensure((size_t)h_cl_[0].n_own + 16));
+        }
+        return 0;
+    }
+    last_error = "workspace planning covers the choose, evolve and decimate steps only";
+    return 1;
 }
 
 int Engine::adjoint_setup(cudaStream_t st)

@@ -10,10 +10,34 @@
 
 namespace rdb {
 
+// Caller-provided device scratch (CUB-style temporary storage).  While an
+// arena is installed on the calling thread (ArenaScope), every DevBuf::ensure
+// carves its buffer out of it (256-byte aligned, bump allocation) instead of
+// calling cudaMalloc, and fails with cudaErrorMemoryAllocation when the arena
+// is exhausted.  A measuring arena (base == nullptr) only adds up the sizes;
+// the buffers it hands out are placeholders that must not be dereferenced,
+// so only size planning runs under it (no kernel, no copy).
+struct DevArena {
+    char* base = nullptr;   // nullptr: measuring
+    size_t cap = 0;
+    size_t used = 0;
+    uint64_t gen = 0;       // set by ArenaScope; buffers from older arenas are stale
+    bool exhausted = false; // a request did not fit
+    bool measuring() const { return base == nullptr; }
+};
+DevArena* current_arena();
+struct ArenaScope {
+    DevArena* prev;
+    explicit ArenaScope(DevArena* a);
+    ~ArenaScope();
+};
+
 // A device buffer that only grows; reused across runs of one engine.
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
+    bool borrowed = false;   // carved from an arena: never freed here
+    uint64_t gen = 0;        // arena generation it was carved from
     cudaError_t ensure(size_t want);
     void release();
     ~DevBuf() { release(); }
@@ -75,6 +99,11 @@ public:
     // cloud's chosen points at its s_off in chosen_mut() and their counts into
     // given_ns.  Blocks until the run is complete.
     int run(cudaStream_t st, bool use_graph, int mode = RUN_FULL);
+    // Size planning for caller-provided scratch: under a measuring arena,
+    // after setup(), adds to the arena every buffer that run(st, *, mode)
+    // would take for the chosen counts in given_ns (RUN_CHOOSE_ONLY,
+    // RUN_EVOLVE_ONLY or RUN_DECIMATE_ONLY).  Launches nothing.
+    int plan_workspace(int mode);
     float* chosen_mut() { return bS_.as<float>(); }
     std::vector<int32_t> given_ns;
     // the adjoint's forward step: assign + ordered mean of one pass, no

@@ -160,3 +160,58 @@ def test_quality_restatement_matches_reference(case):
         b = O.quality(T, I, which, use_ref=True)
         assert np.array_equal(np.float32(a), np.float32(b)), (which, a, b)
     assert O.quality(np.zeros((0, 2), np.float32), I, "hausdorff") == -1.0
+
+
+# --------------------------------------------------------------------------
+# full-size fixtures (tests/golden/make_golden_fullsize.py): the clouds are
+# regenerated from their seeds and checked against the stored SHA-256
+# --------------------------------------------------------------------------
+
+def _regenerate(g):
+    import hashlib
+
+    from ridgedetection_b200 import generators as G
+    P = getattr(G, str(g["gen"]))(int(g["n"]), seed=int(g["seed"]))
+    assert hashlib.sha256(P.tobytes()).hexdigest() == str(g["sha"])
+    return P
+
+
+def test_full_helix_1m_choose_and_first_passes_match_reference():
+    g = np.load(os.path.join(GOLD, "full_helix3d_1m.npz"))
+    P, r1 = _regenerate(g), float(g["r1"])
+    S = O.choose(P, r1)
+    assert bits_equal(S, g["S_choose"])
+    for t in range(g["S_passes"].shape[0]):
+        S, _, _, _, cont = O.evolve_pass(P, S, r1)
+        assert cont == 1 and bits_equal(S, g["S_passes"][t]), t
+
+
+def test_full_tiled_1m_split_matches_reference():
+    g = np.load(os.path.join(GOLD, "full_spiral2d_1m_split.npz"))
+    P = _regenerate(g)
+    S, _, n_leaves = O.ridge_tiled(P, float(g["r1"]), float(g["r2"]),
+                                   int(g["max_tile_capacity"]), g["tiles_per_dim"])
+    assert n_leaves > 64   # the capacity subdivided tiles
+    assert bits_equal(S, g["S_final"])
+
+
+def test_batch_subset_small_clouds_match_reference():
+    """The clouds of the 256-cloud batch fixture with fewer than 5,000 points
+    (the larger ones are checked on the GPU against the same fixture)."""
+    import hashlib
+
+    from ridgedetection_b200 import generators as G
+    g = np.load(os.path.join(GOLD, "batch_subset_256.npz"))
+    spec = G.batch_spec()
+    off, checked = 0, 0
+    for k, c in enumerate(g["cloud_ids"]):
+        n, dim, r1, r2, seed = spec[int(c)]
+        m = int(g["ns"][k]) * dim
+        if n < 5000:
+            P = G.batch_cloud(n, dim, seed)
+            assert hashlib.sha256(P.tobytes()).hexdigest() == str(g["sha"][k])
+            S, _ = O.ridge_bf(P, r1, r2)
+            assert bits_equal(S, g["S_flat"][off:off + m].reshape(-1, dim)), int(c)
+            checked += 1
+        off += m
+    assert checked >= 30
