@@ -73,7 +73,7 @@ def parse_args():
     ap.add_argument("--assign-cull", default="on", choices=["on", "off"],
                     help="exact chunk-box culling of the brute-force assignment (off = all-pairs kernel)")
     ap.add_argument("--shape", default=None,
-                    help="BLOCK,ITEMS of the assignment kernel instead of the autotuner's pick "
+                    help="BLOCK,ITEMS[,CULL_ITEMS] of the assignment instead of the autotuner's pick "
                          "(a profiler distorts the tuner's timings)")
     ap.add_argument("--profile-run", action="store_true",
                     help="no timing and no JSON line: after --warmup solves, run --steps "
@@ -122,7 +122,7 @@ def run_profile(args):
         solve = lambda: rd(r1, r2, n + 1, (64, 64))  # noqa: E731
     else:
         if args.shape:
-            rdb.tune_set(dim, n, *[int(x) for x in args.shape.split(",")])
+            rdb.tune_set(dim, n, *[int(x) for x in args.shape.split(",")], r1=r1)
         else:
             rdb.autotune(dim, n, max(1, rdb.choose_count(dP, r1)), reps=6, points=dP, r1=r1)
         rd = rdb.BruteForceRidgeDetection(n, r1, r2, dim, loop_mode=rdb.LOOP_HOST)
@@ -294,7 +294,8 @@ def run_b200_bf(args, world, rank, local):
     # launch shape of the assignment kernel from the project's autotuner, on a
     # synthetic cloud of this size with the chosen count of the first choose
     # (setup, outside every timed region)
-    tb, ti, tus = rdb.autotune(dim, n, max(1, rdb.choose_count(dP, r1)), reps=6, points=dP, r1=r1)
+    tb, ti, tci, tus = rdb.autotune(dim, n, max(1, rdb.choose_count(dP, r1)), reps=6, points=dP,
+                                    r1=r1)
     rd = rdb.BruteForceRidgeDetection(n, r1, r2, dim)
     rd.set_points(dP)
 
@@ -439,8 +440,9 @@ def run_b200_bf(args, world, rank, local):
                    "l2": "flushed (256 MiB write) between timed steps",
                    "loop": "CUDA graph WHILE node", "parallelism": f"replicas x{world}",
                    "assign": "culled (exact chunk-box culling)" if culled else "all pairs",
-                   "assign_shape": {"block": tb, "items": ti, "source": "rd_autotune",
-                                    "tuned_us_per_launch": tus}},
+                   "assign_shape": {"block": tb, "items": ti, "cull_items": tci,
+                                    "source": "rd_autotune (median of 5 runs per shape)",
+                                    "tuned_us_per_pass": tus}},
         "solves_per_s": world * 1e3 / ms_max,
         "pairs_per_step": pairs_step, "loop_iters_per_step": iters_step,
         "ns_final": ns_final,

@@ -78,13 +78,20 @@ RD_API int rd_supported_dims(void);
 RD_API rd_status rd_probe_fp32_peak(double* tflops, void* stream);
 /* Launch-shape tuning (no reference counterpart: the reference's launch
  * shapes are compile-time constants).  When an engine is set up, the
- * assignment kernel's shape -- CTA size `block` and points per thread
- * `items` -- is looked up for (dim, floor(log2(points of the largest
- * cloud))).  Supported shapes: block 128 with items 4, 8 or 16, block 256
- * with items 4 or 8; unset buckets use 128 x 8.  The table is process-wide
- * and thread-safe; shapes change speed only, never results. */
-RD_API rd_status rd_tune_set(int dim, int64_t n, int block, int items);
-RD_API rd_status rd_tune_get(int dim, int64_t n, int* block, int* items);
+ * assignment's shape is looked up for (dim, floor(log2(points of the largest
+ * cloud)), floor(2 log2(r1 of that cloud))): CTA size `block` and points per
+ * thread `items` of the all-pairs kernel (block x items is also the chunk of
+ * points the grouping kernels work on), and `cull_items`, the points per lane
+ * of the culled kernel (a warp's culling box holds 32 x cull_items points of
+ * the spatial order).  Supported: block 128 with items 4, 8 or 16, block 256
+ * with items 4 or 8; cull_items 2, 4 or 8.  r1 <= 0 stores or looks up an
+ * entry valid for every radius.  A lookup takes the exact bucket, else the
+ * any-radius entry, else the nearest radius bucket of the same dim and size,
+ * else 128 x 8 with cull_items 4.  The table is process-wide and thread-safe;
+ * shapes change speed only, never results. */
+RD_API rd_status rd_tune_set(int dim, int64_t n, float r1, int block, int items, int cull_items);
+RD_API rd_status rd_tune_get(int dim, int64_t n, float r1, int* block, int* items,
+                             int* cull_items);
 RD_API rd_status rd_tune_reset(void);
 /* Exact culling of the brute-force assignment (no reference counterpart; it
  * replaces nothing and changes no result).  rd/cpu/brute_force/evolve.hpp:43-66
@@ -96,15 +103,28 @@ RD_API rd_status rd_tune_reset(void);
  * read when a run starts. */
 RD_API rd_status rd_set_assign_cull(int enable);
 RD_API rd_status rd_get_assign_cull(int* enable);
-/* Times every supported shape on the cloud d_P (device, n x dim ROW_MAJOR;
+/* Cluster evolve of heavy tiles (no reference counterpart; it replaces nothing
+ * and changes no result).  In tiled runs, a tile with at least min_points
+ * evolve points (own + halo) is evolved by a thread-block cluster of 8 CTAs
+ * instead of one CTA, and each of its keys with at least seg_min members is
+ * folded in 8 segments whose exact FP32 sums are composed in index order.
+ * enable = 0: one CTA per tile.  0 for a threshold keeps its default (24,576
+ * points, 8,192 members).  Process-wide, read when a run starts. */
+RD_API rd_status rd_set_tile_clusters(int enable, int64_t min_points, int64_t seg_min);
+RD_API rd_status rd_get_tile_clusters(int* enable, int64_t* min_points, int64_t* seg_min);
+/* Times the supported shapes of the assignment the run would use (culled or
+ * all pairs, rd_get_assign_cull) on the cloud d_P (device, n x dim ROW_MAJOR;
  * NULL = n synthetic points uniform in the unit cube) with its first ns points
- * as the chosen set and assignment radius r1: the assignment kernel is timed
- * with CUDA events over `reps` evolve passes, twice per shape, keeping each
- * shape's better mean.  Stores the fastest for (dim, bucket of n) and returns
- * it with its time per launch in microseconds.  Runs on `stream` and waits
- * for it; d_P is not modified. */
+ * as the chosen set and radius r1: `reps` evolve passes per run, timed whole
+ * with CUDA events; five runs per shape, interleaved over the shapes; the
+ * shape with the lowest median time per pass wins -- unless the table already
+ * holds a shape for this (dim, n, r1) bucket that is within 3% of it, which
+ * is kept.  Stores the pick for the bucket and returns it with its median time
+ * per pass in microseconds.  Runs on `stream` and waits for it; d_P is not
+ * modified. */
 RD_API rd_status rd_autotune(int dim, const float* d_P, int64_t n, int64_t ns, float r1, int reps,
-                             int* block, int* items, double* us_per_launch, void* stream);
+                             int* block, int* items, int* cull_items, double* us_per_pass,
+                             void* stream);
 
 /* Orders a ridge into chains: rd::orderSamples (rd/cpu/brute_force/order.hpp:45)
  * with the condition of the brute-force class's order_ option
@@ -160,8 +180,10 @@ RD_API rd_status rd_save_binary_cloud(const char* path, const float* pts, int64_
  * coordinate d < dim, out[d] = the left-to-right FP32 sum, starting from 0 with
  * one rounding per term, of d_P[d_idx[i]*dim + d] for i = 0..n-1.  method 0
  * evaluates it as a chain of adds, method 1 with the warp-parallel exact
- * evaluation and method 2 with the CTA-wide exact evaluation that the evolve
- * kernels use for large clusters; all are bit-identical to the serial loop.  All pointers are device pointers; d_out
+ * evaluation, method 2 with the CTA-wide exact evaluation in rounds, methods
+ * 3 and 4 with the warp-segmented evaluation (speculative segment starts,
+ * traces composed exactly; 8 and 32 segments) that the tiled evolve kernels
+ * use for large clusters; all are bit-identical to the serial loop.  All pointers are device pointers; d_out
  * holds dim floats.  Runs on `stream` and waits for it. */
 RD_API rd_status rd_ordered_sum(int dim, const float* d_P, const int32_t* d_idx, int64_t n,
                                 float* d_out, int method, void* stream);

@@ -62,14 +62,18 @@ SIGNATURES = {
     "rd_abi_version": [],
     "rd_supported_dims": [],
     "rd_probe_fp32_peak": [ctypes.POINTER(ctypes.c_double), _vp],
-    "rd_tune_set": [ctypes.c_int, ctypes.c_int64, ctypes.c_int, ctypes.c_int],
-    "rd_tune_get": [ctypes.c_int, ctypes.c_int64, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
+    "rd_tune_set": [ctypes.c_int, ctypes.c_int64, ctypes.c_float, ctypes.c_int, ctypes.c_int,
+                    ctypes.c_int],
+    "rd_tune_get": [ctypes.c_int, ctypes.c_int64, ctypes.c_float, ctypes.POINTER(ctypes.c_int),
+                    ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
     "rd_tune_reset": [],
     "rd_set_assign_cull": [ctypes.c_int],
     "rd_get_assign_cull": [ctypes.POINTER(ctypes.c_int)],
+    "rd_set_tile_clusters": [ctypes.c_int, ctypes.c_int64, ctypes.c_int64],
+    "rd_get_tile_clusters": [ctypes.POINTER(ctypes.c_int), _pi64, _pi64],
     "rd_autotune": [ctypes.c_int, _vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_float, ctypes.c_int,
                     ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
-                    ctypes.POINTER(ctypes.c_double), _vp],
+                    ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double), _vp],
     "rd_hausdorff": [_i, _vp, _i64, _vp, _i64, _pf, _vp],
     "rd_distance_stats": [_i, _vp, _i64, _vp, _i64, _pf, _pf, _pf, _pf, _vp],
     "rd_segment_hausdorff": [_i, _vp, _i64, _pf, _vp],

@@ -311,18 +311,23 @@ def pack_clouds(clouds: Sequence[Tuple[np.ndarray, float, float]]):
 # launch-shape tuning (no reference counterpart)
 # ---------------------------------------------------------------------------
 
-def tune_set(dim: int, n: int, block: int, items: int) -> None:
+def tune_set(dim: int, n: int, block: int, items: int, cull_items: int = 4,
+             r1: float = 0.0) -> None:
     """Use CTA size ``block`` and ``items`` points per thread for the
-    assignment kernel of clouds of dimension ``dim`` whose size is in the
-    power-of-two bucket of ``n``."""
-    L.check(L.lib().rd_tune_set(dim, n, block, items))
+    all-pairs assignment (and as the grouping chunk) and ``cull_items`` points
+    per lane for the culled assignment, for clouds of dimension ``dim`` whose
+    size is in the power-of-two bucket of ``n`` and whose r1 is in the
+    half-octave bucket of ``r1`` (r1 <= 0: every radius)."""
+    L.check(L.lib().rd_tune_set(dim, n, float(r1), block, items, cull_items))
 
 
-def tune_get(dim: int, n: int) -> Tuple[int, int]:
-    """(block, items) the engine will use for a ``dim``-D cloud of ``n`` points."""
-    b, i = ctypes.c_int(0), ctypes.c_int(0)
-    L.check(L.lib().rd_tune_get(dim, n, ctypes.byref(b), ctypes.byref(i)))
-    return b.value, i.value
+def tune_get(dim: int, n: int, r1: float = 0.0) -> Tuple[int, int, int]:
+    """(block, items, cull_items) the engine will use for a ``dim``-D cloud of
+    ``n`` points with radius ``r1``."""
+    b, i, c = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+    L.check(L.lib().rd_tune_get(dim, n, float(r1), ctypes.byref(b), ctypes.byref(i),
+                                ctypes.byref(c)))
+    return b.value, i.value, c.value
 
 
 def tune_reset() -> None:
@@ -344,6 +349,20 @@ def get_assign_cull() -> bool:
     return bool(e.value)
 
 
+def set_tile_clusters(enable: bool, min_points: int = 0, seg_min: int = 0) -> None:
+    """Cluster evolve of heavy tiles in tiled runs (changes no result): tiles
+    with at least min_points evolve points are evolved by a thread-block
+    cluster, keys with at least seg_min members folded in segments across it
+    (0 = default threshold).  Process-wide."""
+    L.check(L.lib().rd_set_tile_clusters(1 if enable else 0, int(min_points), int(seg_min)))
+
+
+def get_tile_clusters() -> Tuple[bool, int, int]:
+    e, m, s = ctypes.c_int(0), ctypes.c_int64(0), ctypes.c_int64(0)
+    L.check(L.lib().rd_get_tile_clusters(ctypes.byref(e), ctypes.byref(m), ctypes.byref(s)))
+    return bool(e.value), int(m.value), int(s.value)
+
+
 def choose_count(P, r1: float) -> int:
     """Number of points the greedy r1-ball choose keeps for the cloud P (a
     float32 CUDA tensor or numpy array, ROW_MAJOR n x dim)."""
@@ -360,13 +379,14 @@ def choose_count(P, r1: float) -> int:
 
 
 def autotune(dim: int, n: int, ns: int, reps: int = 5, points=None,
-             r1: float = 2.0) -> Tuple[int, int, float]:
-    """Time every supported assignment shape and keep the fastest for the size
-    bucket of ``n``; returns (block, items, microseconds per launch).  With
-    ``points`` (a float32 CUDA tensor, n x dim) the timing runs on that cloud
-    with its first ``ns`` points as the chosen set and radius ``r1``;
+             r1: float = 2.0) -> Tuple[int, int, int, float]:
+    """Time the supported shapes of the assignment in use and keep the best
+    (median of five runs, the incumbent kept within 3%) for the (dim, size,
+    r1) bucket; returns (block, items, cull_items, microseconds per pass).
+    With ``points`` (a float32 CUDA tensor, n x dim) the timing runs on that
+    cloud with its first ``ns`` points as the chosen set and radius ``r1``;
     otherwise on ``n`` synthetic uniform points."""
-    b, i, us = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_double(0)
+    b, i, c, us = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0), ctypes.c_double(0)
     ptr = None
     if points is not None:
         if not _is_torch_cuda(points):
@@ -374,8 +394,8 @@ def autotune(dim: int, n: int, ns: int, reps: int = 5, points=None,
         ptr = ctypes.c_void_p(points.contiguous().data_ptr())
         n = int(points.shape[0])
     L.check(L.lib().rd_autotune(dim, ptr, n, ns, float(r1), reps, ctypes.byref(b),
-                                ctypes.byref(i), ctypes.byref(us), None))
-    return b.value, i.value, us.value
+                                ctypes.byref(i), ctypes.byref(c), ctypes.byref(us), None))
+    return b.value, i.value, c.value, us.value
 
 
 def order_chains(S, r2: float):

@@ -64,7 +64,7 @@ int AdjointRunner::run(int dim, const float* d_P, int64_t np, const float* d_S0,
                        float r1, int iters, int ckpt, const double* d_W, float* d_S_final,
                        double* d_gP, double* d_gS0, cudaStream_t st)
 {
-    if (dim != 2 && dim != 3) { last_error = "dim must be 2 or 3"; return 6; }
+    if (!dim_supported(dim)) { last_error = "dim must be 1 to 4"; return 6; }
     if (np < 1 || ns < 1 || ns > np || iters < 0 || ckpt < 0) { last_error = "bad sizes"; return 1; }
     CloudDesc cd;
     std::memset(&cd, 0, sizeof(cd));
@@ -122,14 +122,12 @@ int AdjointRunner::run(int dim, const float* d_P, int64_t np, const float* d_S0,
             const int slot = (nseg > 1) ? t - t0 : t;
             const int32_t* kt = bKeys_.as<int32_t>() + (size_t)slot * np;
             const int32_t* ct = bCnt_.as<int32_t>() + (size_t)slot * ns;
-            if (dim == 2) {
-                k_adj_members<2><<<grid_for(np), 256, 0, st>>>(kt, ct, bG_.as<double>(), np, d_gP);
-                k_adj_carry<2><<<grid_for(ns), 256, 0, st>>>(ct, ns, bG_.as<double>());
-            } else {
-                k_adj_members<3><<<grid_for(np), 256, 0, st>>>(kt, ct, bG_.as<double>(), np, d_gP);
-                k_adj_carry<3><<<grid_for(ns), 256, 0, st>>>(ct, ns, bG_.as<double>());
-            }
-            AK(cudaGetLastError());
+            AK(with_dim(dim, [&](auto D) {
+                constexpr int DIM = decltype(D)::value;
+                k_adj_members<DIM><<<grid_for(np), 256, 0, st>>>(kt, ct, bG_.as<double>(), np, d_gP);
+                k_adj_carry<DIM><<<grid_for(ns), 256, 0, st>>>(ct, ns, bG_.as<double>());
+                return cudaGetLastError();
+            }));
         }
     }
     if (d_gS0) AK(cudaMemcpyAsync(d_gS0, bG_.p, sizeof(double) * ns * dim, cudaMemcpyDeviceToDevice, st));

@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(256) k_fma_probe(float* out, int iters, float 
     if (r == 1234.5678f) out[threadIdx.x] = r;  // keeps the chains live
 }
 
-bool dim_ok(int dim) { return dim == 2 || dim == 3; }
+bool dim_ok(int dim) { return dim_supported(dim); }
 
 }  // namespace
 
@@ -222,7 +222,12 @@ const char* rd_last_error(void) { return g_err.c_str(); }
 
 int rd_abi_version(void) { return 2; }
 
-int rd_supported_dims(void) { return (1 << 2) | (1 << 3); }
+int rd_supported_dims(void)
+{
+    int m = 0;
+    for (int d = 1; d <= RD_MAX_DIM; ++d) m |= 1 << d;
+    return m;
+}
 
 rd_status rd_probe_fp32_peak(double* tflops, void* stream)
 {
@@ -257,26 +262,28 @@ rd_status rd_probe_fp32_peak(double* tflops, void* stream)
 static rd_status one_cloud_engine(Engine& e, int dim, int64_t n_points, int64_t capacity, float r1,
                                   float r2);
 
-static bool shape_ok(int dim, int block, int items)
+static bool shape_ok(int dim, int block, int items, int cull_items)
 {
-    return dim_ok(dim) && tune_supported(dim, TuneParams{block, items});
+    return dim_ok(dim) && tune_supported(dim, TuneParams{block, items, cull_items});
 }
 
-rd_status rd_tune_set(int dim, int64_t n, int block, int items)
+rd_status rd_tune_set(int dim, int64_t n, float r1, int block, int items, int cull_items)
 {
-    if (!shape_ok(dim, block, items)) return set_err(RD_ERR_UNSUPPORTED, "unsupported dim or launch shape");
+    if (!shape_ok(dim, block, items, cull_items))
+        return set_err(RD_ERR_UNSUPPORTED, "unsupported dim or launch shape");
     if (n < 1) return set_err(RD_ERR_ARG, "n must be positive");
-    tune_store(dim, n, TuneParams{block, items});
+    tune_store(dim, n, r1, TuneParams{block, items, cull_items});
     return RD_OK;
 }
 
-rd_status rd_tune_get(int dim, int64_t n, int* block, int* items)
+rd_status rd_tune_get(int dim, int64_t n, float r1, int* block, int* items, int* cull_items)
 {
-    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
-    if (!block || !items) return set_err(RD_ERR_ARG, "null argument");
-    const TuneParams tp = tune_lookup(dim, n);
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 1 to 4");
+    if (!block || !items || !cull_items) return set_err(RD_ERR_ARG, "null argument");
+    const TuneParams tp = tune_lookup(dim, n, r1);
     *block = tp.block;
     *items = tp.items;
+    *cull_items = tp.cull_items;
     return RD_OK;
 }
 
@@ -292,6 +299,26 @@ rd_status rd_set_assign_cull(int enable)
     return RD_OK;
 }
 
+rd_status rd_set_tile_clusters(int enable, int64_t min_points, int64_t seg_min)
+{
+    if (min_points < 0 || seg_min < 0 || min_points > INT32_MAX || seg_min > INT32_MAX)
+        return set_err(RD_ERR_ARG, "negative or too large threshold");
+    const TileClusterParams d = tile_cluster_defaults();
+    set_tile_cluster_params(TileClusterParams{enable != 0, min_points ? (int)min_points : d.min_points,
+                                              seg_min ? (int)seg_min : d.seg_min});
+    return RD_OK;
+}
+
+rd_status rd_get_tile_clusters(int* enable, int64_t* min_points, int64_t* seg_min)
+{
+    if (!enable || !min_points || !seg_min) return set_err(RD_ERR_ARG, "null argument");
+    const TileClusterParams p = tile_cluster_params();
+    *enable = p.enabled ? 1 : 0;
+    *min_points = p.min_points;
+    *seg_min = p.seg_min;
+    return RD_OK;
+}
+
 rd_status rd_get_assign_cull(int* enable)
 {
     if (!enable) return set_err(RD_ERR_ARG, "null argument");
@@ -300,10 +327,10 @@ rd_status rd_get_assign_cull(int* enable)
 }
 
 rd_status rd_autotune(int dim, const float* d_P, int64_t n, int64_t ns, float r1, int reps,
-                      int* block, int* items, double* us_per_launch, void* stream)
+                      int* block, int* items, int* cull_items, double* us_per_pass, void* stream)
 {
-    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
-    if (!block || !items) return set_err(RD_ERR_ARG, "null argument");
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 1 to 4");
+    if (!block || !items || !cull_items) return set_err(RD_ERR_ARG, "null argument");
     if (n < 1 || n > INT32_MAX - 1024 || ns < 1 || ns > n || reps < 1 || reps > 1000 || !(r1 > 0.0f))
         return set_err(RD_ERR_ARG, "need 1 <= ns <= n, 1 <= reps <= 1000 and r1 > 0");
     cudaStream_t st = (cudaStream_t)stream;
@@ -319,42 +346,65 @@ rd_status rd_autotune(int dim, const float* d_P, int64_t n, int64_t ns, float r1
     }
     const cudaMemcpyKind kind = d_P ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     const float* src = d_P ? d_P : pts.data();
-    const std::vector<TuneParams>& cand = tune_candidates();
-    std::vector<double> us(cand.size(), -1.0);
-    for (int round = 0; round < 2; ++round) {
+    const bool culled = assign_cull_enabled();
+    const std::vector<TuneParams>& cand = tune_candidates(culled);
+    // Every candidate runs `reps` evolve passes from the same chosen set, the
+    // whole run timed with CUDA events (assignment, grouping and folds: all
+    // that the shape changes); NREP repetitions, interleaved over the
+    // candidates so that clock drift hits them alike; the median decides.
+    constexpr int NREP = 5;
+    std::vector<std::vector<float>> ms(cand.size());
+    cudaEvent_t e0, e1;
+    CK_CUDA(cudaEventCreate(&e0));
+    CK_CUDA(cudaEventCreate(&e1));
+    int passes_run = reps;
+    for (int rep = 0; rep < NREP; ++rep) {
         for (size_t ci = 0; ci < cand.size(); ++ci) {
-            const TuneParams& tp = cand[ci];
-            if (!tune_supported(dim, tp)) continue;
             Engine e;
-            e.tune = tp;
+            e.tune = cand[ci];
             e.tune_locked = true;
             e.max_passes = reps;
-            e.profile_assign = true;
             if (rd_status s = one_cloud_engine(e, dim, n, n, r1, r1)) return s;
             CK_CUDA(cudaMemcpyAsync(e.points(), src, sizeof(float) * n * dim, kind, st));
             CK_CUDA(cudaMemcpyAsync(e.chosen_mut(), src, sizeof(float) * ns * dim, kind, st));
             e.given_ns.assign(1, (int32_t)ns);
+            CK_CUDA(cudaEventRecord(e0, st));
             const int rc = e.run(st, false, Engine::RUN_EVOLVE_ONLY);
+            CK_CUDA(cudaEventRecord(e1, st));
             if (rc && rc != RD_ERR_NOT_CONVERGED) return from_engine(rc, e);
-            const RunStats& rs = e.stats();
-            if (rs.assign_launches <= 0) continue;
-            const double t = 1e3 * rs.assign_ms / (double)rs.assign_launches;
-            if (us[ci] < 0 || t < us[ci]) us[ci] = t;
+            CK_CUDA(cudaEventSynchronize(e1));
+            float t = 0;
+            CK_CUDA(cudaEventElapsedTime(&t, e0, e1));
+            passes_run = std::max<int>(1, (int)e.stats().total_passes);
+            ms[ci].push_back(t / (float)passes_run);
         }
     }
-    CK_CUDA(cudaStreamSynchronize(st));
-    double best = -1.0;
-    TuneParams bt{128, 8};
-    for (size_t ci = 0; ci < cand.size(); ++ci)
-        if (us[ci] >= 0 && (best < 0 || us[ci] < best)) {
-            best = us[ci];
-            bt = cand[ci];
-        }
-    if (best < 0) return set_err(RD_ERR_CUDA, "no launch shape could be timed");
-    tune_store(dim, n, bt);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    auto median = [](std::vector<float> v) {
+        std::sort(v.begin(), v.end());
+        return v[v.size() / 2];
+    };
+    size_t bi = 0;
+    std::vector<float> med(cand.size());
+    for (size_t ci = 0; ci < cand.size(); ++ci) {
+        med[ci] = median(ms[ci]);
+        if (med[ci] < med[bi]) bi = ci;
+    }
+    // keep the shape already in the table unless the new one is 3% faster
+    TuneParams inc;
+    if (tune_find_exact(dim, n, r1, &inc)) {
+        for (size_t ci = 0; ci < cand.size(); ++ci)
+            if (cand[ci].block == inc.block && cand[ci].items == inc.items &&
+                cand[ci].cull_items == inc.cull_items && med[bi] > 0.97f * med[ci])
+                bi = ci;
+    }
+    const TuneParams bt = cand[bi];
+    tune_store(dim, n, r1, bt);
     *block = bt.block;
     *items = bt.items;
-    if (us_per_launch) *us_per_launch = best;
+    *cull_items = bt.cull_items;
+    if (us_per_pass) *us_per_pass = 1e3 * med[bi];
     return RD_OK;
 }
 
@@ -364,7 +414,7 @@ rd_status rd_autotune(int dim, const float* d_P, int64_t n, int64_t ns, float r1
 rd_status rd_hausdorff(int dim, const float* d_T, int64_t nt, const float* d_I, int64_t ni,
                        float* out, void* stream)
 {
-    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 1 to 4");
     if (!out || (nt > 0 && !d_T) || (ni > 0 && !d_I)) return set_err(RD_ERR_ARG, "null argument");
     if (nt < 0 || ni < 0 || nt > INT32_MAX || ni > INT32_MAX) return set_err(RD_ERR_ARG, "bad sizes");
     if (nt == 0) {
@@ -389,7 +439,7 @@ rd_status rd_distance_stats(int dim, const float* d_S, int64_t n, const float* d
                             float* median, float* mean, float* min_dist, float* max_dist,
                             void* stream)
 {
-    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 1 to 4");
     if (!median || !mean || !min_dist || !max_dist || !d_S || (ni > 0 && !d_I))
         return set_err(RD_ERR_ARG, "null argument");
     if (n < 1 || ni < 0 || n > INT32_MAX / 2 || ni > INT32_MAX)
@@ -418,7 +468,7 @@ rd_status rd_distance_stats(int dim, const float* d_S, int64_t n, const float* d
 
 rd_status rd_segment_hausdorff(int dim, const float* d_T, int64_t nt, float* out, void* stream)
 {
-    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 1 to 4");
     if (!out || (nt > 0 && !d_T)) return set_err(RD_ERR_ARG, "null argument");
     if (nt < 0 || nt > INT32_MAX) return set_err(RD_ERR_ARG, "bad size");
     if (nt == 0) {
@@ -439,7 +489,7 @@ rd_status rd_segment_hausdorff(int dim, const float* d_T, int64_t nt, float* out
 rd_status rd_order_chains(int dim, const float* d_S, int64_t ns, float r2, int32_t* d_order,
                           int32_t* d_chain_start, int64_t* n_chains, void* stream)
 {
-    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 1 to 4");
     if (!d_chain_start || !n_chains || (ns > 0 && (!d_S || !d_order)))
         return set_err(RD_ERR_ARG, "null argument");
     if (ns < 0 || ns > INT32_MAX / 2 - 1 || !(r2 > 0.0f)) return set_err(RD_ERR_ARG, "bad ns or r2");
@@ -464,10 +514,10 @@ rd_status rd_order_chains(int dim, const float* d_S, int64_t ns, float r2, int32
 rd_status rd_ordered_sum(int dim, const float* d_P, const int32_t* d_idx, int64_t n,
                          float* d_out, int method, void* stream)
 {
-    if (dim != 2 && dim != 3) return set_err(RD_ERR_ARG, "dim must be 2 or 3");
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 1 to 4");
     if (n < 0 || n > INT32_MAX) return set_err(RD_ERR_ARG, "n out of range");
     if ((n > 0 && (!d_P || !d_idx)) || !d_out) return set_err(RD_ERR_ARG, "null argument");
-    if (method < 0 || method > 2) return set_err(RD_ERR_ARG, "method must be 0, 1 or 2");
+    if (method < 0 || method > 4) return set_err(RD_ERR_ARG, "method must be 0 to 4");
     cudaStream_t st = (cudaStream_t)stream;
     CK_CUDA(launch_ordered_sum(dim, d_P, d_idx, (int)n, d_out, method, st));
     CK_CUDA(cudaStreamSynchronize(st));
@@ -482,7 +532,7 @@ rd_status rd_bf_create(rd_bf** out, int dim, int in_layout, int out_layout, int6
 {
     if (!out) return set_err(RD_ERR_ARG, "null handle pointer");
     *out = nullptr;
-    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 1 to 4");
     if ((in_layout != RD_ROW_MAJOR && in_layout != RD_COL_MAJOR) ||
         (out_layout != RD_ROW_MAJOR && out_layout != RD_COL_MAJOR))
         return set_err(RD_ERR_ARG, "unknown layout");
@@ -590,7 +640,7 @@ rd_status rd_tiled_create(rd_tiled** out, int dim, int in_layout, int out_layout
 {
     if (!out) return set_err(RD_ERR_ARG, "null handle pointer");
     *out = nullptr;
-    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 1 to 4");
     if ((in_layout != RD_ROW_MAJOR && in_layout != RD_COL_MAJOR) ||
         (out_layout != RD_ROW_MAJOR && out_layout != RD_COL_MAJOR))
         return set_err(RD_ERR_ARG, "unknown layout");
@@ -748,7 +798,7 @@ static rd_status one_cloud_engine(Engine& e, int dim, int64_t n_points, int64_t 
 rd_status rd_choose(int dim, const float* d_P, int64_t np, float r1, float* d_S, int64_t* ns_out,
                     void* stream)
 {
-    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 1 to 4");
     if (!d_P || !d_S || !ns_out) return set_err(RD_ERR_ARG, "null argument");
     if (np < 0 || np > INT32_MAX - 1024 || !(r1 > 0.0f)) return set_err(RD_ERR_ARG, "bad np or r1");
     *ns_out = 0;
@@ -768,7 +818,7 @@ rd_status rd_choose(int dim, const float* d_P, int64_t np, float r1, float* d_S,
 rd_status rd_evolve(int dim, const float* d_P, int64_t np, float* d_S, int64_t ns, float r1,
                     int64_t* passes_out, void* stream)
 {
-    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 1 to 4");
     if (!d_P || !d_S) return set_err(RD_ERR_ARG, "null argument");
     if (np < 0 || np > INT32_MAX - 1024 || ns < 0 || ns > INT32_MAX - 1024 || !(r1 > 0.0f))
         return set_err(RD_ERR_ARG, "bad sizes or r1");
@@ -791,7 +841,7 @@ rd_status rd_evolve(int dim, const float* d_P, int64_t np, float* d_S, int64_t n
 rd_status rd_evolve_pass(int dim, const float* d_P, int64_t np, float* d_S, int64_t ns, float r1,
                          int32_t* moved_out, void* stream)
 {
-    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 1 to 4");
     if (!d_P || !d_S || !moved_out) return set_err(RD_ERR_ARG, "null argument");
     if (np < 0 || np > INT32_MAX - 1024 || ns < 0 || ns > INT32_MAX - 1024 || !(r1 > 0.0f))
         return set_err(RD_ERR_ARG, "bad sizes or r1");
@@ -816,7 +866,7 @@ rd_status rd_evolve_pass(int dim, const float* d_P, int64_t np, float* d_S, int6
 
 rd_status rd_decimate(int dim, float* d_S, int64_t ns, float r2, int64_t* ns_out, void* stream)
 {
-    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 1 to 4");
     if (!d_S || !ns_out) return set_err(RD_ERR_ARG, "null argument");
     if (ns < 0 || ns > INT32_MAX - 1024 || !(r2 > 0.0f)) return set_err(RD_ERR_ARG, "bad ns or r2");
     *ns_out = ns;
@@ -899,7 +949,7 @@ rd_status rd_choose_ws(int dim, const float* d_P, int64_t np, int p_layout, int6
                        float r1, float* d_S, int s_layout, int64_t s_pitch, int64_t* ns_out,
                        void* d_temp, size_t* temp_bytes, void* stream)
 {
-    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 1 to 4");
     if (rd_status s = ws_check(d_temp, temp_bytes)) return s;
     if (np < 0 || np > INT32_MAX - 1024 || !(r1 > 0.0f)) return set_err(RD_ERR_ARG, "bad np or r1");
     if (rd_status s = check_layout(p_layout, p_pitch, np, dim, "points")) return s;
@@ -940,7 +990,7 @@ rd_status rd_evolve_ws(int dim, const float* d_P, int64_t np, int p_layout, int6
                        int64_t* passes_out, int32_t* moved_out, void* d_temp, size_t* temp_bytes,
                        void* stream)
 {
-    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 1 to 4");
     if (rd_status s = ws_check(d_temp, temp_bytes)) return s;
     if (np < 0 || nn < 0 || np + nn > INT32_MAX - 1024 || ns < 0 || ns > INT32_MAX - 1024 ||
         max_passes < 0 || !(r1 > 0.0f))
@@ -994,7 +1044,7 @@ rd_status rd_evolve_ws(int dim, const float* d_P, int64_t np, int p_layout, int6
 rd_status rd_decimate_ws(int dim, float* d_S, int64_t ns, int s_layout, int64_t s_pitch, float r2,
                          int64_t* ns_out, void* d_temp, size_t* temp_bytes, void* stream)
 {
-    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 1 to 4");
     if (rd_status s = ws_check(d_temp, temp_bytes)) return s;
     if (ns < 0 || ns > INT32_MAX - 1024 || !(r2 > 0.0f)) return set_err(RD_ERR_ARG, "bad ns or r2");
     if (rd_status s = check_layout(s_layout, s_pitch, ns, dim, "chosen points")) return s;
@@ -1047,7 +1097,7 @@ rd_status rd_evolve_adjoint(int dim, const float* P, int64_t np, const float* S0
                             float* S_final, double* grad_P, double* grad_S0, int on_device,
                             void* stream)
 {
-    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 2 or 3");
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 1 to 4");
     if (!P || !S0 || !W || !grad_P) return set_err(RD_ERR_ARG, "null argument");
     if (np < 1 || np > INT32_MAX - 1024 || ns < 1 || ns > np)
         return set_err(RD_ERR_ARG, "np/ns out of range");
@@ -1144,7 +1194,7 @@ rd_status rd_batch_run(rd_batch* h, const rd_cloud_desc* clouds, int32_t n_cloud
     std::map<int, std::vector<int>> by_dim;
     for (int c = 0; c < n_clouds; ++c) {
         const rd_cloud_desc& d = clouds[c];
-        if (!dim_ok(d.dim)) return set_err(RD_ERR_UNSUPPORTED, "cloud dim must be 2 or 3");
+        if (!dim_ok(d.dim)) return set_err(RD_ERR_UNSUPPORTED, "cloud dim must be 1 to 4");
         if (d.n < 0 || d.n > INT32_MAX - 1024 || d.offset < 0 ||
             d.offset + d.n * d.dim > total_floats)
             return set_err(RD_ERR_ARG, "cloud out of range");

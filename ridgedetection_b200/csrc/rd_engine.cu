@@ -2,6 +2,8 @@
 #include "rd_engine_host.hpp"
 
 #include <algorithm>
+#include <cmath>
+#include <tuple>
 #include <atomic>
 #include <cstring>
 #include <map>
@@ -14,7 +16,8 @@ namespace rdb {
 // ---------------------------------------------------------------------------
 namespace {
 std::mutex g_tune_mu;
-std::map<std::pair<int, int>, TuneParams> g_tune;
+// (dim, size bucket, r1 bucket) -> shape; r1 bucket TUNE_ANY_R1 = any radius
+std::map<std::tuple<int, int, int>, TuneParams> g_tune;
 }  // namespace
 
 int tune_bucket(int64_t n)
@@ -24,17 +27,45 @@ int tune_bucket(int64_t n)
     return b;
 }
 
-TuneParams tune_lookup(int dim, int64_t n)
+int tune_r1_bucket(float r1)
 {
-    std::lock_guard<std::mutex> lk(g_tune_mu);
-    auto it = g_tune.find({dim, tune_bucket(n)});
-    return (it != g_tune.end()) ? it->second : TuneParams{128, 8};
+    if (!(r1 > 0.0f) || !(r1 < INFINITY)) return TUNE_ANY_R1;
+    const double b = std::floor(2.0 * std::log2((double)r1));   // half octaves
+    return (int)std::max(-256.0, std::min(256.0, b));
 }
 
-void tune_store(int dim, int64_t n, const TuneParams& tp)
+TuneParams tune_lookup(int dim, int64_t n, float r1)
 {
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tune[{dim, tune_bucket(n)}] = tp;
+    const int nb = tune_bucket(n), rb = tune_r1_bucket(r1);
+    auto it = g_tune.find({dim, nb, rb});
+    if (it != g_tune.end()) return it->second;
+    it = g_tune.find({dim, nb, TUNE_ANY_R1});
+    if (it != g_tune.end()) return it->second;
+    // the nearest radius bucket tuned for this dimension and size
+    const TuneParams* best = nullptr;
+    int bd = 1 << 30;
+    for (const auto& kv : g_tune) {
+        if (std::get<0>(kv.first) != dim || std::get<1>(kv.first) != nb) continue;
+        const int d = std::abs(std::get<2>(kv.first) - rb);
+        if (d < bd) { bd = d; best = &kv.second; }
+    }
+    return best ? *best : TuneParams{128, 8, 4};
+}
+
+bool tune_find_exact(int dim, int64_t n, float r1, TuneParams* out)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find({dim, tune_bucket(n), tune_r1_bucket(r1)});
+    if (it == g_tune.end()) return false;
+    *out = it->second;
+    return true;
+}
+
+void tune_store(int dim, int64_t n, float r1, const TuneParams& tp)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[{dim, tune_bucket(n), tune_r1_bucket(r1)}] = tp;
 }
 
 void tune_clear()
@@ -43,10 +74,17 @@ void tune_clear()
     g_tune.clear();
 }
 
-const std::vector<TuneParams>& tune_candidates()
+const std::vector<TuneParams>& tune_candidates(bool culled)
 {
-    static const std::vector<TuneParams> c = {{128, 4}, {128, 8}, {128, 16}, {256, 4}, {256, 8}};
-    return c;
+    static const std::vector<TuneParams> all_pairs = {
+        {128, 4, 4}, {128, 8, 4}, {128, 16, 4}, {256, 4, 4}, {256, 8, 4}};
+    static const std::vector<TuneParams> cull = [] {
+        std::vector<TuneParams> c;
+        for (const TuneParams& s : all_pairs)
+            for (int ci : {2, 4, 8}) c.push_back(TuneParams{s.block, s.items, ci});
+        return c;
+    }();
+    return culled ? cull : all_pairs;
 }
 
 
@@ -142,14 +180,19 @@ static cudaError_t upload(DevBuf& b, const std::vector<T>& h, cudaStream_t st)
 int Engine::setup(int dim, const std::vector<CloudDesc>& clouds,
                   const std::vector<GroupDesc>& groups, int64_t total_points)
 {
-    if (dim != 2 && dim != 3) {
-        last_error = "dim must be 2 or 3";
+    if (!dim_supported(dim)) {
+        last_error = "dim must be 1 to 4";
         return 6;  // RD_ERR_UNSUPPORTED
     }
     if (!tune_locked) {
         int64_t nmax = 1;
-        for (const CloudDesc& cd : clouds) nmax = std::max<int64_t>(nmax, cd.n_all);
-        tune = tune_lookup(dim, nmax);
+        float r1 = 0.0f;
+        for (const CloudDesc& cd : clouds)
+            if (cd.n_all >= nmax) {
+                nmax = std::max<int64_t>(nmax, cd.n_all);
+                r1 = cd.r1;
+            }
+        tune = tune_lookup(dim, nmax, r1);
     }
     if (!tune_supported(dim, tune)) {
         last_error = "unsupported tuning parameters";
@@ -278,6 +321,10 @@ EngineView Engine::view() const
     v.Ps = bPs_.as<float>();
     v.sorder = bSorder_.as<int32_t>();
     v.cull = cull_ ? 1 : 0;
+    v.tile_order = bTileOrder_.as<int32_t>();
+    v.n_heavy = n_heavy_;
+    v.tile_cl_grid = tile_cl_grid_;
+    v.tile_seg_min = tile_seg_min_;
     v.n_sms = sms_;
     v.flags = flags_;
     return v;
@@ -419,6 +466,8 @@ int Engine::run(cudaStream_t st, bool use_graph, int mode)
     RD_CK(upload(bCl_, h_cl_, st));
     RD_CK(upload(bGr_, h_gr_, st));
     RD_CK(upload(bChunkCloud_, h_chunk_cloud_, st));
+    build_tile_order();
+    RD_CK(upload(bTileOrder_, h_tile_order_, st));
     if (mode == RUN_EVOLVE_ONLY || mode == RUN_DECIMATE_ONLY) {
         // chosen sets supplied by the caller (given_ns, points already in S)
         if (given_ns.size() != h_cl_.size()) {
@@ -480,9 +529,10 @@ int Engine::run(cudaStream_t st, bool use_graph, int mode)
         RD_CK(launch_spatial_prep(dim_, vs, total_points_, bSpatialTmp_.p, scratch, bPs_.as<float>(),
                                   bSorder_.as<int32_t>(), st));
     }
+    tile_cl_grid_ = 0;
+    if (fused_) RD_CK(prepare_tile_pass(dim_, view(), &tile_cl_grid_));
     const EngineView v = view();
     RD_CK(prepare_pass(dim_, v, tune));
-    if (fused_) RD_CK(prepare_tile_pass(dim_, v));
     // work lists of the first iteration
     RD_CK(launch_loopcond(v, cudaGraphConditionalHandle(), 0, st, 0));
     if (use_graph) {
@@ -517,6 +567,23 @@ int Engine::run(cudaStream_t st, bool use_graph, int mode)
     return collect(st);
 }
 
+// Tiles (clouds) by decreasing evolve points; the heavy ones (evolved by a
+// whole cluster in fused tiled runs) first.
+void Engine::build_tile_order()
+{
+    const size_t nc = h_cl_.size();
+    h_tile_order_.resize(nc);
+    for (size_t c = 0; c < nc; ++c) h_tile_order_[c] = (int32_t)c;
+    std::stable_sort(h_tile_order_.begin(), h_tile_order_.end(),
+                     [&](int32_t a, int32_t b) { return h_cl_[a].n_all > h_cl_[b].n_all; });
+    n_heavy_ = 0;
+    const TileClusterParams tp = tile_cluster_params();
+    tile_seg_min_ = std::max(1, tp.seg_min);
+    if (tp.enabled && nc > 1)
+        while (n_heavy_ < (int)nc && h_cl_[h_tile_order_[n_heavy_]].n_all >= tp.min_points)
+            ++n_heavy_;
+}
+
 int Engine::plan_workspace(int mode)
 {
     DevArena* a = current_arena();
@@ -528,6 +595,8 @@ int Engine::plan_workspace(int mode)
     RD_CK(upload(bCl_, h_cl_, nullptr));
     RD_CK(upload(bGr_, h_gr_, nullptr));
     RD_CK(upload(bChunkCloud_, h_chunk_cloud_, nullptr));
+    build_tile_order();
+    RD_CK(upload(bTileOrder_, h_tile_order_, nullptr));
     if (mode == RUN_EVOLVE_ONLY || mode == RUN_DECIMATE_ONLY) {
         if (int rc = finish_setup_after_choose(nullptr)) return rc;
         if (mode == RUN_EVOLVE_ONLY && cull_assign && assign_cull_enabled() && spatial_ok_ &&

@@ -55,6 +55,7 @@ enum : int {
     CTR_NACT = 4,      // evolving clouds in the current work lists
     CTR_NREADY = 5,    // groups ready for decimation in this iteration
     CTR_NBIG = 6,      // keys in the big-key list of the current pass
+    CTR_TILE_HEAVY = 7,// heavy-tile ticket of the cluster tile kernel
     CTR_COUNT = 8,
 };
 
@@ -121,6 +122,12 @@ struct EngineView {
     const float* Ps;             // evolve points in spatial order inside each cloud
     const int32_t* sorder;       // spatial position -> packed point slot
     int32_t cull;                // passes assign with k_assign_cull + k_keyhist
+    // fused tiled runs: tiles by decreasing evolve points, the first n_heavy
+    // evolved by whole thread-block clusters (rd_tile_cluster.cuh)
+    const int32_t* tile_order;
+    int32_t n_heavy;
+    int32_t tile_cl_grid;        // CTAs of the cluster tile kernel (0 = one-CTA kernel)
+    int32_t tile_seg_min;        // members of a key the cluster folds in segments
 };
 
 // dynamic shared memory of the decimation kernel: two int16 counts and an
@@ -130,14 +137,27 @@ inline int dec_smem_bytes(const EngineView& v)
     return ((v.dec_smem_max * 5 + 15) / 16) * 16 + 4 * ((v.dec_smem_max + 31) / 32) + 16;
 }
 
-// launch configuration picked by the tuner per (dim, cloud size) bucket
+// launch configuration picked by the tuner per (dim, cloud size, r1) bucket
 struct TuneParams {
-    int block;     // assign CTA size
-    int items;     // points per assign thread
+    int block;          // assign CTA size (all-pairs kernel); with items, the chunk size
+    int items;          // points per assign thread
+    int cull_items = 4; // culled kernel: points per lane (a warp's box holds 32 x this)
 };
 
 // host-side launchers (rd_kernels.cu); all enqueue on `st`
 cudaError_t launch_choose(int dim, const EngineView& v, cudaStream_t st);
+// The cluster path of fused tiled runs (process-wide, read when a run
+// starts): on/off (off = one CTA per tile), the evolve points from which a
+// tile is evolved by a whole cluster and the members from which a key is
+// folded in segments across it.
+struct TileClusterParams {
+    bool enabled;
+    int min_points;
+    int seg_min;
+};
+TileClusterParams tile_cluster_params();
+void set_tile_cluster_params(const TileClusterParams& p);
+TileClusterParams tile_cluster_defaults();
 // choose of one large cloud c (n own points) in GPU-wide rounds; v.hash must
 // hold choose_hash_buckets() ints and surv n bytes
 cudaError_t launch_choose_rounds(int dim, const EngineView& v, int c, int n, uint8_t* surv,
@@ -156,7 +176,7 @@ cudaError_t launch_reset(const EngineView& v, cudaStream_t st);
 cudaError_t launch_set_given(const EngineView& v, int queue_decimation, cudaStream_t st);
 // fused per-tile evolve (every active cloud to convergence, one CTA each) +
 // decimation of the groups that became ready; needs every ns <= TILE_NS_MAX
-cudaError_t prepare_tile_pass(int dim, const EngineView& v);
+cudaError_t prepare_tile_pass(int dim, const EngineView& v, int* cl_grid);
 // a0/a1 (optional) are recorded right before and after the tile-evolve kernel
 cudaError_t launch_tile_pass(int dim, const EngineView& v, cudaStream_t st,
                              cudaEvent_t a0 = nullptr, cudaEvent_t a1 = nullptr);

@@ -56,15 +56,23 @@ struct RunStats {
     double point_passes = 0;      // sum over clouds of n_all * evolve passes
 };
 
-// Process-wide tuning table: (dim, size bucket) -> assign launch shape.  The
-// bucket of a cloud of n points is floor(log2(n)); entries come from
-// rd_autotune (measured) or rd_tune_set (given).  Thread-safe.
+// Process-wide tuning table: (dim, size bucket, r1 bucket) -> assignment
+// launch shape.  The size bucket of a cloud of n points is floor(log2(n)), the
+// r1 bucket floor(2 log2(r1)) (half octaves; TUNE_ANY_R1 = an entry for every
+// radius).  A lookup takes the exact bucket, else the any-radius entry, else
+// the nearest radius bucket of the same dim and size, else the default.
+// Entries come from rd_autotune (measured) or rd_tune_set (given).
+// Thread-safe.
+constexpr int TUNE_ANY_R1 = -100000;
 int tune_bucket(int64_t n);
-TuneParams tune_lookup(int dim, int64_t n);
-void tune_store(int dim, int64_t n, const TuneParams& tp);
+int tune_r1_bucket(float r1);
+TuneParams tune_lookup(int dim, int64_t n, float r1);
+bool tune_find_exact(int dim, int64_t n, float r1, TuneParams* out);
+void tune_store(int dim, int64_t n, float r1, const TuneParams& tp);
 void tune_clear();
-// supported launch shapes, in a fixed order
-const std::vector<TuneParams>& tune_candidates();
+// supported launch shapes, in a fixed order (culled = the culled kernel's
+// candidates: every chunk shape with every box size)
+const std::vector<TuneParams>& tune_candidates(bool culled);
 // Process-wide switch of the exact chunk-box culling of the assignment (on by
 // default); read by every engine run.  Thread-safe.
 void set_assign_cull(bool on);
@@ -133,6 +141,7 @@ public:
 
 private:
     int finish_setup_after_choose(cudaStream_t st);
+    void build_tile_order();
     int collect(cudaStream_t st);
     int flags_ = 0;
     int build_graph(cudaStream_t st);
@@ -164,6 +173,11 @@ private:
     bool cull_ = false;           // this run assigns with culling
     bool spatial_ok_ = false;     // the batch layout allows the spatial order
     DevBuf bPs_, bSorder_, bSpatialTmp_;
+    DevBuf bTileOrder_;
+    std::vector<int32_t> h_tile_order_;
+    int n_heavy_ = 0;
+    int tile_cl_grid_ = 0;
+    int tile_seg_min_ = 1 << 30;
     DevBuf bDx_, bDcell_, bDalive_, bDc1_, bDc2_, bDbstart_, bDitems_, bDecHoff_, bDecHbits_;
 
     cudaStream_t cap_stream_ = nullptr;

@@ -235,6 +235,110 @@ __device__ __forceinline__ void dec_for_neighbours(const int i, const float* X,
     }
 }
 
+// Passes of the in-order decimation, resolved in parallel rounds (exact).
+// In one pass the reference visits the alive points in order and removes
+// point i when, at that moment, c1 >= 4 or c2 < 3 (alive points within r2 /
+// 2*r2, self included); a removal lowers the counts of its neighbours.  At
+// i's turn only its EARLIER neighbours can have been removed in this pass, and
+// counts only fall, so with rem = earlier neighbours known removed and und =
+// earlier neighbours still undecided:
+//   c1 at i's turn lies in [c1 - rem1 - und1, c1 - rem1], c2 likewise;
+//   i is surely removed when c1 - rem1 - und1 >= 4 or c2 - rem2 < 3,
+//   surely kept when c1 - rem1 < 4 and c2 - rem2 - und2 >= 3.
+// Rounds decide every point they can until none is undecided; the lowest
+// undecided point always has und = 0, so each round decides at least one.
+// The reference also stops removing once fewer than 3 points would remain
+// (decimate.hpp:62-80 breaks the pass, decimateNoCopy keeps the point); a pass
+// whose removals leave at least 3 points never meets that rule, and a pass
+// that would leave fewer is not applied: *fallback is set and the caller
+// finishes with the sequential scan from the state before that pass.
+// State per point st[i]: 0 dead, 1 alive (undecided in a pass), 2 kept in
+// this pass, 3 removed in this pass; counts c1/c2 of alive points are exact
+// between passes.  Returns the alive count.  All threads of the block call it.
+template <int BLOCK, class CT, class ST>
+__device__ int decimate_round_passes(const int total, int cnt, CT* c1, CT* c2, ST* st_,
+                                     const int32_t* nb_off, const int32_t* nb, int* fallback,
+                                     int32_t* err)
+{
+    volatile ST* st = st_;
+    const int tid = threadIdx.x;
+    *fallback = 0;
+    int guard = 0;
+    while (cnt > 3) {
+        if (++guard > total + 2) {
+            if (tid == 0) atomicOr(err, ERRB_DEC_CAP);
+            break;
+        }
+        // one pass, in rounds
+        for (int round = 0;; ++round) {
+            int und_left = 0;
+            for (int i = tid; i < total; i += BLOCK) {
+                if (st[i] != 1) continue;
+                int rem1 = 0, und1 = 0, rem2 = 0, und2 = 0;
+                const int e1 = nb_off[i + 1];
+                for (int t = nb_off[i]; t < e1; ++t) {
+                    const int e = nb[t];
+                    const int q = e & 0x7fffffff;
+                    if (q >= i) continue;
+                    const int sq = st[q];
+                    const int w1 = (e < 0) ? 1 : 0;
+                    rem2 += (sq == 3);
+                    rem1 += (sq == 3) & w1;
+                    und2 += (sq == 1);
+                    und1 += (sq == 1) & w1;
+                }
+                const int a = (int)c1[i] - rem1, b = (int)c2[i] - rem2;
+                if (a - und1 >= 4 || b < 3) st[i] = 3;
+                else if (a < 4 && b - und2 >= 3) st[i] = 2;
+                else und_left = 1;
+            }
+            if (!__syncthreads_or(und_left)) break;
+            if (round > total) {   // cannot happen: every round decides a point
+                if (tid == 0) atomicOr(err, ERRB_DEC_CAP);
+                break;
+            }
+        }
+        __shared__ int s_removed;
+        if (tid == 0) s_removed = 0;
+        __syncthreads();
+        int mine = 0;
+        for (int i = tid; i < total; i += BLOCK) mine += (st[i] == 3);
+        if (mine) atomicAdd(&s_removed, mine);
+        __syncthreads();
+        const int removed = s_removed;
+        const bool apply = removed > 0 && cnt - removed >= 3;
+        for (int i = tid; i < total; i += BLOCK) {
+            const int v = st[i];
+            if (v == 3) st[i] = apply ? 0 : 1;
+            else if (v == 2) st[i] = 1;
+        }
+        __syncthreads();
+        if (removed == 0) break;            // a pass that changed nothing ends the loop
+        if (!apply) {                       // the minimum-count rule may act
+            *fallback = 1;
+            break;
+        }
+        cnt -= removed;
+        // exact counts of the alive points for the next pass
+        for (int i = tid; i < total; i += BLOCK) {
+            if (st[i] != 1) continue;
+            int n1 = 1, n2 = 1;
+            const int e1 = nb_off[i + 1];
+            for (int t = nb_off[i]; t < e1; ++t) {
+                const int e = nb[t];
+                if (st[e & 0x7fffffff] == 1) {
+                    ++n2;
+                    n1 += (e < 0) ? 1 : 0;
+                }
+            }
+            c1[i] = (CT)n1;
+            c2[i] = (CT)n2;
+        }
+        __syncthreads();
+    }
+    return cnt;
+}
+
 // Same decimation as decimate_scan, faster for large sets: every point's
 // neighbours within 2*r2 are listed once (CSR in nb_off/nb, the sign bit
 // marking "also within r2"), so a removal decrements its neighbours' counts
@@ -370,6 +474,23 @@ __device__ void decimate_scan_lists(const float* X, const int total, const float
     }
     __syncthreads();
     }
+    // passes in parallel rounds while the minimum-count rule cannot act
+    __shared__ int s_alive, s_fallback;
+    {
+        int fb = 0;
+        const int left = in_smem
+            ? decimate_round_passes<BLOCK>(total, total, c1s, c2s, as, nb_off, nb, &fb, err)
+            : decimate_round_passes<BLOCK>(total, total, c1g, c2g, alive, nb_off, nb, &fb, err);
+        if (tid == 0) {
+            s_alive = left;
+            s_fallback = fb;
+        }
+        __syncthreads();
+        if (in_smem)
+            for (int i = tid; i < total; i += BLOCK) alive[i] = as[i];
+        __syncthreads();
+        if (!s_fallback) return;
+    }
     if (in_smem) {
         // Candidate bitmap: bit i set <=> point i is alive and removable now.
         // The in-order scan then jumps from candidate to candidate; a removal
@@ -379,7 +500,7 @@ __device__ void decimate_scan_lists(const float* X, const int total, const float
         const int nwords = (total + 31) >> 5;
         for (int i0 = 0; i0 < nwords * 32; i0 += BLOCK) {
             const int i = i0 + tid;
-            const bool q = (i < total) && (c1s[i] >= 4 || c2s[i] < 3);
+            const bool q = (i < total) && as[i] && (c1s[i] >= 4 || c2s[i] < 3);
             const unsigned bal = __ballot_sync(FULL, q);
             if (lane == 0 && (i >> 5) < nwords) cand[i >> 5] = bal;
         }
@@ -420,7 +541,7 @@ __device__ void decimate_scan_lists(const float* X, const int total, const float
                 }
                 return -1;
             };
-            int cnt = total, left = -1, guard = 0;
+            int cnt = s_alive, left = -1, guard = 0;
             bool stop = false;
             while (left != cnt && cnt > 3 && !stop) {
                 if (++guard > total + 2) { if (lane == 0) atomicOr(err, ERRB_DEC_CAP); break; }
@@ -476,7 +597,7 @@ __device__ void decimate_scan_lists(const float* X, const int total, const float
             const int b = in_smem ? c2s[w] : c2g[w];
             return a >= 4 || b < 3;
         };
-        int cnt = total, left = -1, guard = 0;
+        int cnt = s_alive, left = -1, guard = 0;
         bool stop = false;
         while (left != cnt && cnt > 3 && !stop) {
             if (++guard > total + 2) { if (lane == 0) atomicOr(err, ERRB_DEC_CAP); break; }

@@ -18,8 +18,28 @@
 #include <cfloat>
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <type_traits>
 
 namespace rdb {
+
+// Point dimensions built into the kernels: 1 to RD_MAX_DIM (the reference's
+// CPU path takes the dimension at run time, its GPU classes as a template
+// argument).  with_dim calls f(std::integral_constant<int, DIM>) for a
+// supported dim and returns cudaErrorInvalidValue otherwise.
+constexpr int RD_MAX_DIM = 4;
+__host__ __device__ constexpr bool dim_supported(int dim) { return dim >= 1 && dim <= RD_MAX_DIM; }
+
+template <class F>
+inline cudaError_t with_dim(int dim, F&& f)
+{
+    switch (dim) {
+        case 1: return f(std::integral_constant<int, 1>{});
+        case 2: return f(std::integral_constant<int, 2>{});
+        case 3: return f(std::integral_constant<int, 3>{});
+        case 4: return f(std::integral_constant<int, 4>{});
+        default: return cudaErrorInvalidValue;
+    }
+}
 
 // ---------------------------------------------------------------------------
 // error bits recorded on the device (per cloud and globally); the host turns

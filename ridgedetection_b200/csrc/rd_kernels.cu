@@ -10,8 +10,13 @@
 #include "rd_engine.cuh"
 #include "rd_grid.cuh"
 #include "rd_fold.cuh"
+#include "rd_segfold.cuh"
 
 #include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstring>
 
 namespace rdb {
 
@@ -514,8 +519,9 @@ __global__ void __launch_bounds__(BLOCK) k_assign(EngineView v)
 // then builds the per-chunk histograms in slot order.
 // ---------------------------------------------------------------------------
 constexpr int AC_BLOCK = 256;  // threads of k_assign_cull
-constexpr int AC_ITEMS = 4;    // points per lane per step (a warp: 128 consecutive points)
 constexpr int AC_TS = 1024;    // chosen points per shared-memory batch
+// points per lane per step (ITEMS, a tuning parameter): a warp's box holds 32 x
+// ITEMS consecutive points of the spatial order
 
 // squared gap between s and the box [lo, hi] (0 inside; NaN-free for NaN s)
 template <int DIM>
@@ -530,9 +536,10 @@ __device__ __forceinline__ float box_gap2(const float* s, const float* lo, const
     return g2;
 }
 
-template <int DIM>
+template <int DIM, int AC_ITEMS>
 __global__ void __launch_bounds__(AC_BLOCK) k_assign_cull(EngineView v)
 {
+    static_assert(AC_ITEMS % 2 == 0, "points are evaluated in pairs");
     constexpr int DP = PadDim<DIM>::v;
     constexpr int WPTS = 32 * AC_ITEMS;
     __shared__ __align__(16) float sS[AC_TS * DP];
@@ -558,7 +565,7 @@ __global__ void __launch_bounds__(AC_BLOCK) k_assign_cull(EngineView v)
         const bool may_skip = rsq >= 1.0e-30f && rsq <= 1.0e30f;
         const float thr = __fmul_ru(rsq, 1.0009765625f);
         for (int b0 = start; b0 < end; b0 += AC_BLOCK * AC_ITEMS) {
-            // this warp's points: b0 + warp*128 + j*32 + lane, and their box
+            // this warp's points: b0 + warp*WPTS + j*32 + lane, and their box
             float p[AC_ITEMS][DIM];
             float2 np2[AC_ITEMS / 2][DIM];
             float best[AC_ITEMS];
@@ -1191,25 +1198,165 @@ __device__ void sum_shift_big_one(const EngineView& v, int slot, float (*s_x)[SB
 // Shared memory: chosen points (TILE_NS_MAX, padded to float4 for DIM 3),
 // W x (ns+1) counters, key bases.
 // ---------------------------------------------------------------------------
+// Assignment of the points [r0, r1w) of a tile by one warp (steps of 32 x
+// TILE_PPL points, loads first): keys[i] = nearest chosen point within r1
+// (first index of the minimum), and the warp's members per key in whist.
+// With at most TILE_KB chosen points the counts are kept per key in
+// warp-uniform registers (one ballot per key and step) and stored at the end;
+// otherwise one shared-memory add per distinct key of a step.
+constexpr int TILE_KB = 8;
+
+template <int DIM>
+__device__ __forceinline__ void tile_assign_range(const float* __restrict__ P, const int r0,
+                                                  const int r1w, const float* sS, const int ns,
+                                                  const int nsp, const float rsq,
+                                                  int32_t* __restrict__ keys, int* whist,
+                                                  const int lane)
+{
+    constexpr int KB = TILE_KB;
+    int kc[KB];
+#pragma unroll
+    for (int k = 0; k < KB; ++k) kc[k] = 0;
+    for (int i0 = r0; i0 < r1w; i0 += 32 * TILE_PPL) {
+        float p[TILE_PPL][DIM];
+#pragma unroll
+        for (int h = 0; h < TILE_PPL; ++h) {
+            const int i = i0 + h * 32 + lane;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) p[h][d] = (i < r1w) ? P[(int64_t)i * DIM + d] : 0.0f;
+        }
+#pragma unroll
+        for (int h = 0; h < TILE_PPL; ++h) {
+            const int i = i0 + h * 32 + lane;
+            int key = -1;
+            if (i < r1w) {
+                if (ns <= KB) {
+                    // first index of the minimum, directly
+                    float best = FLT_MAX;
+                    int bk = -1;
+                    for (int k = 0; k < ns; ++k) {
+                        float s[DIM];
+                        load_chosen<DIM>(sS, k, s);
+                        const float dd = sqdist_exact<DIM>(s, p[h]);
+                        if (dd < best) { best = dd; bk = k; }
+                    }
+                    key = (best <= rsq) ? bk : -1;
+                } else {
+                    float best = FLT_MAX;
+                    int blk = -1;
+                    for (int kb = 0; kb < nsp; kb += KB) {
+                        const float old = best;
+#pragma unroll
+                        for (int u = 0; u < KB; ++u) {
+                            float s[DIM];
+                            load_chosen<DIM>(sS, kb + u, s);
+                            best = fminf(best, sqdist_exact<DIM>(s, p[h]));
+                        }
+                        blk = (best < old) ? kb : blk;
+                    }
+                    if (best <= rsq && blk >= 0) {
+                        for (int u = 0; u < KB && blk + u < ns; ++u) {
+                            float s[DIM];
+                            load_chosen<DIM>(sS, blk + u, s);
+                            if (sqdist_exact<DIM>(s, p[h]) == best) { key = blk + u; break; }
+                        }
+                    }
+                }
+                keys[i] = key;
+            }
+            if (ns <= KB) {
+#pragma unroll
+                for (int k = 0; k < KB; ++k)
+                    if (k < ns) kc[k] += __popc(__ballot_sync(FULL, key == k));
+            } else {
+                // a tile's warp step holds few distinct keys: the match
+                // instruction is cheap there (warp_runs suits many keys)
+                const unsigned mm = __match_any_sync(FULL, key);
+                if (key >= 0 && lane == __ffs(mm) - 1) atomicAdd(&whist[key], __popc(mm));
+            }
+        }
+    }
+    if (ns <= KB && lane == 0)
+#pragma unroll
+        for (int k = 0; k < KB; ++k)
+            if (k < ns) whist[k] += kc[k];
+}
+
+// Stable placement of the warp's points [r0, r1w) into perm: the members of
+// key k go, in index order, to cur[k], cur[k] + 1, ... (cur advanced).
+template <int DIM>
+__device__ __forceinline__ void tile_place_range(const int32_t* __restrict__ keys, const int r0,
+                                                 const int r1w, int* cur, const int ns,
+                                                 int32_t* __restrict__ perm, const int lane)
+{
+    constexpr int KB = TILE_KB;
+    int base[KB];
+    if (ns <= KB) {
+#pragma unroll
+        for (int k = 0; k < KB; ++k) base[k] = (k < ns) ? cur[k] : 0;
+    }
+    for (int i0 = r0; i0 < r1w; i0 += 32 * TILE_PPL) {
+        int kq[TILE_PPL];
+#pragma unroll
+        for (int h = 0; h < TILE_PPL; ++h) {
+            const int i = i0 + h * 32 + lane;
+            kq[h] = (i < r1w) ? keys[i] : -1;
+        }
+#pragma unroll
+        for (int h = 0; h < TILE_PPL; ++h) {
+            const int key = kq[h];
+            const int i = i0 + h * 32 + lane;
+            if (ns <= KB) {
+#pragma unroll
+                for (int k = 0; k < KB; ++k) {
+                    if (k < ns) {
+                        const unsigned m = __ballot_sync(FULL, key == k);
+                        if (key == k) perm[base[k] + __popc(m & lanemask_lt())] = i;
+                        base[k] += __popc(m);
+                    }
+                }
+            } else {
+                const unsigned m = __match_any_sync(FULL, key);
+                const int leader = __ffs(m) - 1;
+                int b = 0;
+                if (key >= 0 && lane == leader) {
+                    b = cur[key];
+                    cur[key] = b + __popc(m);
+                }
+                b = __shfl_sync(FULL, b, leader);
+                if (key >= 0) perm[b + __popc(m & lanemask_lt())] = i;
+            }
+        }
+    }
+}
+
 template <int DIM, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_tile_evolve(EngineView v)
+struct TileCtaSmem {
+    float buf[BLOCK / 32][SUM_BP * DIM];
+    int idx[BLOCK / 32][SUM_BP];
+    int moved;
+    SegFoldSmem<BLOCK / 32, DIM> seg;
+};
+
+// One CTA evolves tile c to convergence (see above); dyn is the dynamic
+// shared memory laid out as tile_evolve_smem_bytes describes.
+template <int DIM, int BLOCK>
+__device__ void tile_evolve_one(const EngineView& v, const int c, unsigned char* dyn,
+                                TileCtaSmem<DIM, BLOCK>& ts)
 {
     constexpr int W = BLOCK / 32;
     constexpr int DP = PadDim<DIM>::v;
     constexpr int KB = 8;
     constexpr float FAR = 1e30f;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    float* sS = reinterpret_cast<float*>(smem_raw);                         // TILE_NS_MAX*DP
+    float* sS = reinterpret_cast<float*>(dyn);                              // TILE_NS_MAX*DP
     int* hist = reinterpret_cast<int*>(sS + TILE_NS_MAX * DP);             // W*(TILE_NS_MAX+1)
     int* kbase = hist + W * (TILE_NS_MAX + 1);                              // TILE_NS_MAX+1
-    __shared__ float s_buf[W][SUM_BP * DIM];
-    __shared__ int s_idx[W][SUM_BP];
-    __shared__ int s_moved;
-    __shared__ FoldCtaSmem<W, DIM> s_fold;
+    auto& s_buf = ts.buf;
+    auto& s_idx = ts.idx;
+    int& s_moved = ts.moved;
+    auto& s_seg = ts.seg;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int nact = v.ctr[CTR_NACT];
-    for (int a = blockIdx.x; a < nact; a += gridDim.x) {
-        const int c = v.act_cloud[a];
+    {
         const CloudDesc cd = v.cl[c];
         const int n = cd.n_all;
         const int ns = v.ns[c];
@@ -1231,59 +1378,7 @@ __global__ void __launch_bounds__(BLOCK) k_tile_evolve(EngineView v)
             for (int k = lane; k <= ns; k += 32) hist[warp * (TILE_NS_MAX + 1) + k] = 0;
             __syncthreads();
             int* whist = hist + warp * (TILE_NS_MAX + 1);
-            for (int i0 = r0; i0 < r1w; i0 += 32 * TILE_PPL) {
-                float p[TILE_PPL][DIM];
-#pragma unroll
-                for (int h = 0; h < TILE_PPL; ++h) {
-                    const int i = i0 + h * 32 + lane;
-#pragma unroll
-                    for (int d = 0; d < DIM; ++d) p[h][d] = (i < r1w) ? P[(int64_t)i * DIM + d] : 0.0f;
-                }
-#pragma unroll
-                for (int h = 0; h < TILE_PPL; ++h) {
-                    const int i = i0 + h * 32 + lane;
-                    int key = -1;
-                    if (i < r1w) {
-                        if (ns <= KB) {
-                            // first index of the minimum, directly
-                            float best = FLT_MAX;
-                            int bk = -1;
-                            for (int k = 0; k < ns; ++k) {
-                                float s[DIM];
-                                load_chosen<DIM>(sS, k, s);
-                                const float dd = sqdist_exact<DIM>(s, p[h]);
-                                if (dd < best) { best = dd; bk = k; }
-                            }
-                            key = (best <= rsq) ? bk : -1;
-                        } else {
-                            float best = FLT_MAX;
-                            int blk = -1;
-                            for (int kb = 0; kb < nsp; kb += KB) {
-                                const float old = best;
-#pragma unroll
-                                for (int u = 0; u < KB; ++u) {
-                                    float s[DIM];
-                                    load_chosen<DIM>(sS, kb + u, s);
-                                    best = fminf(best, sqdist_exact<DIM>(s, p[h]));
-                                }
-                                blk = (best < old) ? kb : blk;
-                            }
-                            if (best <= rsq && blk >= 0) {
-                                for (int u = 0; u < KB && blk + u < ns; ++u) {
-                                    float s[DIM];
-                                    load_chosen<DIM>(sS, blk + u, s);
-                                    if (sqdist_exact<DIM>(s, p[h]) == best) { key = blk + u; break; }
-                                }
-                            }
-                        }
-                        keys[i] = key;
-                    }
-                    // a tile's warp step holds few distinct keys: the match
-                    // instruction is cheap there (warp_runs suits many keys)
-                    const unsigned mm = __match_any_sync(FULL, key);
-                    if (key >= 0 && lane == __ffs(mm) - 1) atomicAdd(&whist[key], __popc(mm));
-                }
-            }
+            tile_assign_range<DIM>(P, r0, r1w, sS, ns, nsp, rsq, keys, whist, lane);
             __syncthreads();
             // 2. key bases and per-warp starts (thread per key)
             for (int k = tid; k < ns; k += BLOCK) {
@@ -1321,37 +1416,16 @@ __global__ void __launch_bounds__(BLOCK) k_tile_evolve(EngineView v)
             // 3. stable placement, warp range by warp range (keys of
             //    TILE_PPL warp steps loaded ahead of the dependent placement
             //    chain)
-            int* cur = hist + warp * (TILE_NS_MAX + 1);
-            for (int i0 = r0; i0 < r1w; i0 += 32 * TILE_PPL) {
-                int kq[TILE_PPL];
-#pragma unroll
-                for (int h = 0; h < TILE_PPL; ++h) {
-                    const int i = i0 + h * 32 + lane;
-                    kq[h] = (i < r1w) ? keys[i] : -1;
-                }
-#pragma unroll
-                for (int h = 0; h < TILE_PPL; ++h) {
-                    const int key = kq[h];
-                    const unsigned m = __match_any_sync(FULL, key);
-                    const int leader = __ffs(m) - 1;
-                    int b = 0;
-                    if (key >= 0 && lane == leader) {
-                        b = cur[key];
-                        cur[key] = b + __popc(m);
-                    }
-                    b = __shfl_sync(FULL, b, leader);
-                    if (key >= 0) perm[b + __popc(m & lanemask_lt())] = i0 + h * 32 + lane;
-                }
-            }
+            tile_place_range<DIM>(keys, r0, r1w, hist + warp * (TILE_NS_MAX + 1), ns, perm, lane);
             __syncthreads();
             // 4a. very large keys, one at a time, folded by the whole CTA
             for (int k = 0; k < ns; ++k) {
                 const int cnt = kbase[k + 1] - kbase[k];
                 if (cnt < FOLD_CTA_MIN) continue;
-                fold_members_cta<W, DIM>(perm + kbase[k], cnt, P, s_fold);
+                fold_members_seg<W, DIM>(perm + kbase[k], cnt, P, s_seg);
                 if (tid < DIM) {
                     float cval = sS[k * DP + tid];
-                    if (shift_coord(s_fold.s[tid], cnt, cval)) {
+                    if (shift_coord(s_seg.out[tid], cnt, cval)) {
                         sS[k * DP + tid] = cval;
                         s_moved = 1;
                     }
@@ -1398,12 +1472,27 @@ __global__ void __launch_bounds__(BLOCK) k_tile_evolve(EngineView v)
     }
 }
 
-int tile_evolve_smem_bytes(int dim)
+template <int DIM, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_tile_evolve(EngineView v)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ TileCtaSmem<DIM, BLOCK> ts;
+    const int nact = v.ctr[CTR_NACT];
+    for (int a = blockIdx.x; a < nact; a += gridDim.x) tile_evolve_one<DIM, BLOCK>(v, v.act_cloud[a], smem_raw, ts);
+}
+
+__host__ __device__ constexpr int tile_evolve_smem_bytes(int dim)
 {
     const int dp = (dim == 3) ? 4 : dim;
     const int w = 8;
     return TILE_NS_MAX * dp * 4 + w * (TILE_NS_MAX + 1) * 4 + (TILE_NS_MAX + 1) * 4;
 }
+
+}  // namespace
+}  // namespace rdb
+#include "rd_tile_cluster.cuh"
+namespace rdb {
+namespace {
 
 // ---------------------------------------------------------------------------
 // control: one thread per cloud after each pass.
@@ -1866,6 +1955,7 @@ __global__ void __launch_bounds__(1024) k_loopcond(EngineView v, cudaGraphCondit
         v.ctr[CTR_WORK] = 0;
         v.ctr[CTR_NREADY] = 0;
         v.ctr[CTR_NBIG] = 0;
+        v.ctr[CTR_TILE_HEAVY] = 0;
         const int it = v.ctr[CTR_ITERS] + (count_iter ? 1 : 0);
         v.ctr[CTR_ITERS] = it;
         int a = s_act;
@@ -1944,7 +2034,10 @@ cudaError_t launch_pass_dim(const EngineView& v, const TuneParams& tp, int assig
     const int sms = v.n_sms;
     if (a0) cudaEventRecord(a0, st);
     if (v.cull) {
-        k_assign_cull<DIM><<<std::max(1, std::min(v.n_chunks, sms * 8)), AC_BLOCK, 0, st>>>(v);
+        const int g = std::max(1, std::min(v.n_chunks, sms * 8));
+        if (tp.cull_items == 2) k_assign_cull<DIM, 2><<<g, AC_BLOCK, 0, st>>>(v);
+        else if (tp.cull_items == 8) k_assign_cull<DIM, 8><<<g, AC_BLOCK, 0, st>>>(v);
+        else k_assign_cull<DIM, 4><<<g, AC_BLOCK, 0, st>>>(v);
     } else {
 #define RD_ASSIGN_CASE(B, I)                                                                  \
     if (tp.block == B && tp.items == I) {                                                     \
@@ -2027,41 +2120,29 @@ cudaError_t launch_choose_rounds_dim(const EngineView& v, int c, int n, uint8_t*
 cudaError_t launch_choose_rounds(int dim, const EngineView& v, int c, int n, uint8_t* surv,
                                  cudaStream_t st)
 {
-    switch (dim) {
-        case 2: return launch_choose_rounds_dim<2>(v, c, n, surv, st);
-        case 3: return launch_choose_rounds_dim<3>(v, c, n, surv, st);
-        default: return cudaErrorInvalidValue;
-    }
+    return with_dim(dim, [&](auto D) {
+        return launch_choose_rounds_dim<decltype(D)::value>(v, c, n, surv, st);
+    });
 }
 
 int choose_hash_buckets() { return ChooseSmem<2>::HB; }
 
 cudaError_t launch_choose(int dim, const EngineView& v, cudaStream_t st)
 {
-    switch (dim) {
-        case 2: return launch_choose_dim<2>(v, st);
-        case 3: return launch_choose_dim<3>(v, st);
-        default: return cudaErrorInvalidValue;
-    }
+    return with_dim(dim, [&](auto D) { return launch_choose_dim<decltype(D)::value>(v, st); });
 }
 
 cudaError_t prepare_pass(int dim, const EngineView& v, const TuneParams& tp)
 {
-    switch (dim) {
-        case 2: return prepare_pass_dim<2>(v, tp);
-        case 3: return prepare_pass_dim<3>(v, tp);
-        default: return cudaErrorInvalidValue;
-    }
+    return with_dim(dim, [&](auto D) { return prepare_pass_dim<decltype(D)::value>(v, tp); });
 }
 
 cudaError_t launch_pass(int dim, const EngineView& v, const TuneParams& tp, int assign_grid,
                         cudaStream_t st, cudaEvent_t a0, cudaEvent_t a1)
 {
-    switch (dim) {
-        case 2: return launch_pass_dim<2>(v, tp, assign_grid, st, a0, a1);
-        case 3: return launch_pass_dim<3>(v, tp, assign_grid, st, a0, a1);
-        default: return cudaErrorInvalidValue;
-    }
+    return with_dim(dim, [&](auto D) {
+        return launch_pass_dim<decltype(D)::value>(v, tp, assign_grid, st, a0, a1);
+    });
 }
 
 cudaError_t launch_loopcond(const EngineView& v, cudaGraphConditionalHandle h, int use_handle,
@@ -2071,16 +2152,69 @@ cudaError_t launch_loopcond(const EngineView& v, cudaGraphConditionalHandle h, i
     return cudaGetLastError();
 }
 
-cudaError_t prepare_tile_pass(int dim, const EngineView& v)
+static std::atomic<int> g_tile_cl_on{1}, g_tile_cl_min{TCL_MIN_POINTS}, g_tile_seg_min{TSEG_MIN};
+TileClusterParams tile_cluster_defaults() { return TileClusterParams{true, TCL_MIN_POINTS, TSEG_MIN}; }
+TileClusterParams tile_cluster_params()
 {
-    const int smem = tile_evolve_smem_bytes(dim);
-    cudaError_t e = cudaSuccess;
-    if (dim == 2) e = cudaFuncSetAttribute(k_tile_evolve<2, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    else if (dim == 3) e = cudaFuncSetAttribute(k_tile_evolve<3, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    else return cudaErrorInvalidValue;
+    return TileClusterParams{g_tile_cl_on.load() != 0, g_tile_cl_min.load(), g_tile_seg_min.load()};
+}
+void set_tile_cluster_params(const TileClusterParams& p)
+{
+    g_tile_cl_on.store(p.enabled ? 1 : 0);
+    g_tile_cl_min.store(p.min_points);
+    g_tile_seg_min.store(p.seg_min);
+}
+
+// launch configuration of the cluster tile kernel: one CTA per resident slot
+// (TCL-CTA clusters), dynamic shared memory as tile_cluster_smem_bytes
+template <int DIM>
+static void tile_cl_config(cudaLaunchConfig_t& cfg, cudaLaunchAttribute* at, int grid)
+{
+    std::memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3(grid, 1, 1);
+    cfg.blockDim = dim3(256, 1, 1);
+    cfg.dynamicSmemBytes = tile_cluster_smem_bytes(DIM);
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = TCL;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+}
+
+template <int DIM>
+static cudaError_t tile_cl_prepare(int* cl_grid)
+{
+    cudaError_t e = cudaFuncSetAttribute(k_tile_evolve_cl<DIM, 256>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         tile_cluster_smem_bytes(DIM));
     if (e != cudaSuccess) return e;
-    if (dim == 2) return cudaFuncSetAttribute(k_decimate<2, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, dec_smem_bytes(v));
-    return cudaFuncSetAttribute(k_decimate<3, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, dec_smem_bytes(v));
+    cudaLaunchConfig_t cfg;
+    cudaLaunchAttribute at[1];
+    tile_cl_config<DIM>(cfg, at, TCL);
+    int ncl = 0;
+    e = cudaOccupancyMaxActiveClusters(&ncl, k_tile_evolve_cl<DIM, 256>, &cfg);
+    if (e != cudaSuccess) return e;
+    *cl_grid = (ncl > 0) ? ncl * TCL : 0;
+    return cudaSuccess;
+}
+
+cudaError_t prepare_tile_pass(int dim, const EngineView& v, int* cl_grid)
+{
+    *cl_grid = 0;
+    return with_dim(dim, [&](auto D) {
+        constexpr int DIM = decltype(D)::value;
+        cudaError_t e = cudaFuncSetAttribute(k_tile_evolve<DIM, 256>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             tile_evolve_smem_bytes(DIM));
+        if (e != cudaSuccess) return e;
+        if (v.n_heavy > 0) {
+            e = tile_cl_prepare<DIM>(cl_grid);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaFuncSetAttribute(k_decimate<DIM, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    dec_smem_bytes(v));
+    });
 }
 
 cudaError_t launch_tile_pass(int dim, const EngineView& v, cudaStream_t st, cudaEvent_t a0,
@@ -2089,22 +2223,24 @@ cudaError_t launch_tile_pass(int dim, const EngineView& v, cudaStream_t st, cuda
     const int smem = tile_evolve_smem_bytes(dim);
     const int grid = std::max(1, std::min(v.n_clouds, v.n_sms * 3));
     const int dgrid = std::max(1, std::min(v.n_groups, v.n_sms * 2));
-    if (dim == 2) {
+    return with_dim(dim, [&](auto D) {
+        constexpr int DIM = decltype(D)::value;
         if (a0) cudaEventRecord(a0, st);
-        k_tile_evolve<2, 256><<<grid, 256, smem, st>>>(v);
+        if (v.tile_cl_grid > 0) {
+            cudaLaunchConfig_t cfg;
+            cudaLaunchAttribute at[1];
+            tile_cl_config<DIM>(cfg, at, v.tile_cl_grid);
+            cfg.stream = st;
+            const cudaError_t e = cudaLaunchKernelEx(&cfg, k_tile_evolve_cl<DIM, 256>, v);
+            if (e != cudaSuccess) return e;
+        } else {
+            k_tile_evolve<DIM, 256><<<grid, 256, smem, st>>>(v);
+        }
         if (a1) cudaEventRecord(a1, st);
-        launch_decbig<2>(v, st);
-        k_decimate<2, 512><<<dgrid, 512, dec_smem_bytes(v), st>>>(v);
-    } else if (dim == 3) {
-        if (a0) cudaEventRecord(a0, st);
-        k_tile_evolve<3, 256><<<grid, 256, smem, st>>>(v);
-        if (a1) cudaEventRecord(a1, st);
-        launch_decbig<3>(v, st);
-        k_decimate<3, 512><<<dgrid, 512, dec_smem_bytes(v), st>>>(v);
-    } else {
-        return cudaErrorInvalidValue;
-    }
-    return cudaGetLastError();
+        launch_decbig<DIM>(v, st);
+        k_decimate<DIM, 512><<<dgrid, 512, dec_smem_bytes(v), st>>>(v);
+        return cudaGetLastError();
+    });
 }
 
 template <int DIM>
@@ -2128,19 +2264,26 @@ __global__ void __launch_bounds__(256) k_ordered_sum_cta(const float* P, const i
     if (threadIdx.x < DIM) out[threadIdx.x] = sm.s[threadIdx.x];
 }
 
+template <int DIM, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_ordered_sum_seg(const float* P, const int32_t* idx, int n,
+                                                           float* out)
+{
+    __shared__ SegFoldSmem<BLOCK / 32, DIM> sm;
+    fold_members_seg<BLOCK / 32, DIM>(idx, n, P, sm);
+    if (threadIdx.x < DIM) out[threadIdx.x] = sm.out[threadIdx.x];
+}
+
 cudaError_t launch_ordered_sum(int dim, const float* P, const int32_t* idx, int n, float* out,
                                int method, cudaStream_t st)
 {
-    if (method == 2) {
-        if (dim == 2) k_ordered_sum_cta<2><<<1, 256, 0, st>>>(P, idx, n, out);
-        else if (dim == 3) k_ordered_sum_cta<3><<<1, 256, 0, st>>>(P, idx, n, out);
-        else return cudaErrorInvalidValue;
+    return with_dim(dim, [&](auto D) {
+        constexpr int DIM = decltype(D)::value;
+        if (method == 3) k_ordered_sum_seg<DIM, 256><<<1, 256, 0, st>>>(P, idx, n, out);
+        else if (method == 4) k_ordered_sum_seg<DIM, 1024><<<1, 1024, 0, st>>>(P, idx, n, out);
+        else if (method == 2) k_ordered_sum_cta<DIM><<<1, 256, 0, st>>>(P, idx, n, out);
+        else k_ordered_sum<DIM><<<1, 32, 0, st>>>(P, idx, n, out, method);
         return cudaGetLastError();
-    }
-    if (dim == 2) k_ordered_sum<2><<<1, 32, 0, st>>>(P, idx, n, out, method);
-    else if (dim == 3) k_ordered_sum<3><<<1, 32, 0, st>>>(P, idx, n, out, method);
-    else return cudaErrorInvalidValue;
-    return cudaGetLastError();
+    });
 }
 
 cudaError_t launch_set_given(const EngineView& v, int queue_decimation, cudaStream_t st)
@@ -2155,17 +2298,13 @@ cudaError_t launch_decimate(int dim, const EngineView& v, cudaStream_t st)
     const int grid = std::max(1, std::min(v.n_groups, v.n_sms * 2));
     const int smem = dec_smem_bytes(v);
     cudaError_t e = cudaSuccess;
-    switch (dim) {
-        case 2:
-            e = cudaFuncSetAttribute(k_decimate<2, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-            if (e == cudaSuccess) k_decimate<2, 512><<<grid, 512, smem, st>>>(v);
-            break;
-        case 3:
-            e = cudaFuncSetAttribute(k_decimate<3, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-            if (e == cudaSuccess) k_decimate<3, 512><<<grid, 512, smem, st>>>(v);
-            break;
-        default: return cudaErrorInvalidValue;
-    }
+    e = with_dim(dim, [&](auto D) {
+        constexpr int DIM = decltype(D)::value;
+        cudaError_t r = cudaFuncSetAttribute(k_decimate<DIM, 512>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (r == cudaSuccess) k_decimate<DIM, 512><<<grid, 512, smem, st>>>(v);
+        return r;
+    });
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
@@ -2200,11 +2339,9 @@ cudaError_t launch_evolve_step_dim(const EngineView& v, const TuneParams& tp, in
 cudaError_t launch_evolve_step(int dim, const EngineView& v, const TuneParams& tp, int assign_grid,
                                cudaStream_t st)
 {
-    switch (dim) {
-        case 2: return launch_evolve_step_dim<2>(v, tp, assign_grid, st);
-        case 3: return launch_evolve_step_dim<3>(v, tp, assign_grid, st);
-        default: return cudaErrorInvalidValue;
-    }
+    return with_dim(dim, [&](auto D) {
+        return launch_evolve_step_dim<decltype(D)::value>(v, tp, assign_grid, st);
+    });
 }
 
 cudaError_t launch_reset(const EngineView& v, cudaStream_t st)
@@ -2218,8 +2355,9 @@ cudaError_t launch_reset(const EngineView& v, cudaStream_t st)
 bool tune_supported(int dim, const TuneParams& tp)
 {
     (void)dim;
-    return (tp.block == 128 && (tp.items == 4 || tp.items == 8 || tp.items == 16)) ||
-           (tp.block == 256 && (tp.items == 4 || tp.items == 8));
+    const bool cull_ok = tp.cull_items == 2 || tp.cull_items == 4 || tp.cull_items == 8;
+    return cull_ok && ((tp.block == 128 && (tp.items == 4 || tp.items == 8 || tp.items == 16)) ||
+                       (tp.block == 256 && (tp.items == 4 || tp.items == 8)));
 }
 
 int assign_smem_bytes(int dim, const TuneParams& tp, int hist_ints)
@@ -2243,8 +2381,10 @@ int max_assign_blocks_per_sm(int dim, const TuneParams& tp, int hist_ints)
     const int dyn = hist_ints * 4;
 #define RD_OCC(D, B, I) \
     if (dim == D && tp.block == B && tp.items == I) return occ_of<D, B, I>(dyn);
+    RD_OCC(1, 128, 8) RD_OCC(1, 128, 4) RD_OCC(1, 256, 4) RD_OCC(1, 256, 8) RD_OCC(1, 128, 16)
     RD_OCC(2, 128, 8) RD_OCC(2, 128, 4) RD_OCC(2, 256, 4) RD_OCC(2, 256, 8) RD_OCC(2, 128, 16)
     RD_OCC(3, 128, 8) RD_OCC(3, 128, 4) RD_OCC(3, 256, 4) RD_OCC(3, 256, 8) RD_OCC(3, 128, 16)
+    RD_OCC(4, 128, 8) RD_OCC(4, 128, 4) RD_OCC(4, 256, 4) RD_OCC(4, 256, 8) RD_OCC(4, 128, 16)
 #undef RD_OCC
     return 0;
 }

@@ -108,13 +108,11 @@ cudaError_t launch_order_chains(int dim, const float* S, int ns, float rsq, unsi
                                 int32_t* deq, int32_t* order, int32_t* chain_start,
                                 int32_t* n_chains, cudaStream_t st)
 {
-    if (dim == 2)
-        k_order_chains<2><<<1, ORDER_BLOCK, 0, st>>>(S, ns, rsq, alive, deq, order, chain_start, n_chains);
-    else if (dim == 3)
-        k_order_chains<3><<<1, ORDER_BLOCK, 0, st>>>(S, ns, rsq, alive, deq, order, chain_start, n_chains);
-    else
-        return cudaErrorInvalidValue;
-    return cudaGetLastError();
+    return with_dim(dim, [&](auto D) {
+        k_order_chains<decltype(D)::value><<<1, ORDER_BLOCK, 0, st>>>(S, ns, rsq, alive, deq, order,
+                                                                     chain_start, n_chains);
+        return cudaGetLastError();
+    });
 }
 
 }  // namespace rdb

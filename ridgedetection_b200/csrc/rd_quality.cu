@@ -122,19 +122,19 @@ cudaError_t launch_min_dist(int dim, const float* A, int na, const float* B, int
                             cudaStream_t st)
 {
     if (na <= 0) return cudaSuccess;
-    if (dim == 2) k_min_dist<2><<<q_grid(na), Q_BLOCK, 0, st>>>(A, na, B, nb, out);
-    else if (dim == 3) k_min_dist<3><<<q_grid(na), Q_BLOCK, 0, st>>>(A, na, B, nb, out);
-    else return cudaErrorInvalidValue;
-    return cudaGetLastError();
+    return with_dim(dim, [&](auto D) {
+        k_min_dist<decltype(D)::value><<<q_grid(na), Q_BLOCK, 0, st>>>(A, na, B, nb, out);
+        return cudaGetLastError();
+    });
 }
 
 cudaError_t launch_axis_dist(int dim, const float* T, int n, float* out, cudaStream_t st)
 {
     if (n <= 0) return cudaSuccess;
-    if (dim == 2) k_axis_dist<2><<<(n + 255) / 256, 256, 0, st>>>(T, n, out);
-    else if (dim == 3) k_axis_dist<3><<<(n + 255) / 256, 256, 0, st>>>(T, n, out);
-    else return cudaErrorInvalidValue;
-    return cudaGetLastError();
+    return with_dim(dim, [&](auto D) {
+        k_axis_dist<decltype(D)::value><<<(n + 255) / 256, 256, 0, st>>>(T, n, out);
+        return cudaGetLastError();
+    });
 }
 
 cudaError_t launch_max2(const float* a, int na, const float* b, int nb, float* out, cudaStream_t st)

@@ -44,7 +44,11 @@ __device__ __forceinline__ uint32_t spread_by_2(uint32_t x)
 template <int DIM>
 __device__ __forceinline__ uint32_t morton_code(const float* p, float inv)
 {
-    if constexpr (DIM == 2) {
+    // the order only affects how tight the culling boxes are: one dimension
+    // sorts by its cell, four and more interleave the first three
+    if constexpr (DIM == 1) {
+        return spatial_cell(p[0], inv);
+    } else if constexpr (DIM == 2) {
         return spread_by_1(spatial_cell(p[0], inv)) | (spread_by_1(spatial_cell(p[1], inv)) << 1);
     } else {
         return spread_by_2(spatial_cell(p[0], inv)) | (spread_by_2(spatial_cell(p[1], inv)) << 1) |
@@ -144,8 +148,10 @@ cudaError_t launch_spatial_prep(int dim, const EngineView& v, int64_t n, void* s
                                 size_t scratch_bytes, float* Ps, int32_t* sorder, cudaStream_t st)
 {
     switch (dim) {
+        case 1: return spatial_prep_dim<1>(v, n, scratch, scratch_bytes, Ps, sorder, st);
         case 2: return spatial_prep_dim<2>(v, n, scratch, scratch_bytes, Ps, sorder, st);
         case 3: return spatial_prep_dim<3>(v, n, scratch, scratch_bytes, Ps, sorder, st);
+        case 4: return spatial_prep_dim<4>(v, n, scratch, scratch_bytes, Ps, sorder, st);
         default: return cudaErrorInvalidValue;
     }
 }

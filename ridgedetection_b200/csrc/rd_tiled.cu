@@ -14,7 +14,7 @@ namespace rdb {
 
 namespace {
 
-constexpr int MAXD = 3;
+constexpr int MAXD = RD_MAX_DIM;
 
 __device__ __forceinline__ int f2s(float f)
 {
@@ -208,6 +208,111 @@ __global__ void k_gather_idx(const float* __restrict__ P, const int32_t* __restr
     }
 }
 
+// ---------------------------------------------------------------------------
+// Subdivision of oversize tiles on the device, one level at a time
+// (grouped_tile_tree.inl:247-330).  A level holds nodes; node i's entries are
+// its own points then its halo points (code = 2 i + 0 / 1).  Each node is cut
+// in two halves along one dimension (boxes from the host, computed with the
+// reference's FP32 operations); an own point goes to the own list of the first
+// half that contains it and to the halo list of every half it is near; a halo
+// point to the halo lists it is near.  Outputs are (key, point) pairs with key
+// = 2 (2 i + s) + (0 own / 1 halo), sorted stably, so every list keeps the
+// parent's order (own-derived halo entries before halo-derived ones).
+// ---------------------------------------------------------------------------
+struct SplitBox {
+    float mn[2][MAXD], mx[2][MAXD], emin[2][MAXD], emax[2][MAXD];
+};
+
+// own: mn <= x < mx in every dimension; halo ("nearby"): inside the box
+// grown by r1 on every side (emin = mn - r1, emax = mx + r1, FP32) but not
+// own -- the tests of grouped_tile_tree.inl's isInside / isNearby
+template <int DIM>
+__device__ __forceinline__ void split_flags(const float* p, const SplitBox& b, const int kind,
+                                            int& own_s, bool (&near)[2])
+{
+    own_s = -1;
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+        bool in = true, nb = true;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            if (p[d] < b.mn[s][d] || p[d] >= b.mx[s][d]) in = false;
+            if (p[d] < b.emin[s][d] || p[d] >= b.emax[s][d]) nb = false;
+        }
+        near[s] = nb && !in;
+        if (kind == 0 && in && own_s < 0) own_s = s;
+    }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256) k_split_count(const float* __restrict__ P,
+                                                     const int32_t* __restrict__ E,
+                                                     const int32_t* __restrict__ code, int64_t nE,
+                                                     const SplitBox* __restrict__ boxes,
+                                                     int32_t* __restrict__ cnt)
+{
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nE;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        float p[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) p[d] = P[(int64_t)E[e] * DIM + d];
+        int own_s;
+        bool near[2];
+        split_flags<DIM>(p, boxes[code[e] >> 1], code[e] & 1, own_s, near);
+        cnt[e] = (own_s >= 0) + (int)near[0] + (int)near[1];
+    }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256) k_split_fill(const float* __restrict__ P,
+                                                    const int32_t* __restrict__ E,
+                                                    const int32_t* __restrict__ code, int64_t nE,
+                                                    const SplitBox* __restrict__ boxes,
+                                                    const int32_t* __restrict__ off,
+                                                    uint32_t* __restrict__ keys,
+                                                    int32_t* __restrict__ vals)
+{
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nE;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        float p[DIM];
+        const int32_t i = E[e];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) p[d] = P[(int64_t)i * DIM + d];
+        const int node = code[e] >> 1;
+        int own_s;
+        bool near[2];
+        split_flags<DIM>(p, boxes[node], code[e] & 1, own_s, near);
+        int o = off[e];
+        if (own_s >= 0) {
+            keys[o] = (uint32_t)(2 * (2 * node + own_s));
+            vals[o++] = i;
+        }
+#pragma unroll
+        for (int s = 0; s < 2; ++s)
+            if (near[s]) {
+                keys[o] = (uint32_t)(2 * (2 * node + s) + 1);
+                vals[o++] = i;
+            }
+    }
+}
+
+// gathers the entries of the nodes of a level: tab per node = (first source
+// entry, entries, first destination entry); entries get code 2 node + kind,
+// kind = 1 from own_n on (the node's own points come first)
+__global__ void k_split_seed(const int32_t* __restrict__ src, const int64_t* __restrict__ tab,
+                             int nnodes, int32_t* __restrict__ E, int32_t* __restrict__ code)
+{
+    for (int q = blockIdx.y; q < nnodes; q += gridDim.y) {
+        const int64_t so = tab[4 * q], nn = tab[4 * q + 1], own_n = tab[4 * q + 2],
+                      dof = tab[4 * q + 3];
+        for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nn;
+             e += (int64_t)gridDim.x * blockDim.x) {
+            E[dof + e] = src[so + e];
+            code[dof + e] = 2 * q + (e >= own_n ? 1 : 0);
+        }
+    }
+}
+
 // leaf chosen points -> one array in leaf order; tab: (src float off, n floats, dst float off)
 __global__ void k_concat(const float* __restrict__ S, const int64_t* __restrict__ tab, int nl,
                          float* __restrict__ out)
@@ -249,68 +354,6 @@ void tile_bounds(const HBox& p, int d, int c, int n, float& mn, float& mx)
     if (c == n - 1) mx = p.mx[d];
 }
 
-bool is_inside(const HBox& b, const float* p, int dim)
-{
-    for (int d = 0; d < dim; ++d)
-        if (p[d] < b.mn[d] || p[d] >= b.mx[d]) return false;
-    return true;
-}
-
-bool is_nearby(const HBox& b, const float* p, float r, int dim)
-{
-    for (int d = 0; d < dim; ++d) {
-        const volatile float emin = b.mn[d] - r;
-        const volatile float emax = b.mx[d] + r;
-        if (p[d] < emin || p[d] >= emax) return false;
-    }
-    return !is_inside(b, p, dim);
-}
-
-struct HostLeaf {
-    std::vector<int32_t> own, halo;
-};
-
-// grouped_tile_tree.inl:247-330: half-split along dimension level % dim over
-// the parent's own points, then its halo; drop sub-tiles with < 2 own points;
-// recurse while own points >= cap.
-bool split_tile(const HBox& parent, const std::vector<int32_t>& own,
-                const std::vector<int32_t>& halo, int level, int64_t cap, float r,
-                const float* P, int dim, std::vector<HostLeaf>& out)
-{
-    if (level > 64) return false;
-    const int sd = level % dim;
-    HBox sub[2];
-    for (int s = 0; s < 2; ++s) {
-        for (int d = 0; d < dim; ++d) {
-            if (d == sd) tile_bounds(parent, d, s, 2, sub[s].mn[d], sub[s].mx[d]);
-            else tile_bounds(parent, d, 0, 1, sub[s].mn[d], sub[s].mx[d]);
-        }
-        calc_dist(sub[s], dim);
-    }
-    std::vector<int32_t> so[2], sh[2];
-    for (int32_t i : own) {
-        const float* p = P + (int64_t)i * dim;
-        for (int s = 0; s < 2; ++s)
-            if (is_nearby(sub[s], p, r, dim)) sh[s].push_back(i);
-        for (int s = 0; s < 2; ++s)
-            if (is_inside(sub[s], p, dim)) { so[s].push_back(i); break; }
-    }
-    for (int32_t i : halo) {
-        const float* p = P + (int64_t)i * dim;
-        for (int s = 0; s < 2; ++s)
-            if (is_nearby(sub[s], p, r, dim)) sh[s].push_back(i);
-    }
-    for (int s = 0; s < 2; ++s) {
-        if (so[s].size() <= 1) continue;
-        if ((int64_t)so[s].size() < cap) {
-            out.push_back(HostLeaf{std::move(so[s]), std::move(sh[s])});
-        } else if (!split_tile(sub[s], so[s], sh[s], level + 1, cap, r, P, dim, out)) {
-            return false;
-        }
-    }
-    return true;
-}
-
 }  // namespace
 
 int TiledRunner::fail(const char* what, cudaError_t e)
@@ -333,7 +376,7 @@ int TiledRunner::run(const float* d_points, int64_t n, int dim, float r1, float 
     tm_ = TiledTimers();
     ns_ = 0;
     leaf_ns_.clear();
-    if (dim != 2 && dim != 3) { last_error = "dim must be 2 or 3"; return 6; }
+    if (!dim_supported(dim)) { last_error = "dim must be 1 to 4"; return 6; }
     if (n <= 0) return 0;
     if (n > INT32_MAX / 4) { last_error = "too many points"; return 1; }
     int64_t ntiles = 1;
@@ -346,9 +389,10 @@ int TiledRunner::run(const float* d_points, int64_t n, int dim, float r1, float 
     // 1. bounding box
     TK(bBox_.ensure(8 * MAXD));
     k_bbox_init<<<1, 32, 0, st>>>(bBox_.as<int>(), dim);
-    if (dim == 2) k_bbox<2><<<grid_of(n), 256, 0, st>>>(d_points, n, bBox_.as<int>());
-    else k_bbox<3><<<grid_of(n), 256, 0, st>>>(d_points, n, bBox_.as<int>());
-    TK(cudaGetLastError());
+    TK(with_dim(dim, [&](auto D) {
+        k_bbox<decltype(D)::value><<<grid_of(n), 256, 0, st>>>(d_points, n, bBox_.as<int>());
+        return cudaGetLastError();
+    }));
     int hbox[2 * MAXD];
     TK(cudaMemcpyAsync(hbox, bBox_.p, 8 * dim, cudaMemcpyDeviceToHost, st));
     TK(cudaStreamSynchronize(st));
@@ -386,9 +430,11 @@ int TiledRunner::run(const float* d_points, int64_t n, int dim, float r1, float 
     // 3. emission counts and offsets (point order)
     TK(bCnt_.ensure(4 * (size_t)(n + 1)));
     TK(bOff_.ensure(4 * (size_t)(n + 1)));
-    if (dim == 2) k_emit_count<2><<<grid_of(n), 256, 0, st>>>(d_points, n, gd, tmin, tmax, bCnt_.as<int32_t>());
-    else k_emit_count<3><<<grid_of(n), 256, 0, st>>>(d_points, n, gd, tmin, tmax, bCnt_.as<int32_t>());
-    TK(cudaGetLastError());
+    TK(with_dim(dim, [&](auto D) {
+        k_emit_count<decltype(D)::value><<<grid_of(n), 256, 0, st>>>(d_points, n, gd, tmin, tmax,
+                                                                    bCnt_.as<int32_t>());
+        return cudaGetLastError();
+    }));
     size_t tb = 0;
     TK(cub::DeviceScan::ExclusiveSum(nullptr, tb, bCnt_.as<int32_t>(), bOff_.as<int32_t>(), (int)n, st));
     TK(bTemp_.ensure(tb));
@@ -404,13 +450,12 @@ int TiledRunner::run(const float* d_points, int64_t n, int dim, float r1, float 
     TK(bVals_.ensure(4 * (size_t)(m + 1)));
     TK(bKeys2_.ensure(4 * (size_t)(m + 1)));
     TK(bVals2_.ensure(4 * (size_t)(m + 1)));
-    if (dim == 2)
-        k_emit_fill<2><<<grid_of(n), 256, 0, st>>>(d_points, n, gd, tmin, tmax, bOff_.as<int32_t>(),
-                                                  bKeys_.as<uint32_t>(), bVals_.as<int32_t>());
-    else
-        k_emit_fill<3><<<grid_of(n), 256, 0, st>>>(d_points, n, gd, tmin, tmax, bOff_.as<int32_t>(),
-                                                  bKeys_.as<uint32_t>(), bVals_.as<int32_t>());
-    TK(cudaGetLastError());
+    TK(with_dim(dim, [&](auto D) {
+        k_emit_fill<decltype(D)::value><<<grid_of(n), 256, 0, st>>>(
+            d_points, n, gd, tmin, tmax, bOff_.as<int32_t>(), bKeys_.as<uint32_t>(),
+            bVals_.as<int32_t>());
+        return cudaGetLastError();
+    }));
     int bits = 1;
     while ((int64_t(1) << bits) < 2 * ntiles) ++bits;
     tb = 0;
@@ -430,13 +475,193 @@ int TiledRunner::run(const float* d_points, int64_t n, int dim, float r1, float 
     TK(cudaMemcpyAsync(seg.data(), bSeg_.p, 4 * seg.size(), cudaMemcpyDeviceToHost, st));
     TK(cudaStreamSynchronize(st));
 
-    // 6. leaves in pre-order; oversize tiles are split on the host
+    // 6. leaves in pre-order.  Tiles with cap or more own points are split on
+    //    the device, level by level (k_split_*); their leaves take the tile's
+    //    place in the pre-order, ordered by their split paths.
     std::vector<CloudDesc> cl;
-    std::vector<HostLeaf> extra;
-    std::vector<int64_t> extra_at;  // leaf index of each extra leaf
-    std::vector<float> hP;
     auto own_of = [&](int64_t t, int64_t& s, int64_t& e) { s = seg[4 * t]; e = seg[4 * t + 1]; };
     auto halo_of = [&](int64_t t, int64_t& s, int64_t& e) { s = seg[4 * t + 2]; e = seg[4 * t + 3]; };
+    struct SubLeaf {
+        int64_t root;
+        uint64_t path;     // split choices, left-aligned: pre-order = increasing path
+        int buf;           // level buffer holding its lists
+        int64_t off, own, halo;
+    };
+    struct SplitNode {
+        HBox box;
+        int64_t root;
+        uint64_t path;
+        int depth;         // splits above it (its level is depth + 1)
+        int64_t src, own, halo;  // its lists in the current source buffer
+    };
+    std::vector<SubLeaf> subleaves;
+    std::vector<SplitNode> nodes;
+    for (int64_t t = 0; t < ntiles; ++t) {
+        int64_t os, oe, hs, he;
+        own_of(t, os, oe);
+        halo_of(t, hs, he);
+        const int64_t no = oe - os, nh = he - hs;
+        if (nh > 0 && no > 0 && hs != oe) { last_error = "internal: tile segments not adjacent"; return 2; }
+        if (no <= 1 || no < cap) continue;
+        SplitNode nd;
+        int64_t rem = t;
+        for (int d = 0; d < dim; ++d) {
+            const int c = (int)(rem % tpd[d]);
+            rem /= tpd[d];
+            nd.box.mn[d] = hb[gd.off[d] + c];
+            nd.box.mx[d] = hb[tot + gd.off[d] + c];
+        }
+        calc_dist(nd.box, dim);
+        nd.root = t;
+        nd.path = 0;
+        nd.depth = 0;
+        nd.src = os;
+        nd.own = no;
+        nd.halo = nh;
+        nodes.push_back(nd);
+    }
+    split_bufs_.clear();
+    const int32_t* src_vals = bVals2_.as<int32_t>();
+    while (!nodes.empty()) {
+        const int nn = (int)nodes.size();
+        if (nodes[0].depth + 1 > 64) {
+            last_error = "tile subdivision did not terminate (duplicate points above capacity)";
+            return 1;
+        }
+        // this level's entries and the two halves of every node
+        std::vector<int64_t> tab(4 * (size_t)nn);
+        std::vector<SplitBox> boxes((size_t)nn);
+        std::vector<HBox> halves(2 * (size_t)nn);
+        int64_t nE = 0;
+        for (int q = 0; q < nn; ++q) {
+            const SplitNode& nd = nodes[q];
+            tab[4 * q] = nd.src;
+            tab[4 * q + 1] = nd.own + nd.halo;
+            tab[4 * q + 2] = nd.own;
+            tab[4 * q + 3] = nE;
+            nE += nd.own + nd.halo;
+            const int sd = (nd.depth + 1) % dim;
+            for (int sh = 0; sh < 2; ++sh) {
+                HBox& hbx = halves[2 * q + sh];
+                for (int d = 0; d < dim; ++d) {
+                    if (d == sd) tile_bounds(nd.box, d, sh, 2, hbx.mn[d], hbx.mx[d]);
+                    else tile_bounds(nd.box, d, 0, 1, hbx.mn[d], hbx.mx[d]);
+                }
+                calc_dist(hbx, dim);
+                for (int d = 0; d < MAXD; ++d) {
+                    const bool live = d < dim;
+                    boxes[q].mn[sh][d] = live ? hbx.mn[d] : 0.0f;
+                    boxes[q].mx[sh][d] = live ? hbx.mx[d] : 0.0f;
+                    const volatile float emin = live ? hbx.mn[d] - r1 : 0.0f;
+                    const volatile float emax = live ? hbx.mx[d] + r1 : 0.0f;
+                    boxes[q].emin[sh][d] = emin;
+                    boxes[q].emax[sh][d] = emax;
+                }
+            }
+        }
+        if (nE > INT32_MAX / 4) { last_error = "subdivision level too large"; return 1; }
+        TK(bSplitTab_.ensure(sizeof(int64_t) * tab.size()));
+        TK(cudaMemcpyAsync(bSplitTab_.p, tab.data(), sizeof(int64_t) * tab.size(),
+                           cudaMemcpyHostToDevice, st));
+        TK(bSplitBox_.ensure(sizeof(SplitBox) * boxes.size()));
+        TK(cudaMemcpyAsync(bSplitBox_.p, boxes.data(), sizeof(SplitBox) * boxes.size(),
+                           cudaMemcpyHostToDevice, st));
+        TK(bSplitE_.ensure(4 * (size_t)(nE + 1)));
+        TK(bSplitCode_.ensure(4 * (size_t)(nE + 1)));
+        TK(bSplitCnt_.ensure(4 * (size_t)(nE + 1)));
+        TK(bSplitOff_.ensure(4 * (size_t)(nE + 1)));
+        {
+            dim3 g((unsigned)std::min<int64_t>(64, (nE + 255) / 256 + 1), (unsigned)std::min(nn, 1024));
+            k_split_seed<<<g, 256, 0, st>>>(src_vals, bSplitTab_.as<int64_t>(), nn,
+                                            bSplitE_.as<int32_t>(), bSplitCode_.as<int32_t>());
+            TK(cudaGetLastError());
+        }
+        TK(with_dim(dim, [&](auto D) {
+            k_split_count<decltype(D)::value><<<grid_of(nE), 256, 0, st>>>(
+                d_points, bSplitE_.as<int32_t>(), bSplitCode_.as<int32_t>(), nE,
+                bSplitBox_.as<SplitBox>(), bSplitCnt_.as<int32_t>());
+            return cudaGetLastError();
+        }));
+        size_t sb = 0;
+        TK(cub::DeviceScan::ExclusiveSum(nullptr, sb, bSplitCnt_.as<int32_t>(), bSplitOff_.as<int32_t>(),
+                                         (int)nE, st));
+        TK(bTemp_.ensure(sb));
+        TK(cub::DeviceScan::ExclusiveSum(bTemp_.p, sb, bSplitCnt_.as<int32_t>(), bSplitOff_.as<int32_t>(),
+                                         (int)nE, st));
+        int32_t lo_ = 0, lc_ = 0;
+        TK(cudaMemcpyAsync(&lo_, bSplitOff_.as<int32_t>() + nE - 1, 4, cudaMemcpyDeviceToHost, st));
+        TK(cudaMemcpyAsync(&lc_, bSplitCnt_.as<int32_t>() + nE - 1, 4, cudaMemcpyDeviceToHost, st));
+        TK(cudaStreamSynchronize(st));
+        const int64_t mo = (int64_t)lo_ + lc_;
+        TK(bSplitK_.ensure(4 * (size_t)(mo + 1)));
+        TK(bSplitV_.ensure(4 * (size_t)(mo + 1)));
+        TK(bSplitK2_.ensure(4 * (size_t)(mo + 1)));
+        split_bufs_.emplace_back(new DevBuf());
+        DevBuf& vout = *split_bufs_.back();
+        TK(vout.ensure(4 * (size_t)(mo + 1)));
+        TK(with_dim(dim, [&](auto D) {
+            k_split_fill<decltype(D)::value><<<grid_of(nE), 256, 0, st>>>(
+                d_points, bSplitE_.as<int32_t>(), bSplitCode_.as<int32_t>(), nE,
+                bSplitBox_.as<SplitBox>(), bSplitOff_.as<int32_t>(), bSplitK_.as<uint32_t>(),
+                bSplitV_.as<int32_t>());
+            return cudaGetLastError();
+        }));
+        int kbits = 1;
+        while ((int64_t(1) << kbits) < 4 * (int64_t)nn) ++kbits;
+        sb = 0;
+        TK(cub::DeviceRadixSort::SortPairs(nullptr, sb, bSplitK_.as<uint32_t>(), bSplitK2_.as<uint32_t>(),
+                                           bSplitV_.as<int32_t>(), vout.as<int32_t>(), (int)mo, 0,
+                                           kbits, st));
+        TK(bTemp_.ensure(sb));
+        TK(cub::DeviceRadixSort::SortPairs(bTemp_.p, sb, bSplitK_.as<uint32_t>(), bSplitK2_.as<uint32_t>(),
+                                           bSplitV_.as<int32_t>(), vout.as<int32_t>(), (int)mo, 0,
+                                           kbits, st));
+        TK(bSplitSeg_.ensure(8 * (size_t)(4 * nn + 1)));
+        TK(cudaMemsetAsync(bSplitSeg_.p, 0, 8 * (size_t)(4 * nn), st));
+        if (mo > 0) {
+            k_seg_bounds<<<grid_of(mo), 256, 0, st>>>(bSplitK2_.as<uint32_t>(), mo, bSplitSeg_.as<int32_t>());
+            TK(cudaGetLastError());
+        }
+        std::vector<int32_t> cseg(8 * (size_t)nn);
+        TK(cudaMemcpyAsync(cseg.data(), bSplitSeg_.p, 4 * cseg.size(), cudaMemcpyDeviceToHost, st));
+        TK(cudaStreamSynchronize(st));
+        // the halves: dropped (< 2 own points), leaves (< cap) or next level
+        std::vector<SplitNode> next;
+        const int bi = (int)split_bufs_.size() - 1;
+        for (int q = 0; q < nn; ++q) {
+            for (int sh = 0; sh < 2; ++sh) {
+                const int c = 2 * q + sh;
+                const int64_t os = cseg[4 * c], oe = cseg[4 * c + 1];
+                const int64_t hs = cseg[4 * c + 2], he = cseg[4 * c + 3];
+                const int64_t no = oe - os, nh = he - hs;
+                if (no <= 1) continue;
+                if (nh > 0 && hs != oe) { last_error = "internal: split segments not adjacent"; return 2; }
+                const SplitNode& pn = nodes[q];
+                const uint64_t path = pn.path | ((uint64_t)sh << (63 - pn.depth));
+                if (no < cap) {
+                    subleaves.push_back(SubLeaf{pn.root, path, bi, os, no, nh});
+                } else {
+                    SplitNode ch;
+                    ch.box = halves[c];
+                    ch.root = pn.root;
+                    ch.path = path;
+                    ch.depth = pn.depth + 1;
+                    ch.src = os;
+                    ch.own = no;
+                    ch.halo = nh;
+                    next.push_back(ch);
+                }
+            }
+        }
+        nodes.swap(next);
+        src_vals = vout.as<int32_t>();
+    }
+    std::stable_sort(subleaves.begin(), subleaves.end(), [](const SubLeaf& x, const SubLeaf& y) {
+        return x.root != y.root ? x.root < y.root : x.path < y.path;
+    });
+    size_t nxt = 0;                 // next sub-leaf in pre-order
+    std::vector<int64_t> xoffs;     // per sub-leaf (pre-order): offset in the extra points
+    int64_t xtotal = 0;
     for (int64_t t = 0; t < ntiles; ++t) {
         int64_t os, oe, hs, he;
         own_of(t, os, oe);
@@ -444,7 +669,6 @@ int TiledRunner::run(const float* d_points, int64_t n, int dim, float r1, float 
         const int64_t no = oe - os, nh = he - hs;
         if (no <= 1) continue;
         if (no < cap) {
-            if (nh > 0 && hs != oe) { last_error = "internal: tile segments not adjacent"; return 2; }
             CloudDesc cd;
             std::memset(&cd, 0, sizeof(cd));
             cd.p_off = os;
@@ -455,49 +679,31 @@ int TiledRunner::run(const float* d_points, int64_t n, int dim, float r1, float 
             cl.push_back(cd);
             continue;
         }
-        if (hP.empty()) {
-            hP.resize((size_t)n * dim);
-            TK(cudaMemcpyAsync(hP.data(), d_points, sizeof(float) * n * dim, cudaMemcpyDeviceToHost, st));
-            TK(cudaStreamSynchronize(st));
-        }
-        std::vector<int32_t> own((size_t)no), halo((size_t)nh);
-        TK(cudaMemcpyAsync(own.data(), bVals2_.as<int32_t>() + os, 4 * no, cudaMemcpyDeviceToHost, st));
-        if (nh) TK(cudaMemcpyAsync(halo.data(), bVals2_.as<int32_t>() + hs, 4 * nh, cudaMemcpyDeviceToHost, st));
-        TK(cudaStreamSynchronize(st));
-        HBox tb_;
-        int64_t rem = t;
-        for (int d = 0; d < dim; ++d) {
-            const int c = (int)(rem % tpd[d]);
-            rem /= tpd[d];
-            tb_.mn[d] = hb[gd.off[d] + c];
-            tb_.mx[d] = hb[tot + gd.off[d] + c];
-        }
-        calc_dist(tb_, dim);
-        std::vector<HostLeaf> sub;
-        if (!split_tile(tb_, own, halo, 1, cap, r1, hP.data(), dim, sub)) {
-            last_error = "tile subdivision did not terminate (duplicate points above capacity)";
-            return 1;
-        }
-        for (auto& L : sub) {
+        for (; nxt < subleaves.size() && subleaves[nxt].root == t; ++nxt) {
+            const SubLeaf& L = subleaves[nxt];
             CloudDesc cd;
             std::memset(&cd, 0, sizeof(cd));
-            cd.n_own = (int32_t)L.own.size();
-            cd.n_all = (int32_t)(L.own.size() + L.halo.size());
+            cd.p_off = m + xtotal;
+            cd.n_own = (int32_t)L.own;
+            cd.n_all = (int32_t)(L.own + L.halo);
             cd.r1 = r1;
             cd.r2 = r2;
-            cd.p_off = -1;  // filled below
-            extra_at.push_back((int64_t)cl.size());
             cl.push_back(cd);
-            extra.push_back(std::move(L));
+            xoffs.push_back(xtotal);
+            xtotal += L.own + L.halo;
         }
     }
-    std::vector<int32_t> xidx;
-    for (size_t k = 0; k < extra.size(); ++k) {
-        cl[extra_at[k]].p_off = m + (int64_t)xidx.size();
-        xidx.insert(xidx.end(), extra[k].own.begin(), extra[k].own.end());
-        xidx.insert(xidx.end(), extra[k].halo.begin(), extra[k].halo.end());
+    // the sub-leaves' point lists, in pre-order, behind the tiles' lists
+    if (xtotal > 0) {
+        TK(bExtra_.ensure(4 * (size_t)xtotal));
+        for (size_t k = 0; k < subleaves.size(); ++k) {
+            const SubLeaf& L = subleaves[k];
+            TK(cudaMemcpyAsync(bExtra_.as<int32_t>() + xoffs[k],
+                               split_bufs_[L.buf]->as<int32_t>() + L.off,
+                               4 * (size_t)(L.own + L.halo), cudaMemcpyDeviceToDevice, st));
+        }
     }
-    const int64_t total = m + (int64_t)xidx.size();
+    const int64_t total = m + xtotal;
     std::vector<GroupDesc> gr;
     if (local_policy) {
         // RD_LOCAL: every leaf is its own group, decimated on its own with the
@@ -526,16 +732,20 @@ int TiledRunner::run(const float* d_points, int64_t n, int dim, float r1, float 
     }
     if (int rc = eng_.setup(dim, cl, gr, total)) { last_error = eng_.last_error; return rc; }
     // 7. packed per-leaf evolve points: own then halo, each in input order
-    if (dim == 2) k_gather_idx<2><<<grid_of(m * 2), 256, 0, st>>>(d_points, bVals2_.as<int32_t>(), m, eng_.points());
-    else k_gather_idx<3><<<grid_of(m * 3), 256, 0, st>>>(d_points, bVals2_.as<int32_t>(), m, eng_.points());
-    TK(cudaGetLastError());
-    if (!xidx.empty()) {
-        TK(bExtra_.ensure(4 * xidx.size()));
-        TK(cudaMemcpyAsync(bExtra_.p, xidx.data(), 4 * xidx.size(), cudaMemcpyHostToDevice, st));
-        const int64_t xm = (int64_t)xidx.size();
-        if (dim == 2) k_gather_idx<2><<<grid_of(xm * 2), 256, 0, st>>>(d_points, bExtra_.as<int32_t>(), xm, eng_.points() + m * 2);
-        else k_gather_idx<3><<<grid_of(xm * 3), 256, 0, st>>>(d_points, bExtra_.as<int32_t>(), xm, eng_.points() + m * 3);
-        TK(cudaGetLastError());
+    TK(with_dim(dim, [&](auto D) {
+        constexpr int DIM = decltype(D)::value;
+        k_gather_idx<DIM><<<grid_of(m * DIM), 256, 0, st>>>(d_points, bVals2_.as<int32_t>(), m,
+                                                            eng_.points());
+        return cudaGetLastError();
+    }));
+    if (xtotal > 0) {
+        const int64_t xm = xtotal;
+        TK(with_dim(dim, [&](auto D) {
+            constexpr int DIM = decltype(D)::value;
+            k_gather_idx<DIM><<<grid_of(xm * DIM), 256, 0, st>>>(d_points, bExtra_.as<int32_t>(), xm,
+                                                                 eng_.points() + m * DIM);
+            return cudaGetLastError();
+        }));
     }
     TK(cudaStreamSynchronize(st));
     const auto t1 = clk::now();

@@ -26,6 +26,7 @@
 #include "rd_engine_host.hpp"
 
 #include <cstdint>
+#include <memory>
 #include <vector>
 
 namespace rdb {
@@ -60,7 +61,12 @@ private:
     int fail(const char* what, cudaError_t e);
     Engine eng_;
     DevBuf bBox_, bBounds_, bCnt_, bOff_, bKeys_, bVals_, bKeys2_, bVals2_, bTemp_, bSeg_;
-    DevBuf bExtra_, bOut_, bTab_, bHostP_;
+    DevBuf bExtra_, bOut_, bTab_;
+    // subdivision of oversize tiles on the device: per-level scratch, and the
+    // sorted point lists of every level (the leaves' lists stay there)
+    DevBuf bSplitTab_, bSplitBox_, bSplitE_, bSplitCode_, bSplitCnt_, bSplitOff_, bSplitK_,
+        bSplitV_, bSplitK2_, bSplitSeg_;
+    std::vector<std::unique_ptr<DevBuf>> split_bufs_;
     std::vector<int32_t> leaf_ns_;
     int64_t ns_ = 0;
     TiledTimers tm_;

@@ -1,6 +1,7 @@
-"""Ordered FP32 sums (rd_ordered_sum): the add chain, the warp-parallel and the
-CTA-wide exact evaluations must all reproduce the serial loop of rd/cpu/brute_force/evolve.hpp:71-74
-bit for bit, including ties, binade crossings, cancellation and non-finite terms."""
+"""Ordered FP32 sums (rd_ordered_sum): the add chain, the warp-parallel, the
+CTA-wide and the warp-segmented (8 and 32 segments) exact evaluations must all
+reproduce the serial loop of rd/cpu/brute_force/evolve.hpp:71-74 bit for bit,
+including ties, binade crossings, cancellation and non-finite terms."""
 import ctypes
 
 import numpy as np
@@ -79,7 +80,7 @@ def _cases():
 CASES = _cases()
 
 
-@pytest.mark.parametrize("method", [0, 1, 2])
+@pytest.mark.parametrize("method", [0, 1, 2, 3, 4])
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_ordered_sum_matches_serial(env, name, method):
     X = CASES[name]
@@ -96,7 +97,7 @@ def test_ordered_sum_ragged_sizes(env, n):
     X = np.random.default_rng(n).normal(size=(max(n, 1), 2)).astype(np.float32) + 3.0
     idx = np.arange(n)
     want = serial_sum(X, idx)
-    for method in (0, 1, 2):
+    for method in (0, 1, 2, 3, 4):
         assert same(gpu_sum(env, X, idx, method), want), (n, method)
 
 

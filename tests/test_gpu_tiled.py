@@ -105,3 +105,31 @@ def test_tiled_local_policy_matches_oracle(rdb, case):
     assert nl == nl_ref
     assert st.err_bits == 0
     assert bits_equal(S, S_ref)
+
+
+@pytest.mark.parametrize("case", [
+    # deep subdivision: a small capacity splits tiles over many levels
+    ("spiral_deep", 30_000, 0.2, 0.4, 200, (2, 2)),
+    ("helix_deep", 30_000, 0.15, 0.3, 300, (2, 1, 2)),
+    ("sine_deep", 20_000, 0.3, 0.6, 150, (3, 1)),
+])
+def test_device_subdivision_matches_oracle(rdb, case):
+    """Tiles with max_tile_capacity or more own points are split level by level
+    on the device (grouped_tile_tree.inl:247-330); the leaves, their order and
+    the ridge equal the oracle's."""
+    kind, n, r1, r2, cap, tpd = case
+    P = {"spiral_deep": lambda: G.spiral2d(n, seed=51), "helix_deep": lambda: G.helix3d(n, seed=52),
+         "sine_deep": lambda: G.sine2d(n, seed=53)}[kind]()
+    S_ref, _, nl_ref = O.ridge_tiled(P, r1, r2, cap, tpd)
+    S, st, nl = rdb.tiled_ridge_detection(P, r1, r2, cap, tpd)
+    assert nl == nl_ref and nl > 20
+    assert bits_equal(S, S_ref) and st.err_bits == 0
+
+
+def test_subdivision_of_duplicates_is_an_error(rdb):
+    """Identical points above the capacity can never be separated: the split
+    gives up after 64 levels with an error instead of looping."""
+    P = np.zeros((500, 2), np.float32)
+    P[:250] = 1.0
+    with pytest.raises(rdb.RDError):
+        rdb.tiled_ridge_detection(P, 0.2, 0.4, 100, (1, 1))

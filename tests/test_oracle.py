@@ -215,3 +215,21 @@ def test_batch_subset_small_clouds_match_reference():
             checked += 1
         off += m
     assert checked >= 30
+
+
+@pytest.mark.parametrize("dim", [1, 4])
+def test_restatement_matches_reference_in_other_dims(dim):
+    """The restatement against the reference's own serial code in 1 and 4
+    dimensions (the CPU API takes the dimension at run time)."""
+    r = np.random.default_rng(dim)
+    if dim == 1:
+        P = np.sort(r.normal(0, 2, 3000))[r.permutation(3000)][:, None].astype(np.float32)
+        r1, r2 = 0.1, 0.2
+    else:
+        t = r.uniform(0, 6 * np.pi, 3000)
+        P = np.stack([np.cos(t), np.sin(t), 0.15 * t, 0.3 * np.sin(2 * t)], 1)
+        P = (P + r.normal(0, 0.05, P.shape)).astype(np.float32)
+        r1, r2 = 0.2, 0.4
+    S, _ = O.ridge_bf(P, r1, r2)
+    assert bits_equal(S, O.ref_ridge_bf(P, r1, r2))
+    assert bits_equal(O.choose(P, r1), O.ref_choose(P, r1))
