@@ -406,6 +406,9 @@ def run_b200_bf(args, world, rank, local):
     else:
         roofline = dict(all_pairs)
 
+    # like-for-like with the CPU baseline: evolve passes from the chosen set
+    # right after choose, nothing else
+    sw_pairs, sw_s, sw_passes = same_work_gpu(dP, r1)
     if world > 1:
         torch.distributed.barrier()
     rd.close()
@@ -451,16 +454,66 @@ def run_b200_bf(args, world, rank, local):
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(P.nbytes),
                 "d2h_bytes_per_step": int(ns_final * dim * 4)},
         # per loop iteration: assign, key histogram (culled), chunk scan, key
-        # bases, scatter, sum+shift, control, decimate, loop condition; per
-        # solve about 32 more (reset, choose rounds, spatial order)
-        "gpu_launches": args.steps * ((9 if culled else 8) * iters_step + 32),
+        # bases, scatter, sum+shift (with the control step), decimate, loop
+        # condition; per solve about 40 more (reset, choose rounds with their
+        # survivor compaction, spatial order)
+        "gpu_launches": args.steps * ((8 if culled else 7) * iters_step + 40),
         "clocks": clocks,
         "cpu_baseline": cpu,
+    }
+    line["same_work"] = {
+        "what": "evolve passes over the whole cloud from the chosen set right after choose "
+                "(the CPU baseline's work), rd_evolve_ws with caller scratch, per-pass time from "
+                "a (k+1)-pass minus a 1-pass call",
+        "gpu_pairs_per_s": sw_pairs / sw_s, "gpu_ms_per_pass": sw_s * 1e3,
+        "pairs_per_pass": sw_pairs, "passes": sw_passes,
+        "cpu_pairs_per_s": cpu["value"] if cpu else None,
+        "gpu_over_cpu": (sw_pairs / sw_s / cpu["value"]) if cpu and cpu.get("value") else None,
     }
     line.update(subs)
     print(json.dumps(line))
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+def same_work_gpu(dP, r1, passes=20):
+    """Evolve passes over the cloud dP from the chosen set right after choose
+    -- the work the CPU baseline times -- through rd_evolve_ws with caller
+    scratch.  A (passes+1)-pass call and a 1-pass call are timed with CUDA
+    events; their difference per pass removes the call's setup.  Returns
+    (pairs per pass, seconds per pass, passes run in the long call)."""
+    import torch
+    from ridgedetection_b200 import _lib as L
+    lib = L.lib()
+    n, dim = dP.shape
+    st = torch.cuda.current_stream()
+    vs = ctypes.c_void_p(st.cuda_stream)
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    dS = torch.empty_like(dP)
+    tb = ctypes.c_size_t(0)
+    ns = ctypes.c_int64(0)
+    L.check(lib.rd_choose_ws(dim, vp(dP), n, 0, 0, r1, None, 0, 0, None, None, ctypes.byref(tb), vs))
+    ws = torch.empty(tb.value, dtype=torch.uint8, device=dP.device)
+    L.check(lib.rd_choose_ws(dim, vp(dP), n, 0, 0, r1, vp(dS), 0, 0, ctypes.byref(ns), vp(ws),
+                             ctypes.byref(tb), vs))
+    S0 = dS[: ns.value].clone()
+    L.check(lib.rd_evolve_ws(dim, vp(dP), n, 0, 0, None, 0, 0, 0, vp(S0), ns.value, 0, 0, r1, passes + 1,
+                             None, None, None, ctypes.byref(tb), vs))
+    ws = torch.empty(tb.value, dtype=torch.uint8, device=dP.device)
+    times = {}
+    ran = ctypes.c_int64(0)
+    for k in (1, passes + 1, 1, passes + 1):
+        S = S0.clone()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        L.check(lib.rd_evolve_ws(dim, vp(dP), n, 0, 0, None, 0, 0, 0, vp(S), ns.value, 0, 0, r1, k,
+                                 ctypes.byref(ran), None, vp(ws), ctypes.byref(tb), vs))
+        b.record(st)
+        b.synchronize()
+        times[k] = (a.elapsed_time(b), ran.value)   # the second round (warm) is kept
+    (t1, p1), (tk, pk) = times[1], times[passes + 1]
+    per_pass_s = max(1e-9, (tk - t1) * 1e-3 / max(1, pk - p1))
+    return float(n) * ns.value, per_pass_s, pk
 
 
 def measured_hbm_gbs():
@@ -779,9 +832,10 @@ def run_b200_batch(args, world, rank, local, embedded=False):
             "e2e": {"value": n_all / (ms_e2e * 1e-3), "unit": "solves/s",
                     "h2d_bytes_per_step": int(packed.nbytes), "d2h_bytes_per_step": d2h},
             # per loop iteration: assign, key histogram (culled), two chunk
-            # scans, key bases, scatter, sum+shift, control, decimate, loop
-            # condition; per run about 32 more (reset, choose, spatial order)
-            "gpu_launches": args.steps * ((10 if rdb.get_assign_cull() else 9) * stb.loop_iters + 32),
+            # scans, key bases, scatter, sum+shift (with the control step),
+            # decimate, loop condition; per run about 32 more (reset, choose,
+            # spatial order)
+            "gpu_launches": args.steps * ((9 if rdb.get_assign_cull() else 8) * stb.loop_iters + 32),
             "clocks": clocks,
             "cpu_baseline": cpu,
         }

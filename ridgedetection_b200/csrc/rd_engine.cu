@@ -496,11 +496,14 @@ int Engine::run(cudaStream_t st, bool use_graph, int mode)
         if (rounds) {
             RD_CK(bHash_.ensure(4 * (size_t)choose_hash_buckets()));
             RD_CK(bSurv_.ensure((size_t)h_cl_[0].n_own + 16));
+            RD_CK(bSel_.ensure(4 * (size_t)(h_cl_[0].n_own + 2)));
+            RD_CK(bSelTmp_.ensure(choose_select_scratch_bytes(h_cl_[0].n_own)));
         }
         EngineView v0 = view();
         RD_CK(launch_reset(v0, st));
         if (rounds)
-            RD_CK(launch_choose_rounds(dim_, v0, 0, h_cl_[0].n_own, bSurv_.as<uint8_t>(), st));
+            RD_CK(launch_choose_rounds(dim_, v0, 0, h_cl_[0].n_own, bSurv_.as<uint8_t>(),
+                                       bSel_.as<int32_t>(), bSelTmp_.p, bSelTmp_.bytes, st));
         else
             RD_CK(launch_choose(dim_, v0, st));
         if (mode == RUN_CHOOSE_ONLY) {
@@ -611,6 +614,8 @@ int Engine::plan_workspace(int mode)
         if (h_cl_.size() == 1 && h_cl_[0].n_own >= (1 << 16)) {
             RD_CK(bHash_.ensure(4 * (size_t)choose_hash_buckets()));
             RD_CK(bSurv_.ensure((size_t)h_cl_[0].n_own + 16));
+            RD_CK(bSel_.ensure(4 * (size_t)(h_cl_[0].n_own + 2)));
+            RD_CK(bSelTmp_.ensure(choose_select_scratch_bytes(h_cl_[0].n_own)));
         }
         return 0;
     }

@@ -56,7 +56,8 @@ enum : int {
     CTR_NREADY = 5,    // groups ready for decimation in this iteration
     CTR_NBIG = 6,      // keys in the big-key list of the current pass
     CTR_TILE_HEAVY = 7,// heavy-tile ticket of the cluster tile kernel
-    CTR_COUNT = 8,
+    CTR_SUM_DONE = 8,  // CTAs of k_sum_shift finished (the last one runs the control step)
+    CTR_COUNT = 9,
 };
 
 struct EngineView {
@@ -161,7 +162,10 @@ TileClusterParams tile_cluster_defaults();
 // choose of one large cloud c (n own points) in GPU-wide rounds; v.hash must
 // hold choose_hash_buckets() ints and surv n bytes
 cudaError_t launch_choose_rounds(int dim, const EngineView& v, int c, int n, uint8_t* surv,
-                                 cudaStream_t st);
+                                 int32_t* sel, void* tmp, size_t tmp_bytes, cudaStream_t st);
+// scratch of the survivor compaction of launch_choose_rounds for n points;
+// sel holds n + 1 ints (the list, then its length)
+size_t choose_select_scratch_bytes(int64_t n);
 int choose_hash_buckets();
 cudaError_t prepare_pass(int dim, const EngineView& v, const TuneParams& tp);
 // a0/a1 (optional) are recorded on `st` right before and after the assign kernel

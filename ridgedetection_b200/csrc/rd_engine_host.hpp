@@ -174,6 +174,7 @@ private:
     bool spatial_ok_ = false;     // the batch layout allows the spatial order
     DevBuf bPs_, bSorder_, bSpatialTmp_;
     DevBuf bTileOrder_;
+    DevBuf bSel_, bSelTmp_;       // GPU-wide choose: survivor list and its compaction scratch
     std::vector<int32_t> h_tile_order_;
     int n_heavy_ = 0;
     int tile_cl_grid_ = 0;

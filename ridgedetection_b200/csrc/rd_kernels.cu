@@ -13,6 +13,7 @@
 #include "rd_segfold.cuh"
 
 #include <cuda_runtime.h>
+#include <cub/cub.cuh>
 
 #include <algorithm>
 #include <atomic>
@@ -22,11 +23,11 @@ namespace rdb {
 
 namespace {
 
-// members from which a key is folded by a whole CTA of k_sum_shift (seven
-// warps gather, one warp runs the add chain) instead of by one warp -- while
-// the pass has at most two such keys per big-key CTA.  A CTA folds a key
-// about 2.5x sooner than a warp but takes 8 warps, so with many big keys (a
-// batch of large clouds) the per-warp folds finish first.
+// members from which a key is folded by a whole CTA of k_sum_shift (the
+// warp-segmented exact fold of rd_segfold.cuh) instead of by one warp's add
+// chain -- while the pass has at most two such keys per big-key CTA; with more
+// (a batch of large clouds) every key is folded by a warp, which keeps all
+// SMs busy.
 constexpr int SUM_BIG_MIN = 2048;
 constexpr int SUM_BIG_PER_CTA = 2;
 
@@ -209,10 +210,10 @@ __global__ void __launch_bounds__(BLOCK) k_choose(EngineView v)
 // choose for one large cloud, in rounds over growing ranges [a, b) of its
 // points (same semantics as k_choose).  k_choose_filter, spread over the whole
 // GPU, drops every point of the range that has a point chosen in earlier rounds
-// within r1 (hash grid read from global memory); k_choose_resolve, one CTA,
-// walks the survivors in order and applies the sequential greedy rule with a
-// shared-memory mirror of the grid, then writes the grid back for the next
-// round's filter.
+// within r1 (hash grid read from global memory); a stable compaction lists the
+// survivors in order; k_choose_resolve, one CTA, walks that list and applies
+// the sequential greedy rule with a shared-memory mirror of the grid, then
+// writes the grid back for the next round's filter.
 // ---------------------------------------------------------------------------
 template <int DIM>
 __global__ void __launch_bounds__(256) k_choose_filter(EngineView v, int c, int a, int b,
@@ -251,9 +252,12 @@ __global__ void __launch_bounds__(256) k_choose_filter(EngineView v, int c, int 
     }
 }
 
+// sel: the survivors of [a, b) in order, *nsel of them (nullptr in the first
+// round, where every point of the range is a candidate)
 template <int DIM, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_choose_resolve(EngineView v, int c, int a, int b,
-                                                          const uint8_t* __restrict__ surv,
+                                                          const int32_t* __restrict__ sel,
+                                                          const int32_t* __restrict__ nsel,
                                                           int first)
 {
     using CS = ChooseSmem<DIM>;
@@ -286,9 +290,11 @@ __global__ void __launch_bounds__(BLOCK) k_choose_resolve(EngineView v, int c, i
         return (q < CS::SCAP) ? s_S[q * DIM + d] : gS[(int64_t)q * DIM + d];
     };
     auto nxt = [&](int q) -> int { return (q < CS::SCAP) ? s_next[q] : gnext[q]; };
-    for (int base = a; base < b; base += BLOCK) {
-        const int i = base + tid;
-        const bool f = (i < b) && surv[i - a];
+    const int cnt = sel ? *nsel : (b - a);
+    for (int base = 0; base < cnt; base += BLOCK) {
+        const int j = base + tid;
+        const bool f = j < cnt;
+        const int i = f ? (sel ? sel[j] : a + j) : -1;
         if (!__syncthreads_or(f)) continue;
         const unsigned bal = __ballot_sync(FULL, f);
         if (lane == 0) s_wsum[warp] = __popc(bal);
@@ -983,44 +989,60 @@ constexpr int SUM_BP_WIDE = 256;
 // assignment (placement) loop
 constexpr int TILE_PPL = 8;
 // members from which the fused tile kernel folds a key with the whole CTA
-// (exact parallel evaluation, rd_fold.cuh) instead of one warp's add chain
+// (warp-segmented exact evaluation, rd_segfold.cuh) instead of one warp's add
+// chain
 constexpr int FOLD_CTA_MIN = 4096;
-// members per shared-memory buffer of a CTA-folded key (two buffers)
-constexpr int SB_CHUNK = 1024;
 
 template <int DIM>
 __device__ void sum_shift_one(const EngineView& v, int c, int k, float* buf, int* sidx, int lane,
                               bool cta_big);
 
 template <int DIM>
-__device__ void sum_shift_big_one(const EngineView& v, int slot, float (*s_x)[SB_CHUNK * DIM]);
+__device__ void sum_shift_big_one(const EngineView& v, int slot, SegFoldSmem<8, DIM>& sm);
+
+// the per-cloud control step after a pass (k_control), over clouds first,
+// first + stride, ... of the active list
+__device__ void control_clouds(const EngineView& v, const int first, const int stride);
 
 // grid = big_ctas CTAs for the listed big keys (one key at a time each), then
 // the CTAs whose warps take one smaller key each
+// with_control: the last CTA to finish runs the control step of k_control
+// (the moved flags of every fold are then complete)
 template <int DIM>
-__global__ void __launch_bounds__(256) k_sum_shift(EngineView v, int big_ctas)
+__global__ void __launch_bounds__(256) k_sum_shift(EngineView v, int big_ctas, int with_control)
 {
     __shared__ __align__(16) unsigned char s_raw[8 * SUM_BP_WIDE * (DIM + 1) * 4];
+    __shared__ int s_last;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nbig = v.ctr[CTR_NBIG];
     const bool cta_big = nbig <= SUM_BIG_PER_CTA * big_ctas;  // else every key goes to a warp
     if ((int)blockIdx.x < big_ctas) {
-        static_assert(2 * SB_CHUNK * DIM <= 8 * SUM_BP_WIDE * (DIM + 1), "big-key buffers");
-        float (*s_x)[SB_CHUNK * DIM] = reinterpret_cast<float (*)[SB_CHUNK * DIM]>(s_raw);
+        static_assert(sizeof(SegFoldSmem<8, DIM>) <= sizeof(s_raw), "big-key fold scratch");
+        SegFoldSmem<8, DIM>& sm = *reinterpret_cast<SegFoldSmem<8, DIM>*>(s_raw);
         if (cta_big)
-            for (int i = blockIdx.x; i < nbig; i += big_ctas) sum_shift_big_one<DIM>(v, v.big[i], s_x);
-        return;
+            for (int i = blockIdx.x; i < nbig; i += big_ctas) sum_shift_big_one<DIM>(v, v.big[i], sm);
+    } else {
+        float* s_buf = reinterpret_cast<float*>(s_raw) + warp * SUM_BP_WIDE * DIM;
+        int* s_idx = reinterpret_cast<int*>(s_raw + 8 * SUM_BP_WIDE * DIM * 4) + warp * SUM_BP_WIDE;
+        const ActiveList al(v, ACT_SLOT);
+        const int b = (int)blockIdx.x - big_ctas, nb = (int)gridDim.x - big_ctas;
+        for (int t = b * 8 + warp; t < al.total; t += nb * 8) {
+            __syncwarp();
+            int c, k;
+            al.locate(t, c, k);
+            sum_shift_one<DIM>(v, c, k, s_buf, s_idx, lane, cta_big);
+        }
     }
-    float* s_buf = reinterpret_cast<float*>(s_raw) + warp * SUM_BP_WIDE * DIM;
-    int* s_idx = reinterpret_cast<int*>(s_raw + 8 * SUM_BP_WIDE * DIM * 4) + warp * SUM_BP_WIDE;
-    const ActiveList al(v, ACT_SLOT);
-    const int b = (int)blockIdx.x - big_ctas, nb = (int)gridDim.x - big_ctas;
-    for (int t = b * 8 + warp; t < al.total; t += nb * 8) {
-        __syncwarp();
-        int c, k;
-        al.locate(t, c, k);
-        sum_shift_one<DIM>(v, c, k, s_buf, s_idx, lane, cta_big);
-    }
+    if (!with_control) return;
+    // every thread's writes (chosen points, moved flags) before the count
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(&v.ctr[CTR_SUM_DONE], 1) == (int)gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    control_clouds(v, threadIdx.x, blockDim.x);
+    if (threadIdx.x == 0) v.ctr[CTR_SUM_DONE] = 0;
 }
 
 // Sequential FP32 fold, in list order, of the points P[perm[0..n)] (one warp;
@@ -1126,62 +1148,22 @@ __device__ void sum_shift_one(const EngineView& v, int c, int k, float* buf, int
 // folds the other with the same chain of rounded adds (lane d: coordinate
 // d), so the gathers of a large cluster no longer stall its add chain.
 // ---------------------------------------------------------------------------
+// One big key folded by the whole CTA: the warp-segmented exact fold of
+// rd_segfold.cuh (eight warp segments from speculative starts, traces replayed
+// from the exact start), then the shift.
 template <int DIM>
-__device__ void sum_shift_big_one(const EngineView& v, int slot, float (*s_x)[SB_CHUNK * DIM])
+__device__ void sum_shift_big_one(const EngineView& v, int slot, SegFoldSmem<8, DIM>& sm)
 {
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int c = v.slot_cloud[slot];
     const CloudDesc cd = v.cl[c];
     const int k = (int)(slot - cd.key_off);
     const int n = v.cnt[slot];
     const int32_t* mp = v.perm + cd.p_off + v.base[slot];
     const float* Pc = v.P + cd.p_off * DIM;
-    const int nchunk = (n + SB_CHUNK - 1) / SB_CHUNK;
-    auto gather = [&](int ch, float* dst) {  // warps 1..7
-        const int off = ch * SB_CHUNK;
-        const int m = min(SB_CHUNK, n - off);
-        for (int j0 = tid - 32; j0 < m; j0 += 224 * 4) {
-            int ix[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int j = j0 + u * 224;
-                ix[u] = (j < m) ? mp[off + j] : 0;
-            }
-            float x[4][DIM];
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-#pragma unroll
-                for (int d = 0; d < DIM; ++d)
-                    x[u][d] = (j0 + u * 224 < m) ? Pc[(int64_t)ix[u] * DIM + d] : 0.0f;
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int j = j0 + u * 224;
-                if (j < m)
-#pragma unroll
-                    for (int d = 0; d < DIM; ++d) dst[j * DIM + d] = x[u][d];
-            }
-        }
-    };
-    __syncthreads();  // the previous key's buffers are no longer read
-    if (warp > 0) gather(0, s_x[0]);
-    __syncthreads();
-    float sum = 0.0f;
-    for (int ch = 0; ch < nchunk; ++ch) {
-        if (warp > 0) {
-            if (ch + 1 < nchunk) gather(ch + 1, s_x[(ch + 1) & 1]);
-        } else if (lane < DIM) {
-            const float* x = s_x[ch & 1];
-            const int m = min(SB_CHUNK, n - ch * SB_CHUNK);
-            if (m == SB_CHUNK) {
-#pragma unroll 32
-                for (int j = 0; j < SB_CHUNK; ++j) sum = __fadd_rn(sum, x[j * DIM + lane]);
-            } else {
-                for (int j = 0; j < m; ++j) sum = __fadd_rn(sum, x[j * DIM + lane]);
-            }
-        }
-        __syncthreads();
-    }
-    if (warp == 0) apply_shift<DIM>(v, c, cd, k, n, sum, lane);
+    __syncthreads();  // the previous key's scratch is no longer read
+    fold_members_seg<8, DIM>(mp, n, Pc, sm);
+    if (warp == 0) apply_shift<DIM>(v, c, cd, k, n, (lane < DIM) ? sm.out[lane] : 0.0f, lane);
 }
 
 // ---------------------------------------------------------------------------
@@ -1497,10 +1479,10 @@ namespace {
 // ---------------------------------------------------------------------------
 // control: one thread per cloud after each pass.
 // ---------------------------------------------------------------------------
-__global__ void k_control(EngineView v)
+__device__ void control_clouds(const EngineView& v, const int first, const int stride)
 {
     const int nact = v.ctr[CTR_NACT];
-    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nact; a += gridDim.x * blockDim.x) {
+    for (int a = first; a < nact; a += stride) {
         const int c = v.act_cloud[a];
         const CloudDesc cd = v.cl[c];
         v.pairs[c] += (unsigned long long)cd.n_all * (unsigned long long)v.ns[c];
@@ -1524,6 +1506,11 @@ __global__ void k_control(EngineView v)
                 v.ready[atomicAdd(&v.ctr[CTR_NREADY], 1)] = cd.group;
         }
     }
+}
+
+__global__ void k_control(EngineView v)
+{
+    control_clouds(v, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -2065,9 +2052,10 @@ cudaError_t launch_pass_dim(const EngineView& v, const TuneParams& tp, int assig
         // at most (points / SUM_BIG_MIN) keys can be big
         const int big_ctas = (int)std::min<int64_t>(
             ((int64_t)v.n_chunks * v.chunk_pts + SUM_BIG_MIN - 1) / SUM_BIG_MIN, sms);
-        k_sum_shift<DIM><<<big_ctas + std::min((v.n_slots + 7) / 8, sms * 8), 256, 0, st>>>(v, big_ctas);
+        k_sum_shift<DIM><<<big_ctas + std::min((v.n_slots + 7) / 8, sms * 8), 256, 0, st>>>(v, big_ctas, 1);
+    } else {
+        k_control<<<std::min((v.n_clouds + 255) / 256, sms), 256, 0, st>>>(v);
     }
-    k_control<<<std::min((v.n_clouds + 255) / 256, sms), 256, 0, st>>>(v);
     k_decimate<DIM, 512><<<std::min(v.n_groups, sms * 2), 512, dec_smem_bytes(v), st>>>(v);
     return cudaGetLastError();
 }
@@ -2089,7 +2077,7 @@ cudaError_t launch_choose_dim(const EngineView& v, cudaStream_t st)
 // surv (n bytes)
 template <int DIM>
 cudaError_t launch_choose_rounds_dim(const EngineView& v, int c, int n, uint8_t* surv,
-                                     cudaStream_t st)
+                                     int32_t* sel, void* tmp, size_t tmp_bytes, cudaStream_t st)
 {
     using CS = ChooseSmem<DIM>;
     constexpr int B = 1024;
@@ -2098,16 +2086,20 @@ cudaError_t launch_choose_rounds_dim(const EngineView& v, int c, int n, uint8_t*
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return e;
     int a = 0, size = 4096, first = 1;
+    int32_t* nsel = sel + n;
     while (a < n) {
         const int b = (int)std::min<int64_t>((int64_t)n, (int64_t)a + size);
         if (first) {
-            e = cudaMemsetAsync(surv, 1, (size_t)(b - a), st);
-            if (e != cudaSuccess) return e;
+            k_choose_resolve<DIM, B><<<1, B, bytes, st>>>(v, c, a, b, nullptr, nullptr, first);
         } else {
             const int grid = std::max(1, std::min((b - a + 255) / 256, 148 * 16));
             k_choose_filter<DIM><<<grid, 256, 0, st>>>(v, c, a, b, surv);
+            size_t tb = tmp_bytes;
+            e = cub::DeviceSelect::Flagged(tmp, tb, cub::CountingInputIterator<int32_t>(a), surv, sel,
+                                           nsel, b - a, st);
+            if (e != cudaSuccess) return e;
+            k_choose_resolve<DIM, B><<<1, B, bytes, st>>>(v, c, a, b, sel, nsel, first);
         }
-        k_choose_resolve<DIM, B><<<1, B, bytes, st>>>(v, c, a, b, surv, first);
         a = b;
         size = (int)std::min<int64_t>((int64_t)size * 2, 1 << 30);
         first = 0;
@@ -2118,14 +2110,22 @@ cudaError_t launch_choose_rounds_dim(const EngineView& v, int c, int n, uint8_t*
 }  // namespace
 
 cudaError_t launch_choose_rounds(int dim, const EngineView& v, int c, int n, uint8_t* surv,
-                                 cudaStream_t st)
+                                 int32_t* sel, void* tmp, size_t tmp_bytes, cudaStream_t st)
 {
     return with_dim(dim, [&](auto D) {
-        return launch_choose_rounds_dim<decltype(D)::value>(v, c, n, surv, st);
+        return launch_choose_rounds_dim<decltype(D)::value>(v, c, n, surv, sel, tmp, tmp_bytes, st);
     });
 }
 
 int choose_hash_buckets() { return ChooseSmem<2>::HB; }
+
+size_t choose_select_scratch_bytes(int64_t n)
+{
+    size_t tb = 0;
+    cub::DeviceSelect::Flagged(nullptr, tb, cub::CountingInputIterator<int32_t>(0), (const uint8_t*)nullptr,
+                               (int32_t*)nullptr, (int32_t*)nullptr, (int)std::max<int64_t>(n, 1));
+    return tb + 256;
+}
 
 cudaError_t launch_choose(int dim, const EngineView& v, cudaStream_t st)
 {
@@ -2331,7 +2331,7 @@ cudaError_t launch_evolve_step_dim(const EngineView& v, const TuneParams& tp, in
         // at most (points / SUM_BIG_MIN) keys can be big
         const int big_ctas = (int)std::min<int64_t>(
             ((int64_t)v.n_chunks * v.chunk_pts + SUM_BIG_MIN - 1) / SUM_BIG_MIN, sms);
-        k_sum_shift<DIM><<<big_ctas + std::min((v.n_slots + 7) / 8, sms * 8), 256, 0, st>>>(v, big_ctas);
+        k_sum_shift<DIM><<<big_ctas + std::min((v.n_slots + 7) / 8, sms * 8), 256, 0, st>>>(v, big_ctas, 0);
     }
     return cudaGetLastError();
 }
