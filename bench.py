@@ -444,7 +444,7 @@ def run_b200_bf(args, world, rank, local):
                    "loop": "CUDA graph WHILE node", "parallelism": f"replicas x{world}",
                    "assign": "culled (exact chunk-box culling)" if culled else "all pairs",
                    "assign_shape": {"block": tb, "items": ti, "cull_items": tci,
-                                    "source": "rd_autotune (median of 5 runs per shape)",
+                                    "source": "rd_autotune (whole evolve passes timed, median of 5 runs per shape)",
                                     "tuned_us_per_pass": tus}},
         "solves_per_s": world * 1e3 / ms_max,
         "pairs_per_step": pairs_step, "loop_iters_per_step": iters_step,
@@ -453,11 +453,11 @@ def run_b200_bf(args, world, rank, local):
         "all_pairs": all_pairs,
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(P.nbytes),
                 "d2h_bytes_per_step": int(ns_final * dim * 4)},
-        # per loop iteration: assign, key histogram (culled), chunk scan, key
-        # bases, scatter, sum+shift (with the control step), decimate, loop
-        # condition; per solve about 40 more (reset, choose rounds with their
-        # survivor compaction, spatial order)
-        "gpu_launches": args.steps * ((8 if culled else 7) * iters_step + 40),
+        # per loop iteration: assign (culled: with the key histogram), chunk
+        # scan (with the key bases), scatter, sum+shift (with the control
+        # step), decimate (with the loop condition); per solve about 40 more
+        # (reset, choose rounds with their survivor compaction, spatial order)
+        "gpu_launches": args.steps * (5 * iters_step + 40),
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
@@ -670,7 +670,10 @@ def run_b200_tiled(args, world, rank, local, embedded=False):
                      "launches": pst.assign_launches, "traffic": None},
         "e2e": {"value": world * n / (e2e_ms * 1e-3), "unit": "points/s",
                 "h2d_bytes_per_step": int(P.nbytes), "d2h_bytes_per_step": int(ns_final * dim * 4)},
-        "gpu_launches": args.steps * (12 + 10 * max(1, st.loop_iters)),
+        # per loop iteration: tile evolve, seven neighbour-list kernels of the
+        # global decimation, decimate (with the loop condition); per solve
+        # about 12 more (tile build, reset, choose)
+        "gpu_launches": args.steps * (12 + 9 * max(1, st.loop_iters)),
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
@@ -831,11 +834,11 @@ def run_b200_batch(args, world, rank, local, embedded=False):
             "pairs_per_step_rank0": stb.pairs, "loop_iters_rank0": stb.loop_iters,
             "e2e": {"value": n_all / (ms_e2e * 1e-3), "unit": "solves/s",
                     "h2d_bytes_per_step": int(packed.nbytes), "d2h_bytes_per_step": d2h},
-            # per loop iteration: assign, key histogram (culled), two chunk
-            # scans, key bases, scatter, sum+shift (with the control step),
-            # decimate, loop condition; per run about 32 more (reset, choose,
-            # spatial order)
-            "gpu_launches": args.steps * ((9 if rdb.get_assign_cull() else 8) * stb.loop_iters + 32),
+            # per loop iteration: assign (culled: with the key histogram), two
+            # chunk scans (with the key bases), scatter, sum+shift (with the
+            # control step), decimate (with the loop condition); per run about
+            # 32 more (reset, choose, spatial order)
+            "gpu_launches": args.steps * (6 * stb.loop_iters + 32),
             "clocks": clocks,
             "cpu_baseline": cpu,
         }

@@ -115,13 +115,14 @@ RD_API rd_status rd_get_tile_clusters(int* enable, int64_t* min_points, int64_t*
 /* Times the supported shapes of the assignment the run would use (culled or
  * all pairs, rd_get_assign_cull) on the cloud d_P (device, n x dim ROW_MAJOR;
  * NULL = n synthetic points uniform in the unit cube) with its first ns points
- * as the chosen set and radius r1: `reps` evolve passes per run, timed whole
- * with CUDA events; five runs per shape, interleaved over the shapes; the
- * shape with the lowest median time per pass wins -- unless the table already
- * holds a shape for this (dim, n, r1) bucket that is within 3% of it, which
- * is kept.  Stores the pick for the bucket and returns it with its median time
- * per pass in microseconds.  Runs on `stream` and waits for it; d_P is not
- * modified. */
+ * as the chosen set and radius r1: CUDA events around each of `reps` evolve
+ * passes (the shape sets the assignment's launch and the chunking of the
+ * grouping that follows it; the run's one-time setup is left out); five runs
+ * per shape, interleaved over the shapes; the shape with the lowest median
+ * time per pass wins -- unless the table already holds a shape for this (dim,
+ * n, r1) bucket that is within 3% of it, which is kept.  Stores the pick for
+ * the bucket and returns it with its median time per pass in microseconds.
+ * Runs on `stream` and waits for it; d_P is not modified. */
 RD_API rd_status rd_autotune(int dim, const float* d_P, int64_t n, int64_t ns, float r1, int reps,
                              int* block, int* items, int* cull_items, double* us_per_pass,
                              void* stream);

@@ -382,7 +382,8 @@ def autotune(dim: int, n: int, ns: int, reps: int = 5, points=None,
              r1: float = 2.0) -> Tuple[int, int, int, float]:
     """Time the supported shapes of the assignment in use and keep the best
     (median of five runs, the incumbent kept within 3%) for the (dim, size,
-    r1) bucket; returns (block, items, cull_items, microseconds per pass).
+    r1) bucket; returns (block, items, cull_items, microseconds per
+    evolve pass).
     With ``points`` (a float32 CUDA tensor, n x dim) the timing runs on that
     cloud with its first ``ns`` points as the chosen set and radius ``r1``;
     otherwise on ``n`` synthetic uniform points."""

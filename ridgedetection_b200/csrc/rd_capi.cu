@@ -348,39 +348,33 @@ rd_status rd_autotune(int dim, const float* d_P, int64_t n, int64_t ns, float r1
     const float* src = d_P ? d_P : pts.data();
     const bool culled = assign_cull_enabled();
     const std::vector<TuneParams>& cand = tune_candidates(culled);
-    // Every candidate runs `reps` evolve passes from the same chosen set, the
-    // whole run timed with CUDA events (assignment, grouping and folds: all
-    // that the shape changes); NREP repetitions, interleaved over the
-    // candidates so that clock drift hits them alike; the median decides.
+    // The shape sets the assignment kernel's launch and the chunking of the
+    // grouping kernels that follow it, so whole passes are timed: CUDA events
+    // around each of `reps` evolve passes from the same chosen set (the run's
+    // one-time setup stays out of the figure); NREP runs, interleaved over
+    // the candidates so that clock drift hits them alike; the median of the
+    // per-run means decides.
     constexpr int NREP = 5;
     std::vector<std::vector<float>> ms(cand.size());
-    cudaEvent_t e0, e1;
-    CK_CUDA(cudaEventCreate(&e0));
-    CK_CUDA(cudaEventCreate(&e1));
-    int passes_run = reps;
     for (int rep = 0; rep < NREP; ++rep) {
         for (size_t ci = 0; ci < cand.size(); ++ci) {
             Engine e;
             e.tune = cand[ci];
             e.tune_locked = true;
             e.max_passes = reps;
+            e.profile_pass = true;
             if (rd_status s = one_cloud_engine(e, dim, n, n, r1, r1)) return s;
             CK_CUDA(cudaMemcpyAsync(e.points(), src, sizeof(float) * n * dim, kind, st));
             CK_CUDA(cudaMemcpyAsync(e.chosen_mut(), src, sizeof(float) * ns * dim, kind, st));
             e.given_ns.assign(1, (int32_t)ns);
-            CK_CUDA(cudaEventRecord(e0, st));
             const int rc = e.run(st, false, Engine::RUN_EVOLVE_ONLY);
-            CK_CUDA(cudaEventRecord(e1, st));
             if (rc && rc != RD_ERR_NOT_CONVERGED) return from_engine(rc, e);
-            CK_CUDA(cudaEventSynchronize(e1));
-            float t = 0;
-            CK_CUDA(cudaEventElapsedTime(&t, e0, e1));
-            passes_run = std::max<int>(1, (int)e.stats().total_passes);
-            ms[ci].push_back(t / (float)passes_run);
+            CK_CUDA(cudaStreamSynchronize(st));
+            const RunStats& rs = e.stats();
+            ms[ci].push_back(rs.assign_launches > 0 ? (float)(rs.assign_ms / rs.assign_launches)
+                                                    : 0.0f);
         }
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     auto median = [](std::vector<float> v) {
         std::sort(v.begin(), v.end());
         return v[v.size() / 2];

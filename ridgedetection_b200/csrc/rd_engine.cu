@@ -241,6 +241,7 @@ int Engine::setup(int dim, const std::vector<CloudDesc>& clouds,
     RD_CK(bNext_.ensure(sizeof(int32_t) * (size_t)(s_off + 1)));
     RD_CK(bKeys_.ensure(sizeof(int32_t) * (size_t)(total_points + 1)));
     RD_CK(bGrouped_.ensure(sizeof(int32_t) * (size_t)(total_points + 4)));
+    RD_CK(bPg_.ensure(sizeof(float) * (size_t)(total_points * pad_dim(dim) + 4)));
     RD_CK(bNs_.ensure(4 * (nc + 1)));
     RD_CK(bPhase_.ensure(4 * (nc + 1)));
     RD_CK(bCont_.ensure(4 * (nc + 1)));
@@ -250,6 +251,7 @@ int Engine::setup(int dim, const std::vector<CloudDesc>& clouds,
     RD_CK(bErr_.ensure(4 * (nc + 1)));
     RD_CK(bPairs_.ensure(8 * (nc + 1)));
     RD_CK(bCtr_.ensure(4 * CTR_COUNT));
+    RD_CK(bKbDone_.ensure(4 * (nc + 1)));
     RD_CK(bActCloud_.ensure(4 * (nc + 1)));
     RD_CK(bActPre_.ensure(4 * ACT_KINDS * (nc + 1)));
     RD_CK(bGroupConv_.ensure(4 * (h_gr_.size() + 1)));
@@ -271,10 +273,12 @@ EngineView Engine::view() const
     v.S = bS_.as<float>();
     v.keys = bKeys_.as<int32_t>();
     v.perm = bGrouped_.as<int32_t>();
+    v.Pg = bPg_.as<float>();
     v.hist = bHist_.as<int32_t>();
     v.cnt = bCnt_.as<int32_t>();
     v.base = bBase_.as<int32_t>();
     v.big = bBig_.as<int32_t>();
+    v.kbdone = bKbDone_.as<int32_t>();
     v.next = bNext_.as<int32_t>();
     v.hash = bHash_.as<int32_t>();
     v.ns = bNs_.as<int32_t>();
@@ -363,6 +367,7 @@ int Engine::finish_setup_after_choose(cudaStream_t st)
         for (int k = 0; k < cd.ns_cap; ++k) h_slot_cloud_.push_back((int32_t)c);
     }
     n_slots_ = (int32_t)key;
+    hist_ints_ = hist;
     n_kblk_ = (int32_t)kblk;
     n_kblk_warp_ = (int32_t)kblk_warp;
     // group decimation scratch
@@ -445,13 +450,14 @@ int Engine::build_graph(cudaStream_t st)
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     RD_CK(cudaStreamBeginCaptureToGraph(cap_stream_, body, nullptr, nullptr, 0,
                                         cudaStreamCaptureModeThreadLocal));
-    cudaError_t e1 = fused_ ? launch_tile_pass(dim_, v, cap_stream_)
-                            : launch_pass(dim_, v, tune, assign_grid_, cap_stream_);
-    cudaError_t e2 = launch_loopcond(v, h, 1, cap_stream_);
+    LoopCond lc;
+    lc.h = h;
+    lc.use_handle = 1;
+    cudaError_t e1 = fused_ ? launch_tile_pass(dim_, v, lc, cap_stream_)
+                            : launch_pass(dim_, v, tune, assign_grid_, lc, cap_stream_);
     cudaGraph_t out = nullptr;
     cudaError_t e3 = cudaStreamEndCapture(cap_stream_, &out);
     if (e1 != cudaSuccess) return fail("capture pass", e1);
-    if (e2 != cudaSuccess) return fail("capture loopcond", e2);
     if (e3 != cudaSuccess) return fail("end capture", e3);
     RD_CK(cudaGraphInstantiate(&exec_, graph_, 0));
     graph_key_ = key;
@@ -525,12 +531,15 @@ int Engine::run(cudaStream_t st, bool use_graph, int mode)
     cull_ = cull_assign && assign_cull_enabled() && !fused_ && spatial_ok_ && total_points_ > 0;
     if (cull_) {
         const size_t scratch = spatial_prep_scratch_bytes(total_points_);
-        RD_CK(bPs_.ensure(sizeof(float) * (size_t)(total_points_ * dim_ + 4)));
+        RD_CK(bPs_.ensure(sizeof(float) * (size_t)(total_points_ * pad_dim(dim_) + 4)));
         RD_CK(bSorder_.ensure(sizeof(int32_t) * (size_t)(total_points_ + 1)));
         RD_CK(bSpatialTmp_.ensure(scratch));
         const EngineView vs = view();
         RD_CK(launch_spatial_prep(dim_, vs, total_points_, bSpatialTmp_.p, scratch, bPs_.as<float>(),
                                   bSorder_.as<int32_t>(), st));
+        // the culled assignment adds its counts into the histogram rows, which
+        // k_scatter_cta zeroes again after every pass
+        RD_CK(cudaMemsetAsync(bHist_.p, 0, 4 * (size_t)(hist_ints_ + 1), st));
     }
     tile_cl_grid_ = 0;
     if (fused_) RD_CK(prepare_tile_pass(dim_, view(), &tile_cl_grid_));
@@ -543,16 +552,21 @@ int Engine::run(cudaStream_t st, bool use_graph, int mode)
         RD_CK(cudaGraphLaunch(exec_, st));
     } else {
         cudaEvent_t a0 = nullptr, a1 = nullptr;
-        if (profile_assign) {
+        if (profile_assign || profile_pass) {
             RD_CK(cudaEventCreate(&a0));
             RD_CK(cudaEventCreate(&a1));
         }
         stats_.assign_ms = 0;
         stats_.assign_launches = 0;
         for (;;) {
-            if (fused_) RD_CK(launch_tile_pass(dim_, v, st, a0, a1));
-            else RD_CK(launch_pass(dim_, v, tune, assign_grid_, st, a0, a1));
-            RD_CK(launch_loopcond(v, cudaGraphConditionalHandle(), 0, st));
+            // profile_pass: the events bracket the whole iteration instead of
+            // the assignment kernel
+            cudaEvent_t k0 = profile_pass ? nullptr : a0, k1 = profile_pass ? nullptr : a1;
+            if (profile_pass) RD_CK(cudaEventRecord(a0, st));
+            const LoopCond lc;  // no handle: the count is read below
+            if (fused_) RD_CK(launch_tile_pass(dim_, v, lc, st, k0, k1));
+            else RD_CK(launch_pass(dim_, v, tune, assign_grid_, lc, st, k0, k1));
+            if (profile_pass) RD_CK(cudaEventRecord(a1, st));
             int32_t act = 0;
             RD_CK(cudaMemcpyAsync(&act, v.ctr + CTR_ACTIVE, 4, cudaMemcpyDeviceToHost, st));
             RD_CK(cudaStreamSynchronize(st));
@@ -604,7 +618,7 @@ int Engine::plan_workspace(int mode)
         if (int rc = finish_setup_after_choose(nullptr)) return rc;
         if (mode == RUN_EVOLVE_ONLY && cull_assign && assign_cull_enabled() && spatial_ok_ &&
             total_points_ > 0) {
-            RD_CK(bPs_.ensure(sizeof(float) * (size_t)(total_points_ * dim_ + 4)));
+            RD_CK(bPs_.ensure(sizeof(float) * (size_t)(total_points_ * pad_dim(dim_) + 4)));
             RD_CK(bSorder_.ensure(sizeof(int32_t) * (size_t)(total_points_ + 1)));
             RD_CK(bSpatialTmp_.ensure(spatial_prep_scratch_bytes(total_points_)));
         }

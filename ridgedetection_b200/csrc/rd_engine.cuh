@@ -57,7 +57,8 @@ enum : int {
     CTR_NBIG = 6,      // keys in the big-key list of the current pass
     CTR_TILE_HEAVY = 7,// heavy-tile ticket of the cluster tile kernel
     CTR_SUM_DONE = 8,  // CTAs of k_sum_shift finished (the last one runs the control step)
-    CTR_COUNT = 9,
+    CTR_DEC_DONE = 9,  // CTAs of k_decimate finished (the last one sets the loop condition)
+    CTR_COUNT = 10,
 };
 
 struct EngineView {
@@ -69,10 +70,14 @@ struct EngineView {
     float* S;                    // chosen points, ROW_MAJOR, capacity n_own per cloud
     int32_t* keys;               // per point slot: assigned chosen index or -1
     int32_t* perm;               // per point slot: point indices grouped by key, index order
+                                 // (tiled kernels)
+    float* Pg;                   // per point slot: the points' coordinates grouped by key in
+                                 // index order, PadDim floats each (lockstep passes)
     int32_t* hist;               // per cloud: n_chunks x ns_cap key histogram (then its prefix over chunks)
     int32_t* cnt;                // per chosen slot: members in the last pass
     int32_t* base;               // per chosen slot: first slot of its segment of perm
     int32_t* big;                // chosen slots with SUM_BIG_MIN+ members in this pass
+    int32_t* kbdone;             // per cloud: key blocks of the chunk scan finished in this pass
     int32_t* hash;               // choose hash heads
     int32_t* next;               // per chosen slot: choose hash chain
     int32_t* ns;                 // per cloud: current chosen count
@@ -168,11 +173,22 @@ cudaError_t launch_choose_rounds(int dim, const EngineView& v, int c, int n, uin
 size_t choose_select_scratch_bytes(int64_t n);
 int choose_hash_buckets();
 cudaError_t prepare_pass(int dim, const EngineView& v, const TuneParams& tp);
-// a0/a1 (optional) are recorded on `st` right before and after the assign kernel
+// How an iteration ends: the last CTA of its decimation kernel rebuilds the
+// work lists and sets the loop condition (k_loopcond's step), leaving the
+// count of unfinished clouds in ctr[CTR_ACTIVE] and, with use_handle, setting
+// the graph WHILE handle.
+struct LoopCond {
+    cudaGraphConditionalHandle h = 0;
+    int use_handle = 0;
+};
+// One iteration: evolve pass, control, decimation, loop condition.  a0/a1
+// (optional) are recorded on `st` right before and after the assign kernel.
 cudaError_t launch_pass(int dim, const EngineView& v, const TuneParams& tp, int assign_grid,
-                        cudaStream_t st, cudaEvent_t a0 = nullptr, cudaEvent_t a1 = nullptr);
+                        const LoopCond& lc, cudaStream_t st, cudaEvent_t a0 = nullptr,
+                        cudaEvent_t a1 = nullptr);
 // Sets the loop condition and rebuilds the work lists of the next iteration
-// (count_iter = 0 for the initial build before the first iteration).
+// as a kernel of its own (count_iter = 0 for the initial build before the
+// first iteration).
 cudaError_t launch_loopcond(const EngineView& v, cudaGraphConditionalHandle h, int use_handle,
                             cudaStream_t st, int count_iter = 1);
 cudaError_t launch_reset(const EngineView& v, cudaStream_t st);
@@ -181,8 +197,9 @@ cudaError_t launch_set_given(const EngineView& v, int queue_decimation, cudaStre
 // fused per-tile evolve (every active cloud to convergence, one CTA each) +
 // decimation of the groups that became ready; needs every ns <= TILE_NS_MAX
 cudaError_t prepare_tile_pass(int dim, const EngineView& v, int* cl_grid);
-// a0/a1 (optional) are recorded right before and after the tile-evolve kernel
-cudaError_t launch_tile_pass(int dim, const EngineView& v, cudaStream_t st,
+// a0/a1 (optional) are recorded right before and after the tile-evolve kernel;
+// the iteration ends with the loop condition as in launch_pass
+cudaError_t launch_tile_pass(int dim, const EngineView& v, const LoopCond& lc, cudaStream_t st,
                              cudaEvent_t a0 = nullptr, cudaEvent_t a1 = nullptr);
 cudaError_t launch_decimate(int dim, const EngineView& v, cudaStream_t st);
 // quality metrics (rd_quality.cu)

@@ -51,7 +51,8 @@ struct RunStats {
     int64_t max_passes = 0;       // max over clouds
     double pairs = 0;             // sum over clouds of sum over passes of n_all*ns
     int err_bits = 0;
-    double assign_ms = 0;         // host-loop runs with profile_assign: assign kernel time
+    double assign_ms = 0;         // host-loop runs with profile_assign (profile_pass): time
+                                  // of the assign kernels (of whole iterations)
     int64_t assign_launches = 0;
     double point_passes = 0;      // sum over clouds of n_all * evolve passes
 };
@@ -135,6 +136,8 @@ public:
     TuneParams tune{128, 8};
     bool tune_locked = false;     // keep `tune`; otherwise setup() takes tune_lookup()
     bool profile_assign = false;  // host loop only: time every assign launch with events
+    bool profile_pass = false;    // host loop only: time every whole iteration instead
+                                  // (into assign_ms / assign_launches)
     bool fuse_tiles = true;       // tiled runs: per-tile evolve kernel (see run())
     bool cull_assign = true;      // lockstep passes: exact chunk-box culling of the assignment
     std::string last_error;
@@ -156,6 +159,7 @@ private:
     std::vector<int64_t> h_dec_hoff_;
     std::vector<int32_t> h_dec_hbits_;
     int32_t n_chunks_ = 0, n_slots_ = 0, n_kblk_ = 0, n_kblk_warp_ = 0;
+    int64_t hist_ints_ = 0;  // entries of the chunk x key histogram
     int chunk_pts_ = 1024;
     int chunk_max_ = 0;
     int sms_ = 148;
@@ -164,8 +168,8 @@ private:
     RunStats stats_;
 
     DevBuf bCl_, bGr_, bChunkCloud_, bSlotCloud_;
-    DevBuf bP_, bS_, bKeys_, bGrouped_, bHist_, bCnt_, bBase_, bBig_, bNext_, bHash_, bSurv_;
-    DevBuf bNs_, bPhase_, bCont_, bPasses_, bTotPasses_, bOuter_, bErr_, bPairs_, bCtr_;
+    DevBuf bP_, bS_, bKeys_, bGrouped_, bPg_, bHist_, bCnt_, bBase_, bBig_, bNext_, bHash_, bSurv_;
+    DevBuf bNs_, bPhase_, bCont_, bPasses_, bTotPasses_, bOuter_, bErr_, bPairs_, bCtr_, bKbDone_;
     DevBuf bActCloud_, bActPre_, bGroupConv_, bReady_, bDnbOff_, bDnb_, bDbig_, bDcpre_;
     int dec_smem_max_ = 0;
     int dec_nb_pp_ = DEC_NB_MIN_PER_POINT;

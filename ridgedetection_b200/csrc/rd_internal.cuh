@@ -89,6 +89,11 @@ struct GroupDesc {
     int64_t s_scratch;   // first scratch slot of the group's decimation
 };
 
+// coordinates per point in padded device copies: DIM 3 is stored as float4
+template <int DIM>
+struct PadDim { static constexpr int v = (DIM == 3) ? 4 : DIM; };
+inline int pad_dim(int dim) { return dim == 3 ? 4 : dim; }
+
 constexpr int KBLK = 32;  // chosen points per histogram-scan block (one per lane)
 
 // ---------------------------------------------------------------------------

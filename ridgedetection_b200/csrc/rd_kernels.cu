@@ -365,9 +365,6 @@ __global__ void __launch_bounds__(BLOCK) k_choose_resolve(EngineView v, int c, i
 // histogram row.  This is the hot kernel.
 // ---------------------------------------------------------------------------
 template <int DIM>
-struct PadDim { static constexpr int v = (DIM == 3) ? 4 : DIM; };
-
-template <int DIM>
 __device__ __forceinline__ void load_chosen(const float* sS, int kk, float* s)
 {
     constexpr int DP = PadDim<DIM>::v;
@@ -507,27 +504,40 @@ __global__ void __launch_bounds__(BLOCK) k_assign(EngineView v)
 }
 
 // ---------------------------------------------------------------------------
-// Culled assignment: the same keys as k_assign, over chunks of the spatial
-// order (Ps, built once per run by launch_spatial_prep) instead of the slot
-// order.  Each warp takes 128 consecutive points of that order (4 per lane)
-// and their bounding box; a chosen point s takes part in the warp's argmin
-// only when the squared gap between s and the box, g2, is at most
-// thr = r1^2 (1 + 2^-10) (rounded up).  Exactness: the computed g2 exceeds the
-// exact squared gap G by at most a relative 2^-20 (a few roundings of
-// non-negative terms), and every computed distance from s to a point of the
-// box is at least G (1 - 2^-20); so g2 > thr makes every such distance > r1^2.
-// A skipped chosen point can then neither be the nearest one within r1 nor tie
-// with it, and the minimum over the remaining points, visited in index order
-// with strict '<', is the reference's (rd/cpu/brute_force/evolve.hpp:54-66).
-// The bound needs r1^2 in the normal range; any other r1 disables the skip.
-// NaN gaps never skip.  The chosen points are staged in shared memory in
-// batches of AC_TS.  Keys are written back to the points' slots; k_keyhist
-// then builds the per-chunk histograms in slot order.
+// Culled assignment: the same keys as k_assign, over the spatial order (Ps,
+// built once per run by launch_spatial_prep, DIM padded to PadDim) instead of
+// the slot order.  A work item is a block of AC_BLOCK x AC_ITEMS consecutive
+// points of that order; each warp takes 32 x AC_ITEMS of them and their
+// bounding box.  A chosen point s takes part in a box's argmin only when the
+// squared gap between s and the box, g2, is at most thr = r1^2 (1 + 2^-10)
+// (rounded up).  Exactness: the computed g2 exceeds the exact squared gap G by
+// at most a relative 2^-20 (a few roundings of non-negative terms), and every
+// computed distance from s to a point of the box is at least G (1 - 2^-20);
+// so g2 > thr makes every such distance > r1^2.  A skipped chosen point can
+// then neither be the nearest one within r1 nor tie with it, and the minimum
+// over the remaining points, visited in index order with strict '<', is the
+// reference's (rd/cpu/brute_force/evolve.hpp:54-66).  The bound needs r1^2 in
+// the normal range; any other r1 disables the skip.  NaN gaps never skip.
+//
+// The test runs at two levels.  The CTA's box (the union of its warps' boxes)
+// is tested against every chosen point of the cloud, each thread taking a few
+// of them; the survivors are compacted in index order into a shared list.
+// The argument above holds for any box that contains the points, so a point
+// dropped there is dropped for every warp.  Each warp then tests the short
+// list against its own box and evaluates the distances of the kept chosen
+// points, still in index order.  The chosen points stay staged in shared
+// memory across the CTA's work items while they belong to one cloud of at
+// most AC_TS chosen points.
+//
+// Keys are written back to the points' slots, and each assigned point adds
+// one to its key's entry in the histogram row of its slot-order chunk (the
+// rows k_assign writes itself; k_scatter_cta zeroes them again after use).
 // ---------------------------------------------------------------------------
-constexpr int AC_BLOCK = 256;  // threads of k_assign_cull
-constexpr int AC_TS = 1024;    // chosen points per shared-memory batch
-// points per lane per step (ITEMS, a tuning parameter): a warp's box holds 32 x
-// ITEMS consecutive points of the spatial order
+constexpr int AC_BLOCK = 256;             // threads of k_assign_cull
+constexpr int AC_WARPS = AC_BLOCK / 32;
+constexpr int AC_TS = 1024;               // chosen points per shared-memory batch
+// points per lane (AC_ITEMS, a tuning parameter): a warp's box holds 32 x
+// AC_ITEMS consecutive points of the spatial order
 
 // squared gap between s and the box [lo, hi] (0 inside; NaN-free for NaN s)
 template <int DIM>
@@ -542,149 +552,245 @@ __device__ __forceinline__ float box_gap2(const float* s, const float* lo, const
     return g2;
 }
 
+// slot-order chunk of position i of a cloud of n points in m chunks: the lc
+// with floor(lc n / m) <= i < floor((lc + 1) n / m), i.e. lc n < (i + 1) m <=
+// (lc + 1) n; a float estimate corrected with exact integer products
+__device__ __forceinline__ int slot_chunk(int i, int n, int m, float ratio)
+{
+    int lc = min(max(__float2int_rz(__fmul_rn((float)i, ratio)), 0), m - 1);
+    const int64_t t = (int64_t)(i + 1) * m;
+    while (lc > 0 && (int64_t)lc * n >= t) --lc;
+    while (lc < m - 1 && (int64_t)(lc + 1) * n < t) ++lc;
+    return lc;
+}
+
 template <int DIM, int AC_ITEMS>
 __global__ void __launch_bounds__(AC_BLOCK) k_assign_cull(EngineView v)
 {
     static_assert(AC_ITEMS % 2 == 0, "points are evaluated in pairs");
     constexpr int DP = PadDim<DIM>::v;
     constexpr int WPTS = 32 * AC_ITEMS;
-    __shared__ __align__(16) float sS[AC_TS * DP];
-    __shared__ int s_item;
+    constexpr int SUBPTS = AC_BLOCK * AC_ITEMS;
+    __shared__ __align__(16) float sS[AC_TS * DP];  // staged chosen batch
+    __shared__ int sK[2][AC_TS];                     // CTA survivors: batch positions
+    __shared__ float s_box[2][AC_WARPS][2 * DIM];    // warp boxes
+    __shared__ float s_cbox[2][2 * DIM];             // the CTA's box
+    __shared__ int s_wcnt[2][AC_WARPS];              // survivors per warp range
+    __shared__ int s_item[2];
+    __shared__ int s_staged;                         // cloud whose whole chosen set is in sS
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
     const ActiveList al(v, ACT_CHUNK);
-    for (;;) {
-        if (tid == 0) s_item = atomicAdd(&v.ctr[CTR_WORK], 1);
-        __syncthreads();
-        const int item = s_item;
-        __syncthreads();
-        if (item >= al.total) break;
-        int c, lc;
-        al.locate(item, c, lc);
-        const CloudDesc cd = v.cl[c];
+    const int subs = (v.chunk_pts + SUBPTS - 1) / SUBPTS;
+    const int total = al.total * subs;
+
+    // A work item's cloud, point range and this lane's points with their
+    // slots; the next item's are loaded while the current one is evaluated.
+    struct Item {
+        int c, b0, b1;
+        float p[AC_ITEMS][DIM];
+        int slot[AC_ITEMS];
+    };
+    auto load_item = [&](const int item, Item& t) {
+        t.c = -1;
+        t.b0 = t.b1 = 0;
+#pragma unroll
+        for (int j = 0; j < AC_ITEMS; ++j) {
+            t.slot[j] = -1;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) t.p[j][d] = 0.0f;
+        }
+        if (item >= total) return;
+        int lc;
+        al.locate(item / subs, t.c, lc);
+        const CloudDesc cd = v.cl[t.c];
         const int start = (int)(((int64_t)lc * cd.n_all) / cd.n_chunks);
         const int end = (int)(((int64_t)(lc + 1) * cd.n_all) / cd.n_chunks);
+        t.b0 = start + (item % subs) * SUBPTS;
+        t.b1 = min(end, t.b0 + SUBPTS);
+        const float* Ps = v.Ps + cd.p_off * DP;
+#pragma unroll
+        for (int j = 0; j < AC_ITEMS; ++j) {
+            const int i = t.b0 + warp * WPTS + j * 32 + lane;
+            if (i < t.b1) {
+                load_chosen<DIM>(Ps, i, t.p[j]);
+                t.slot[j] = v.sorder[cd.p_off + i];
+            }
+        }
+    };
+
+    if (tid == 0) {
+        s_item[0] = atomicAdd(&v.ctr[CTR_WORK], 1);
+        s_staged = -1;
+    }
+    __syncthreads();
+    Item cur;
+    load_item(s_item[0], cur);
+    // Shared arrays indexed by `buf` alternate between work items, so a warp
+    // still reading the previous item's list never races the next item's
+    // writes; sS is rewritten only after the barrier that every warp reaches
+    // once it is done with the previous item.
+    for (int it = 0;; ++it) {
+        const int buf = it & 1;
+        const int item = s_item[buf];
+        if (item >= total) break;
+        if (tid == 0) s_item[buf ^ 1] = atomicAdd(&v.ctr[CTR_WORK], 1);
+        const int c = cur.c;
+        const CloudDesc cd = v.cl[c];
         const int ns = v.ns[c];
-        const float* Ps = v.Ps + cd.p_off * DIM;
         const float* gS = v.S + cd.s_off * DIM;
         const float rsq = sqr_rn(cd.r1);
         const bool may_skip = rsq >= 1.0e-30f && rsq <= 1.0e30f;
         const float thr = __fmul_ru(rsq, 1.0009765625f);
-        for (int b0 = start; b0 < end; b0 += AC_BLOCK * AC_ITEMS) {
-            // this warp's points: b0 + warp*WPTS + j*32 + lane, and their box
-            float p[AC_ITEMS][DIM];
-            float2 np2[AC_ITEMS / 2][DIM];
-            float best[AC_ITEMS];
-            int bi[AC_ITEMS];
-            float blo[DIM], bhi[DIM];
+
+        // this warp's box (empty when the item has no points here)
+        float blo[DIM], bhi[DIM];
 #pragma unroll
-            for (int d = 0; d < DIM; ++d) {
-                blo[d] = INFINITY;
-                bhi[d] = -INFINITY;
-            }
+        for (int d = 0; d < DIM; ++d) {
+            blo[d] = INFINITY;
+            bhi[d] = -INFINITY;
+        }
 #pragma unroll
-            for (int j = 0; j < AC_ITEMS; ++j) {
-                const int i = b0 + warp * WPTS + j * 32 + lane;
+        for (int j = 0; j < AC_ITEMS; ++j)
+            if (cur.slot[j] >= 0)
 #pragma unroll
                 for (int d = 0; d < DIM; ++d) {
-                    p[j][d] = (i < end) ? Ps[(int64_t)i * DIM + d] : 0.0f;
-                    if (i < end) {
-                        blo[d] = fminf(blo[d], p[j][d]);
-                        bhi[d] = fmaxf(bhi[d], p[j][d]);
-                    }
+                    blo[d] = fminf(blo[d], cur.p[j][d]);
+                    bhi[d] = fmaxf(bhi[d], cur.p[j][d]);
                 }
-                best[j] = FLT_MAX;
-                bi[j] = -1;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                blo[d] = fminf(blo[d], __shfl_xor_sync(FULL, blo[d], o));
+                bhi[d] = fmaxf(bhi[d], __shfl_xor_sync(FULL, bhi[d], o));
             }
+        }
+        if (lane == 0) {
 #pragma unroll
             for (int d = 0; d < DIM; ++d) {
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    blo[d] = fminf(blo[d], __shfl_xor_sync(FULL, blo[d], o));
-                    bhi[d] = fmaxf(bhi[d], __shfl_xor_sync(FULL, bhi[d], o));
-                }
-            }
-#pragma unroll
-            for (int jj = 0; jj < AC_ITEMS / 2; ++jj)
-#pragma unroll
-                for (int d = 0; d < DIM; ++d)
-                    np2[jj][d] = make_float2(-p[2 * jj][d], -p[2 * jj + 1][d]);
-            for (int t0 = 0; t0 < ns; t0 += AC_TS) {
-                const int tl = min(AC_TS, ns - t0);
-                __syncthreads();  // the previous batch is no longer read
-                for (int e = tid; e < tl; e += AC_BLOCK)
-#pragma unroll
-                    for (int d = 0; d < DIM; ++d) sS[e * DP + d] = gS[(int64_t)(t0 + e) * DIM + d];
-                __syncthreads();
-                for (int q0 = 0; q0 < tl; q0 += 32) {
-                    const int q = q0 + lane;
-                    bool keep = false;
-                    if (q < tl) {
-                        float s[DIM];
-                        load_chosen<DIM>(sS, q, s);
-                        keep = !(may_skip && box_gap2<DIM>(s, blo, bhi) > thr);
-                    }
-                    unsigned bal = __ballot_sync(FULL, keep);
-                    while (bal) {  // kept chosen points in index order, warp-uniform
-                        const int b = __ffs(bal) - 1;
-                        bal &= bal - 1;
-                        float s[DIM];
-                        load_chosen<DIM>(sS, q0 + b, s);
-                        const int kk = t0 + q0 + b;
-#pragma unroll
-                        for (int jj = 0; jj < AC_ITEMS / 2; ++jj) {
-                            const float2 dd = sqdist2_exact<DIM>(s, np2[jj]);
-                            if (dd.x < best[2 * jj]) { best[2 * jj] = dd.x; bi[2 * jj] = kk; }
-                            if (dd.y < best[2 * jj + 1]) { best[2 * jj + 1] = dd.y; bi[2 * jj + 1] = kk; }
-                        }
-                    }
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < AC_ITEMS; ++j) {
-                const int i = b0 + warp * WPTS + j * 32 + lane;
-                if (i < end) v.keys[v.sorder[cd.p_off + i]] = (best[j] <= rsq) ? bi[j] : -1;
+                s_box[buf][warp][d] = blo[d];
+                s_box[buf][warp][DIM + d] = bhi[d];
             }
         }
-    }
-}
-
-// per-chunk key histograms in slot order after k_assign_cull (the rows
-// k_assign writes itself)
-constexpr int KH_BLOCK = 256;
-
-__global__ void __launch_bounds__(KH_BLOCK) k_keyhist(EngineView v)
-{
-    extern __shared__ int s_hist[];
-    const int tid = threadIdx.x;
-    const ActiveList al(v, ACT_CHUNK);
-    for (int item = blockIdx.x; item < al.total; item += gridDim.x) {
-        int c, lc;
-        al.locate(item, c, lc);
-        const CloudDesc cd = v.cl[c];
-        const int ns = v.ns[c];
-        const int start = (int)(((int64_t)lc * cd.n_all) / cd.n_chunks);
-        const int end = (int)(((int64_t)(lc + 1) * cd.n_all) / cd.n_chunks);
-        const int32_t* keys = v.keys + cd.p_off;
-        int32_t* row = v.hist + cd.hist_off + (int64_t)lc * cd.ns_cap;
-        if (ns <= v.hist_smem) {
-            for (int k = tid; k < ns; k += KH_BLOCK) s_hist[k] = 0;
+        float2 np2[AC_ITEMS / 2][DIM];
+        float best[AC_ITEMS];
+        int bi[AC_ITEMS];
+#pragma unroll
+        for (int jj = 0; jj < AC_ITEMS / 2; ++jj)
+#pragma unroll
+            for (int d = 0; d < DIM; ++d)
+                np2[jj][d] = make_float2(-cur.p[2 * jj][d], -cur.p[2 * jj + 1][d]);
+#pragma unroll
+        for (int j = 0; j < AC_ITEMS; ++j) {
+            best[j] = FLT_MAX;
+            bi[j] = -1;
+        }
+        __syncthreads();  // warp boxes and the next item visible; the previous item is done
+        // the next item's points are in flight while this one is evaluated
+        Item nxt;
+        load_item(s_item[buf ^ 1], nxt);
+        if (warp == 0 && lane < 2 * DIM) {
+            const bool hi = lane >= DIM;
+            float x = s_box[buf][0][lane];
+            for (int w = 1; w < AC_WARPS; ++w)
+                x = hi ? fmaxf(x, s_box[buf][w][lane]) : fminf(x, s_box[buf][w][lane]);
+            s_cbox[buf][lane] = x;
+        }
+        const bool cached = s_staged == c && ns <= AC_TS;
+        for (int t0 = 0; t0 < ns; t0 += AC_TS) {
+            const int tl = min(AC_TS, ns - t0);
+            if (!(t0 == 0 && cached)) {
+                if (t0 > 0) __syncthreads();  // the previous batch is no longer read
+                for (int e = tid; e < tl; e += AC_BLOCK) {
+                    float s[DIM];
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) s[d] = gS[(int64_t)(t0 + e) * DIM + d];
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) sS[e * DP + d] = s[d];
+                }
+            }
+            __syncthreads();  // batch staged, CTA box known
+            if (t0 == 0 && !cached && tid == 0) s_staged = (ns <= AC_TS) ? c : -1;
+            float clo[DIM], chi[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                clo[d] = s_cbox[buf][d];
+                chi[d] = s_cbox[buf][DIM + d];
+            }
+            // CTA-level test: warp w takes batch positions [w*cw, (w+1)*cw)
+            const int cw = ((tl + AC_BLOCK - 1) / AC_BLOCK) * 32;
+            unsigned keepbits = 0;
+            int wc = 0;
+            for (int r = 0; r * 32 < cw; ++r) {
+                const int e = warp * cw + r * 32 + lane;
+                bool keep = false;
+                if (e < tl) {
+                    float s[DIM];
+                    load_chosen<DIM>(sS, e, s);
+                    keep = !(may_skip && box_gap2<DIM>(s, clo, chi) > thr);
+                }
+                keepbits |= keep ? (1u << r) : 0u;
+                wc += __popc(__ballot_sync(FULL, keep));
+            }
+            if (lane == 0) s_wcnt[buf][warp] = wc;
             __syncthreads();
-            for (int i = start + tid; i < end; i += KH_BLOCK) {
-                const int k = keys[i];
-                if (k >= 0) atomicAdd(&s_hist[k], 1);
+            int pos = 0, nk = 0;
+#pragma unroll
+            for (int w = 0; w < AC_WARPS; ++w) {
+                const int x = s_wcnt[buf][w];
+                pos += (w < warp) ? x : 0;
+                nk += x;
+            }
+            for (int r = 0; r * 32 < cw; ++r) {
+                const bool keep = (keepbits >> r) & 1u;
+                const unsigned bal = __ballot_sync(FULL, keep);
+                if (keep) sK[buf][pos + __popc(bal & ((1u << lane) - 1u))] = warp * cw + r * 32 + lane;
+                pos += __popc(bal);
             }
             __syncthreads();
-            for (int k = tid; k < ns; k += KH_BLOCK) row[k] = s_hist[k];
-        } else {
-            for (int k = tid; k < ns; k += KH_BLOCK) row[k] = 0;
-            __syncthreads();
-            for (int i = start + tid; i < end; i += KH_BLOCK) {
-                const int k = keys[i];
-                if (k >= 0) atomicAdd(&row[k], 1);
+            // warp level: the survivors against this warp's box, then distances
+            for (int q0 = 0; q0 < nk; q0 += 32) {
+                const int q = q0 + lane;
+                int e = 0;
+                bool keep = false;
+                if (q < nk) {
+                    e = sK[buf][q];
+                    float s[DIM];
+                    load_chosen<DIM>(sS, e, s);
+                    keep = !(may_skip && box_gap2<DIM>(s, blo, bhi) > thr);
+                }
+                unsigned bal = __ballot_sync(FULL, keep);
+                while (bal) {  // kept chosen points in index order, warp-uniform
+                    const int b = __ffs(bal) - 1;
+                    bal &= bal - 1;
+                    const int eb = __shfl_sync(FULL, e, b);
+                    float s[DIM];
+                    load_chosen<DIM>(sS, eb, s);
+                    const int kk = t0 + eb;
+#pragma unroll
+                    for (int jj = 0; jj < AC_ITEMS / 2; ++jj) {
+                        const float2 dd = sqdist2_exact<DIM>(s, np2[jj]);
+                        if (dd.x < best[2 * jj]) { best[2 * jj] = dd.x; bi[2 * jj] = kk; }
+                        if (dd.y < best[2 * jj + 1]) { best[2 * jj + 1] = dd.y; bi[2 * jj + 1] = kk; }
+                    }
+                }
             }
         }
-        __syncthreads();
+        const float ratio = (float)cd.n_chunks / (float)cd.n_all;
+        int32_t* hist = v.hist + cd.hist_off;
+#pragma unroll
+        for (int j = 0; j < AC_ITEMS; ++j) {
+            if (cur.slot[j] >= 0) {
+                const int key = (best[j] <= rsq) ? bi[j] : -1;
+                v.keys[cur.slot[j]] = key;
+                if (key >= 0) {
+                    const int r = slot_chunk((int)(cur.slot[j] - cd.p_off), cd.n_all, cd.n_chunks, ratio);
+                    atomicAdd(&hist[(int64_t)r * cd.ns_cap + key], 1);
+                }
+            }
+        }
+        cur = nxt;
     }
 }
 
@@ -698,27 +804,102 @@ __global__ void __launch_bounds__(KH_BLOCK) k_keyhist(EngineView v)
 //                     them, exchange the warp totals, and rescan their rows
 //                     writing the prefixes;
 //   k_chunkscan_warp  the other clouds: one warp per item, a single pass.
+// The key bases follow in the same kernel: the CTA (warp) that finishes the
+// last key block of a cloud -- a per-cloud counter of finished blocks says
+// which -- forms the exclusive prefix of the cloud's member counts (each
+// key's first grouped slot) and lists the keys of SUM_BIG_MIN or more members
+// for the CTA-wide folds of k_sum_shift.
 // ---------------------------------------------------------------------------
 constexpr int CS_W = 16;   // warps of the CTA-wide scan
 constexpr int CSW_W = 8;   // items (warps) per CTA of the warp-wide scan
 constexpr int CS_LOADS = 16;  // histogram loads in flight per lane
+constexpr int CS_REG = 32;    // rows per warp kept in registers between the two passes
+
+// key bases of cloud c by the whole CTA (any multiple of 32 threads)
+__device__ void key_bases_cta(const EngineView& v, const int c, int* s_w, int& s_carry)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const CloudDesc cd = v.cl[c];
+    const int ns = v.ns[c];
+    const int32_t* cnt = v.cnt + cd.key_off;
+    int32_t* base = v.base + cd.key_off;
+    __syncthreads();  // earlier readers of s_w / s_carry are done
+    if (threadIdx.x == 0) s_carry = 0;
+    for (int k0 = 0; k0 < ns; k0 += blockDim.x) {
+        __syncthreads();
+        const int k = k0 + threadIdx.x;
+        const int x = (k < ns) ? cnt[k] : 0;
+        int incl = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) s_w[warp] = incl;
+        __syncthreads();
+        int wpre = 0, tot = 0;
+        for (int w = 0; w < nw; ++w) {
+            wpre += (w < warp) ? s_w[w] : 0;
+            tot += s_w[w];
+        }
+        const int carry = s_carry;
+        if (k < ns) base[k] = carry + wpre + incl - x;
+        if (x >= SUM_BIG_MIN) v.big[atomicAdd(&v.ctr[CTR_NBIG], 1)] = (int)(cd.key_off + k);
+        __syncthreads();
+        if (threadIdx.x == 0) s_carry = carry + tot;
+    }
+}
+
+// the same by one warp
+__device__ void key_bases_warp(const EngineView& v, const int c, const int lane)
+{
+    const CloudDesc cd = v.cl[c];
+    const int ns = v.ns[c];
+    const int32_t* cnt = v.cnt + cd.key_off;
+    int32_t* base = v.base + cd.key_off;
+    int carry = 0;
+    for (int k0 = 0; k0 < ns; k0 += 32) {
+        const int k = k0 + lane;
+        const int x = (k < ns) ? cnt[k] : 0;
+        int incl = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (k < ns) base[k] = carry + incl - x;
+        if (x >= SUM_BIG_MIN) v.big[atomicAdd(&v.ctr[CTR_NBIG], 1)] = (int)(cd.key_off + k);
+        carry += __shfl_sync(FULL, incl, 31);
+    }
+}
 
 __global__ void __launch_bounds__(CS_W * 32) k_chunkscan_cta(EngineView v)
 {
     __shared__ int s_part[CS_W][32];
+    __shared__ int s_w[CS_W];
+    __shared__ int s_carry, s_last;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const ActiveList al(v, ACT_KBLK);
     for (int item = blockIdx.x; item < al.total; item += gridDim.x) {
         int c, kb;
         al.locate(item, c, kb);
         const CloudDesc cd = v.cl[c];
+        const int ns = v.ns[c];
         const int k = kb * KBLK + lane;
-        const bool ok = k < v.ns[c];
+        const bool ok = k < ns;
         const int rows = cd.n_chunks;
         const int rw0 = (warp * rows) / CS_W, rw1 = ((warp + 1) * rows) / CS_W;
         int32_t* h = v.hist + cd.hist_off + k;
+        // the first CS_REG rows of the warp's range stay in registers for the
+        // rescan; longer ranges reload the rest
+        int xr[CS_REG];
         int sum = 0;
-        for (int r0 = rw0; r0 < rw1; r0 += CS_LOADS) {
+#pragma unroll
+        for (int u = 0; u < CS_REG; ++u)
+            xr[u] = (ok && rw0 + u < rw1) ? h[(int64_t)(rw0 + u) * cd.ns_cap] : 0;
+#pragma unroll
+        for (int u = 0; u < CS_REG; ++u) sum += xr[u];
+        for (int r0 = rw0 + CS_REG; r0 < rw1; r0 += CS_LOADS) {
             int x[CS_LOADS];
 #pragma unroll
             for (int u = 0; u < CS_LOADS; ++u)
@@ -735,7 +916,12 @@ __global__ void __launch_bounds__(CS_W * 32) k_chunkscan_cta(EngineView v)
             run += (w < warp) ? y : 0;
             tot += y;
         }
-        for (int r0 = rw0; r0 < rw1; r0 += CS_LOADS) {
+#pragma unroll
+        for (int u = 0; u < CS_REG; ++u) {
+            if (ok && rw0 + u < rw1) h[(int64_t)(rw0 + u) * cd.ns_cap] = run;
+            run += xr[u];
+        }
+        for (int r0 = rw0 + CS_REG; r0 < rw1; r0 += CS_LOADS) {
             int x[CS_LOADS];
 #pragma unroll
             for (int u = 0; u < CS_LOADS; ++u)
@@ -747,7 +933,17 @@ __global__ void __launch_bounds__(CS_W * 32) k_chunkscan_cta(EngineView v)
             }
         }
         if (warp == 0 && ok) v.cnt[cd.key_off + k] = tot;
-        __syncthreads();  // s_part is reused by the next item
+        // the last key block of the cloud: its key bases
+        __threadfence();
+        __syncthreads();  // also: s_part is reused by the next item
+        if (threadIdx.x == 0)
+            s_last = atomicAdd(&v.kbdone[c], 1) == (ns + KBLK - 1) / KBLK - 1;
+        __syncthreads();
+        if (s_last) {
+            __threadfence();
+            key_bases_cta(v, c, s_w, s_carry);
+            if (threadIdx.x == 0) v.kbdone[c] = 0;
+        }
     }
 }
 
@@ -760,8 +956,9 @@ __global__ void __launch_bounds__(CSW_W * 32) k_chunkscan_warp(EngineView v)
         int c, kb;
         al.locate(item, c, kb);
         const CloudDesc cd = v.cl[c];
+        const int ns = v.ns[c];
         const int k = kb * KBLK + lane;
-        const bool ok = k < v.ns[c];
+        const bool ok = k < ns;
         const int rows = cd.n_chunks;
         int32_t* h = v.hist + cd.hist_off + k;
         int run = 0;
@@ -777,65 +974,47 @@ __global__ void __launch_bounds__(CSW_W * 32) k_chunkscan_warp(EngineView v)
             }
         }
         if (ok) v.cnt[cd.key_off + k] = run;
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Key bases: one CTA per evolving cloud, exclusive prefix of the member
-// counts over its keys (first grouped slot of each key); keys of SUM_BIG_MIN
-// or more members are listed for the CTA-wide folds of k_sum_shift.
-// ---------------------------------------------------------------------------
-template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_keybase(EngineView v)
-{
-    __shared__ int s_w[BLOCK / 32];
-    __shared__ int s_carry;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int nact = v.ctr[CTR_NACT];
-    for (int a = blockIdx.x; a < nact; a += gridDim.x) {
-        __syncthreads();  // the previous cloud's readers of s_w / s_carry are done
-        const int c = v.act_cloud[a];
-        const CloudDesc cd = v.cl[c];
-        const int ns = v.ns[c];
-        const int32_t* cnt = v.cnt + cd.key_off;
-        int32_t* base = v.base + cd.key_off;
-        if (threadIdx.x == 0) s_carry = 0;
-        for (int k0 = 0; k0 < ns; k0 += BLOCK) {
-            __syncthreads();
-            const int k = k0 + threadIdx.x;
-            const int x = (k < ns) ? cnt[k] : 0;
-            int incl = x;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(FULL, incl, o);
-                if (lane >= o) incl += y;
-            }
-            if (lane == 31) s_w[warp] = incl;
-            __syncthreads();
-            int wpre = 0, tot = 0;
-            for (int w = 0; w < BLOCK / 32; ++w) {
-                wpre += (w < warp) ? s_w[w] : 0;
-                tot += s_w[w];
-            }
-            const int carry = s_carry;
-            if (k < ns) base[k] = carry + wpre + incl - x;
-            if (x >= SUM_BIG_MIN) v.big[atomicAdd(&v.ctr[CTR_NBIG], 1)] = (int)(cd.key_off + k);
-            __syncthreads();
-            if (threadIdx.x == 0) s_carry = carry + tot;
+        // the last key block of the cloud: its key bases
+        __threadfence();
+        __syncwarp();
+        int last = 0;
+        if (lane == 0) last = atomicAdd(&v.kbdone[c], 1) == (ns + KBLK - 1) / KBLK - 1;
+        if (__shfl_sync(FULL, last, 0)) {
+            __threadfence();
+            key_bases_warp(v, c, lane);
+            if (lane == 0) v.kbdone[c] = 0;
         }
     }
 }
 
 // ---------------------------------------------------------------------------
 // stable scatter: one warp per chunk walks its points in index order and
-// writes each assigned point's index to the next free slot of its key's
-// segment of the permutation, so every segment lists its members in
-// cloud-point index order.  Keys of the chunk and the per-key start slots are
+// writes each assigned point's coordinates to the next free row of its key's
+// segment of the grouped copy Pg, so every segment lists its members in
+// cloud-point index order as one contiguous stream for the folds.  Keys of the chunk and the per-key start slots are
 // staged in shared memory first; the ordered walk then touches shared memory
 // only (match_any groups equal keys of 32 consecutive points, the group
 // leader advances the key's cursor).
 // ---------------------------------------------------------------------------
+template <int DIM>
 __device__ void scatter_chunk(const EngineView& v, int c, int lc, int* s_keys, int lane);
+
+// row r of a grouped copy (PadDim<DIM> floats per row)
+template <int DIM>
+__device__ __forceinline__ void store_row(float* rows, int64_t r, const float (&q)[DIM])
+{
+    constexpr int DP = PadDim<DIM>::v;
+    if constexpr (DP == 4) {
+        reinterpret_cast<float4*>(rows)[r] =
+            make_float4(q[0], DIM > 1 ? q[DIM > 1 ? 1 : 0] : 0.0f, DIM > 2 ? q[DIM > 2 ? 2 : 0] : 0.0f,
+                        DIM > 3 ? q[DIM > 3 ? 3 : 0] : 0.0f);
+    } else if constexpr (DP == 2) {
+        reinterpret_cast<float2*>(rows)[r] = make_float2(q[0], q[1]);
+    } else {
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) rows[r * DP + d] = q[d];
+    }
+}
 
 
 // One CTA per chunk for clouds with at most SCAT_HMAX chosen points.  The
@@ -847,9 +1026,14 @@ __device__ void scatter_chunk(const EngineView& v, int c, int lc, int* s_keys, i
 // chosen sets use scatter_chunk (one warp) in warp 0.
 constexpr int SCAT_W = 8;
 constexpr int SCAT_HMAX = 1024;
+constexpr int SCAT_KS = 8;   // chunk keys per thread loaded together (covers 2,048-point chunks)
+constexpr int SCAT_SP = 8;   // placement steps whose coordinates are loaded together
+static_assert(SCAT_HMAX % (SCAT_W * 32) == 0, "key bases: whole loads per thread");
 
+template <int DIM>
 __global__ void __launch_bounds__(SCAT_W * 32) k_scatter_cta(EngineView v)
 {
+    constexpr int DP = PadDim<DIM>::v;
     extern __shared__ int s_dyn[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const ActiveList al(v, ACT_CHUNK);
@@ -860,7 +1044,7 @@ __global__ void __launch_bounds__(SCAT_W * 32) k_scatter_cta(EngineView v)
         const CloudDesc cd = v.cl[c];
         const int ns = v.ns[c];
         if (ns > SCAT_HMAX) {
-            if (warp == 0) scatter_chunk(v, c, lc, s_dyn, lane);
+            if (warp == 0) scatter_chunk<DIM>(v, c, lc, s_dyn, lane);
             continue;
         }
         const int start = (int)(((int64_t)lc * cd.n_all) / cd.n_chunks);
@@ -869,40 +1053,91 @@ __global__ void __launch_bounds__(SCAT_W * 32) k_scatter_cta(EngineView v)
         int* s_keys = s_dyn;                 // chunk_max
         int* hw = s_dyn + v.chunk_max;       // SCAT_W x ns: counts, then start slots
         const int32_t* keys = v.keys + cd.p_off + start;
-        for (int e = tid; e < len; e += SCAT_W * 32) s_keys[e] = keys[e];
+        int32_t* row = v.hist + cd.hist_off + (int64_t)lc * cd.ns_cap;
+        const int32_t* bs = v.base + cd.key_off;
+        const float* Pc = v.P + (cd.p_off + start) * DIM;
+        const int r0 = (warp * len) / SCAT_W, r1 = ((warp + 1) * len) / SCAT_W;
+        // Every global load of the chunk is issued up front -- its keys, its
+        // key bases and histogram row, and the coordinates of this warp's
+        // first SCAT_SP placement steps -- so the chunk waits for one memory
+        // round trip instead of one per loop step.
+        int kv[SCAT_KS];
+#pragma unroll
+        for (int u = 0; u < SCAT_KS; ++u) {
+            const int e = u * SCAT_W * 32 + tid;
+            kv[u] = (e < len) ? keys[e] : -1;
+        }
+        int bsv[SCAT_HMAX / (SCAT_W * 32)], rwv[SCAT_HMAX / (SCAT_W * 32)];
+#pragma unroll
+        for (int u = 0; u < SCAT_HMAX / (SCAT_W * 32); ++u) {
+            const int k = u * SCAT_W * 32 + tid;
+            bsv[u] = (k < ns) ? bs[k] : 0;
+            rwv[u] = (k < ns) ? row[k] : 0;
+        }
+        float pc[SCAT_SP][DIM];
+#pragma unroll
+        for (int q = 0; q < SCAT_SP; ++q) {
+            const int i = r0 + q * 32 + lane;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) pc[q][d] = (i < r1) ? Pc[(int64_t)i * DIM + d] : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < SCAT_KS; ++u) {
+            const int e = u * SCAT_W * 32 + tid;
+            if (e < len) s_keys[e] = kv[u];
+        }
+        for (int e = SCAT_KS * SCAT_W * 32 + tid; e < len; e += SCAT_W * 32) s_keys[e] = keys[e];
         for (int e = tid; e < SCAT_W * ns; e += SCAT_W * 32) hw[e] = 0;
         __syncthreads();
-        const int r0 = (warp * len) / SCAT_W, r1 = ((warp + 1) * len) / SCAT_W;
         for (int i0 = r0; i0 < r1; i0 += 32) {
             const int i = i0 + lane;
             const WarpRun r = warp_runs((i < r1) ? s_keys[i] : -1, lane);
             if (r.key >= 0 && lane == r.head) atomicAdd(&hw[warp * ns + r.key], r.count);
         }
         __syncthreads();
-        const int32_t* row = v.hist + cd.hist_off + (int64_t)lc * cd.ns_cap;
-        const int32_t* bs = v.base + cd.key_off;
-        for (int k = tid; k < ns; k += SCAT_W * 32) {
-            int run = bs[k] + row[k];
 #pragma unroll
-            for (int w = 0; w < SCAT_W; ++w) {
-                const int x = hw[w * ns + k];
-                hw[w * ns + k] = run;
-                run += x;
+        for (int u = 0; u < SCAT_HMAX / (SCAT_W * 32); ++u) {
+            const int k = u * SCAT_W * 32 + tid;
+            if (k < ns) {
+                int run = bsv[u] + rwv[u];
+                row[k] = 0;  // the row is free again for the next pass's counts
+#pragma unroll
+                for (int w = 0; w < SCAT_W; ++w) {
+                    const int x = hw[w * ns + k];
+                    hw[w * ns + k] = run;
+                    run += x;
+                }
             }
         }
         __syncthreads();
         int* cur = hw + warp * ns;
-        int32_t* perm = v.perm + cd.p_off;
-        for (int i0 = r0; i0 < r1; i0 += 32) {
-            const int i = i0 + lane;
-            const WarpRun r = warp_runs((i < r1) ? s_keys[i] : -1, lane);
-            int b = 0;
-            if (r.key >= 0 && lane == r.head) {
-                b = cur[r.key];
-                cur[r.key] = b + r.count;
+        float* Pg = v.Pg + cd.p_off * DP;
+        for (int g0 = r0; g0 < r1; g0 += 32 * SCAT_SP) {
+            if (g0 > r0) {  // ranges longer than SCAT_SP steps: the next steps' coordinates
+#pragma unroll
+                for (int q = 0; q < SCAT_SP; ++q) {
+                    const int i = g0 + q * 32 + lane;
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) pc[q][d] = (i < r1) ? Pc[(int64_t)i * DIM + d] : 0.0f;
+                }
             }
-            b = __shfl_sync(FULL, b, r.head);
-            if (r.key >= 0) perm[b + r.rank] = start + i0 + r.src;
+#pragma unroll
+            for (int q = 0; q < SCAT_SP; ++q) {
+                const int i0 = g0 + q * 32;
+                if (i0 >= r1) break;
+                const int i = i0 + lane;
+                const WarpRun r = warp_runs((i < r1) ? s_keys[i] : -1, lane);
+                int b = 0;
+                if (r.key >= 0 && lane == r.head) {
+                    b = cur[r.key];
+                    cur[r.key] = b + r.count;
+                }
+                b = __shfl_sync(FULL, b, r.head);
+                float qv[DIM];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) qv[d] = __shfl_sync(FULL, pc[q][d], r.src);
+                if (r.key >= 0) store_row<DIM>(Pg, b + r.rank, qv);
+            }
         }
     }
 }
@@ -915,8 +1150,10 @@ inline int scatter_cta_smem_bytes(const EngineView& v)
     return 4 * (block_path > warp_path ? block_path : warp_path);
 }
 
+template <int DIM>
 __device__ void scatter_chunk(const EngineView& v, int c, int lc, int* s_keys, int lane)
 {
+    constexpr int DP = PadDim<DIM>::v;
     const CloudDesc cd = v.cl[c];
     const int ns = v.ns[c];
     int32_t* row = v.hist + cd.hist_off + (int64_t)lc * cd.ns_cap;
@@ -958,9 +1195,13 @@ __device__ void scatter_chunk(const EngineView& v, int c, int lc, int* s_keys, i
         }
     }
     __syncwarp();
-    int32_t* perm = v.perm + cd.p_off;
+    const float* Pc = v.P + (cd.p_off + start) * DIM;
+    float* Pg = v.Pg + cd.p_off * DP;
     for (int off = 0; off < len; off += 32) {
         const int i = off + lane;
+        float pc[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) pc[d] = (i < len) ? Pc[(int64_t)i * DIM + d] : 0.0f;
         const WarpRun r = warp_runs((i < len) ? s_keys[i] : -1, lane);
         int b = 0;
         if (r.key >= 0 && lane == r.head) {
@@ -968,9 +1209,13 @@ __device__ void scatter_chunk(const EngineView& v, int c, int lc, int* s_keys, i
             ctr[r.key] = b + r.count;
         }
         b = __shfl_sync(FULL, b, r.head);
-        if (r.key >= 0) perm[b + r.rank] = start + off + r.src;
+        float q[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) q[d] = __shfl_sync(FULL, pc[d], r.src);
+        if (r.key >= 0) store_row<DIM>(Pg, b + r.rank, q);
         __syncwarp();
     }
+    for (int k = lane; k < ns; k += 32) row[k] = 0;  // free for the next pass's counts
 }
 
 // ---------------------------------------------------------------------------
@@ -994,8 +1239,7 @@ constexpr int TILE_PPL = 8;
 constexpr int FOLD_CTA_MIN = 4096;
 
 template <int DIM>
-__device__ void sum_shift_one(const EngineView& v, int c, int k, float* buf, int* sidx, int lane,
-                              bool cta_big);
+__device__ void sum_shift_one(const EngineView& v, int c, int k, float* buf, int lane, bool cta_big);
 
 template <int DIM>
 __device__ void sum_shift_big_one(const EngineView& v, int slot, SegFoldSmem<8, DIM>& sm);
@@ -1022,15 +1266,14 @@ __global__ void __launch_bounds__(256) k_sum_shift(EngineView v, int big_ctas, i
         if (cta_big)
             for (int i = blockIdx.x; i < nbig; i += big_ctas) sum_shift_big_one<DIM>(v, v.big[i], sm);
     } else {
-        float* s_buf = reinterpret_cast<float*>(s_raw) + warp * SUM_BP_WIDE * DIM;
-        int* s_idx = reinterpret_cast<int*>(s_raw + 8 * SUM_BP_WIDE * DIM * 4) + warp * SUM_BP_WIDE;
+        float* s_buf = reinterpret_cast<float*>(s_raw) + warp * SUM_BP_WIDE * PadDim<DIM>::v;
         const ActiveList al(v, ACT_SLOT);
         const int b = (int)blockIdx.x - big_ctas, nb = (int)gridDim.x - big_ctas;
         for (int t = b * 8 + warp; t < al.total; t += nb * 8) {
             __syncwarp();
             int c, k;
             al.locate(t, c, k);
-            sum_shift_one<DIM>(v, c, k, s_buf, s_idx, lane, cta_big);
+            sum_shift_one<DIM>(v, c, k, s_buf, lane, cta_big);
         }
     }
     if (!with_control) return;
@@ -1128,16 +1371,70 @@ __device__ void apply_shift(const EngineView& v, int c, const CloudDesc& cd, int
     if (__any_sync(FULL, moved) && lane == 0) v.cont[c] = 1;
 }
 
+// Sequential FP32 fold, in order, of n contiguous rows of a grouped copy
+// (PadDim<DIM> floats each); one warp, the sum of coordinate d returned in
+// lane d < DIM.  A block of BP rows is loaded with coalesced vector loads into
+// the warp's buffer (BP x PadDim floats) while the previous block is folded.
+template <int DIM, int BP>
+__device__ float fold_rows(const float* __restrict__ rows, const int n, float* buf, const int lane)
+{
+    constexpr int DP = PadDim<DIM>::v;
+    constexpr int VW = (DP == 4) ? 4 : (DP == 2 ? 2 : 1);  // floats per vector load
+    constexpr int R = BP * DP / (32 * VW);                 // vector loads per lane per block
+    static_assert(BP * DP % (32 * VW) == 0, "block of whole vector loads");
+    float nxt[R][VW];
+    auto load = [&](int off) {
+        const int lim = min(BP, n - off) * DP;  // valid floats of the block
+        const float* src = rows + (int64_t)off * DP;
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+            const int e = (u * 32 + lane) * VW;
+            if constexpr (VW == 4) {
+                const float4 t = (e < lim) ? reinterpret_cast<const float4*>(src)[u * 32 + lane]
+                                           : make_float4(0.f, 0.f, 0.f, 0.f);
+                nxt[u][0] = t.x; nxt[u][VW > 1 ? 1 : 0] = t.y;
+                nxt[u][VW > 2 ? 2 : 0] = t.z; nxt[u][VW > 3 ? 3 : 0] = t.w;
+            } else if constexpr (VW == 2) {
+                const float2 t = (e < lim) ? reinterpret_cast<const float2*>(src)[u * 32 + lane]
+                                           : make_float2(0.f, 0.f);
+                nxt[u][0] = t.x; nxt[u][VW > 1 ? 1 : 0] = t.y;
+            } else {
+                nxt[u][0] = (e < lim) ? src[e] : 0.0f;
+            }
+        }
+    };
+    load(0);
+    float sum = 0.0f;
+    for (int off = 0; off < n; off += BP) {
+        const int m = min(BP, n - off);
+        __syncwarp();  // every lane is done reading the previous block
+#pragma unroll
+        for (int u = 0; u < R; ++u)
+#pragma unroll
+            for (int w = 0; w < VW; ++w) buf[(u * 32 + lane) * VW + w] = nxt[u][w];
+        if (off + BP < n) load(off + BP);  // in flight during the fold
+        __syncwarp();
+        if (lane < DIM) {
+            if (m == BP) {
+#pragma unroll 32
+                for (int j = 0; j < BP; ++j) sum = __fadd_rn(sum, buf[j * DP + lane]);
+            } else {
+                for (int j = 0; j < m; ++j) sum = __fadd_rn(sum, buf[j * DP + lane]);
+            }
+        }
+    }
+    __syncwarp();
+    return sum;
+}
+
 template <int DIM>
-__device__ void sum_shift_one(const EngineView& v, int c, int k, float* buf, int* sidx, int lane,
-                              bool cta_big)
+__device__ void sum_shift_one(const EngineView& v, int c, int k, float* buf, int lane, bool cta_big)
 {
     const CloudDesc cd = v.cl[c];
     const int n = v.cnt[cd.key_off + k];
     if (n == 0 || (cta_big && n >= SUM_BIG_MIN)) return;  // big keys: the CTA path
-    const int32_t* mp = v.perm + cd.p_off + v.base[cd.key_off + k];
-    const float* Pc = v.P + cd.p_off * DIM;
-    const float sum = fold_members<DIM, SUM_BP_WIDE>(mp, n, Pc, buf, sidx, lane);
+    const float* rows = v.Pg + (cd.p_off + v.base[cd.key_off + k]) * PadDim<DIM>::v;
+    const float sum = fold_rows<DIM, SUM_BP_WIDE>(rows, n, buf, lane);
     apply_shift<DIM>(v, c, cd, k, n, sum, lane);
 }
 
@@ -1159,10 +1456,9 @@ __device__ void sum_shift_big_one(const EngineView& v, int slot, SegFoldSmem<8, 
     const CloudDesc cd = v.cl[c];
     const int k = (int)(slot - cd.key_off);
     const int n = v.cnt[slot];
-    const int32_t* mp = v.perm + cd.p_off + v.base[slot];
-    const float* Pc = v.P + cd.p_off * DIM;
+    const float* rows = v.Pg + (cd.p_off + v.base[slot]) * PadDim<DIM>::v;
     __syncthreads();  // the previous key's scratch is no longer read
-    fold_members_seg<8, DIM>(mp, n, Pc, sm);
+    fold_members_seg_src<8, DIM>(RowSrc<DIM>{rows}, n, sm);
     if (warp == 0) apply_shift<DIM>(v, c, cd, k, n, (lane < DIM) ? sm.out[lane] : 0.0f, lane);
 }
 
@@ -1264,12 +1560,14 @@ __device__ __forceinline__ void tile_assign_range(const float* __restrict__ P, c
             if (k < ns) whist[k] += kc[k];
 }
 
-// Stable placement of the warp's points [r0, r1w) into perm: the members of
-// key k go, in index order, to cur[k], cur[k] + 1, ... (cur advanced).
+// Stable placement of the warp's points [r0, r1w): the coordinates of the
+// members of key k go, in index order, to rows cur[k], cur[k] + 1, ... of the
+// grouped copy Pg (cur advanced).
 template <int DIM>
-__device__ __forceinline__ void tile_place_range(const int32_t* __restrict__ keys, const int r0,
+__device__ __forceinline__ void tile_place_range(const float* __restrict__ P,
+                                                 const int32_t* __restrict__ keys, const int r0,
                                                  const int r1w, int* cur, const int ns,
-                                                 int32_t* __restrict__ perm, const int lane)
+                                                 float* __restrict__ Pg, const int lane)
 {
     constexpr int KB = TILE_KB;
     int base[KB];
@@ -1279,21 +1577,23 @@ __device__ __forceinline__ void tile_place_range(const int32_t* __restrict__ key
     }
     for (int i0 = r0; i0 < r1w; i0 += 32 * TILE_PPL) {
         int kq[TILE_PPL];
+        float pq[TILE_PPL][DIM];
 #pragma unroll
         for (int h = 0; h < TILE_PPL; ++h) {
             const int i = i0 + h * 32 + lane;
             kq[h] = (i < r1w) ? keys[i] : -1;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) pq[h][d] = (i < r1w) ? P[(int64_t)i * DIM + d] : 0.0f;
         }
 #pragma unroll
         for (int h = 0; h < TILE_PPL; ++h) {
             const int key = kq[h];
-            const int i = i0 + h * 32 + lane;
             if (ns <= KB) {
 #pragma unroll
                 for (int k = 0; k < KB; ++k) {
                     if (k < ns) {
                         const unsigned m = __ballot_sync(FULL, key == k);
-                        if (key == k) perm[base[k] + __popc(m & lanemask_lt())] = i;
+                        if (key == k) store_row<DIM>(Pg, base[k] + __popc(m & lanemask_lt()), pq[h]);
                         base[k] += __popc(m);
                     }
                 }
@@ -1306,7 +1606,7 @@ __device__ __forceinline__ void tile_place_range(const int32_t* __restrict__ key
                     cur[key] = b + __popc(m);
                 }
                 b = __shfl_sync(FULL, b, leader);
-                if (key >= 0) perm[b + __popc(m & lanemask_lt())] = i;
+                if (key >= 0) store_row<DIM>(Pg, b + __popc(m & lanemask_lt()), pq[h]);
             }
         }
     }
@@ -1314,8 +1614,7 @@ __device__ __forceinline__ void tile_place_range(const int32_t* __restrict__ key
 
 template <int DIM, int BLOCK>
 struct TileCtaSmem {
-    float buf[BLOCK / 32][SUM_BP * DIM];
-    int idx[BLOCK / 32][SUM_BP];
+    float buf[BLOCK / 32][SUM_BP * PadDim<DIM>::v];   // fold_rows blocks
     int moved;
     SegFoldSmem<BLOCK / 32, DIM> seg;
 };
@@ -1334,7 +1633,6 @@ __device__ void tile_evolve_one(const EngineView& v, const int c, unsigned char*
     int* hist = reinterpret_cast<int*>(sS + TILE_NS_MAX * DP);             // W*(TILE_NS_MAX+1)
     int* kbase = hist + W * (TILE_NS_MAX + 1);                              // TILE_NS_MAX+1
     auto& s_buf = ts.buf;
-    auto& s_idx = ts.idx;
     int& s_moved = ts.moved;
     auto& s_seg = ts.seg;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -1345,7 +1643,7 @@ __device__ void tile_evolve_one(const EngineView& v, const int c, unsigned char*
         const float* P = v.P + cd.p_off * DIM;
         float* gS = v.S + cd.s_off * DIM;
         int32_t* keys = v.keys + cd.p_off;
-        int32_t* perm = v.perm + cd.p_off;
+        float* Pg = v.Pg + cd.p_off * DP;
         const float rsq = sqr_rn(cd.r1);
         const int nsp = (ns + KB - 1) / KB * KB;
         __syncthreads();
@@ -1398,13 +1696,13 @@ __device__ void tile_evolve_one(const EngineView& v, const int c, unsigned char*
             // 3. stable placement, warp range by warp range (keys of
             //    TILE_PPL warp steps loaded ahead of the dependent placement
             //    chain)
-            tile_place_range<DIM>(keys, r0, r1w, hist + warp * (TILE_NS_MAX + 1), ns, perm, lane);
+            tile_place_range<DIM>(P, keys, r0, r1w, hist + warp * (TILE_NS_MAX + 1), ns, Pg, lane);
             __syncthreads();
             // 4a. very large keys, one at a time, folded by the whole CTA
             for (int k = 0; k < ns; ++k) {
                 const int cnt = kbase[k + 1] - kbase[k];
                 if (cnt < FOLD_CTA_MIN) continue;
-                fold_members_seg<W, DIM>(perm + kbase[k], cnt, P, s_seg);
+                fold_members_seg_src<W, DIM>(RowSrc<DIM>{Pg + (int64_t)kbase[k] * DP}, cnt, s_seg);
                 if (tid < DIM) {
                     float cval = sS[k * DP + tid];
                     if (shift_coord(s_seg.out[tid], cnt, cval)) {
@@ -1418,7 +1716,7 @@ __device__ void tile_evolve_one(const EngineView& v, const int c, unsigned char*
             for (int k = warp; k < ns; k += W) {
                 const int cnt = kbase[k + 1] - kbase[k];
                 if (cnt == 0 || cnt >= FOLD_CTA_MIN) continue;
-                const float sum = fold_members<DIM>(perm + kbase[k], cnt, P, s_buf[warp], s_idx[warp], lane);
+                const float sum = fold_rows<DIM, SUM_BP>(Pg + (int64_t)kbase[k] * DP, cnt, s_buf[warp], lane);
                 int moved = 0;
                 if (lane < DIM) {
                     float cval = sS[k * DP + lane];
@@ -1859,20 +2157,43 @@ cudaError_t launch_decbig(const EngineView& v, cudaStream_t st)
     return cudaGetLastError();
 }
 
-// one CTA per group queued by k_control in this iteration
+__device__ void loop_condition(const EngineView& v, cudaGraphConditionalHandle h, int use_handle,
+                               int count_iter);
+
+// one CTA per group queued by the control step in this iteration; with_cond:
+// the last CTA to finish then runs the loop-condition step (the phases and
+// chosen counts of every group are final by then)
 template <int DIM, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_decimate(EngineView v)
+__global__ void __launch_bounds__(BLOCK) k_decimate(EngineView v, cudaGraphConditionalHandle h,
+                                                    int with_cond, int use_handle)
 {
+    __shared__ int s_last;
     const int nready = v.ctr[CTR_NREADY];
     for (int r = blockIdx.x; r < nready; r += gridDim.x) decimate_group<DIM, BLOCK>(v, v.ready[r]);
+    if (!with_cond) return;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(&v.ctr[CTR_DEC_DONE], 1) == (int)gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (threadIdx.x == 0) v.ctr[CTR_DEC_DONE] = 0;
+    loop_condition(v, h, use_handle, 1);
 }
 
 // ---------------------------------------------------------------------------
 // loop condition: any unfinished cloud?  Sets the graph WHILE handle (graph
 // mode) and/or leaves the count in ctr[CTR_ACTIVE] for the host (plain mode).
+// Run by one whole CTA (any size up to 1024 threads).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(1024) k_loopcond(EngineView v, cudaGraphConditionalHandle h,
                                                    int use_handle, int count_iter)
+{
+    loop_condition(v, h, use_handle, count_iter);
+}
+
+__device__ void loop_condition(const EngineView& v, cudaGraphConditionalHandle h, int use_handle,
+                               int count_iter)
 {
     __shared__ int s_act;
     __shared__ int s_w[32][ACT_KINDS + 1];
@@ -1978,6 +2299,7 @@ __global__ void k_reset(EngineView v)
     if (c == 0) v.dbig[0] = 0;
     if (c < v.n_groups) v.group_conv[c] = 0;
     if (c >= v.n_clouds) return;
+    v.kbdone[c] = 0;
     v.cont[c] = 0;
     v.passes[c] = 0;
     v.total_passes[c] = 0;
@@ -1991,6 +2313,24 @@ cudaError_t set_assign_attrs(int dyn)
 {
     return cudaFuncSetAttribute(k_assign<DIM, BLOCK, ITEMS>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+}
+
+// persistent grid of k_assign_cull: every resident CTA, at most one per item
+template <int DIM, int ITEMS>
+void launch_assign_cull(const EngineView& v, cudaStream_t st)
+{
+    static std::atomic<int> per_sm{0};
+    int b = per_sm.load(std::memory_order_relaxed);
+    if (b == 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_assign_cull<DIM, ITEMS>, AC_BLOCK, 0) !=
+                cudaSuccess || b < 1)
+            b = 1;
+        per_sm.store(b, std::memory_order_relaxed);
+    }
+    const int subs = (v.chunk_pts + AC_BLOCK * ITEMS - 1) / (AC_BLOCK * ITEMS);
+    const int64_t items = (int64_t)v.n_chunks * subs;
+    const int g = (int)std::max<int64_t>(1, std::min<int64_t>(items, (int64_t)v.n_sms * b));
+    k_assign_cull<DIM, ITEMS><<<g, AC_BLOCK, 0, st>>>(v);
 }
 
 template <int DIM>
@@ -2007,24 +2347,21 @@ cudaError_t prepare_pass_dim(const EngineView& v, const TuneParams& tp)
     e = cudaFuncSetAttribute(k_decimate<DIM, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              dec_smem_bytes(v));
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_keyhist, cudaFuncAttributeMaxDynamicSharedMemorySize, hist_bytes);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_scatter_cta, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    return cudaFuncSetAttribute(k_scatter_cta<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 scatter_cta_smem_bytes(v));
 }
 
 template <int DIM>
 cudaError_t launch_pass_dim(const EngineView& v, const TuneParams& tp, int assign_grid,
-                            cudaStream_t st, cudaEvent_t a0, cudaEvent_t a1)
+                            const LoopCond& lc, cudaStream_t st, cudaEvent_t a0, cudaEvent_t a1)
 {
     const int hist_bytes = v.hist_smem * 4;
     const int sms = v.n_sms;
     if (a0) cudaEventRecord(a0, st);
     if (v.cull) {
-        const int g = std::max(1, std::min(v.n_chunks, sms * 8));
-        if (tp.cull_items == 2) k_assign_cull<DIM, 2><<<g, AC_BLOCK, 0, st>>>(v);
-        else if (tp.cull_items == 8) k_assign_cull<DIM, 8><<<g, AC_BLOCK, 0, st>>>(v);
-        else k_assign_cull<DIM, 4><<<g, AC_BLOCK, 0, st>>>(v);
+        if (tp.cull_items == 2) launch_assign_cull<DIM, 2>(v, st);
+        else if (tp.cull_items == 8) launch_assign_cull<DIM, 8>(v, st);
+        else launch_assign_cull<DIM, 4>(v, st);
     } else {
 #define RD_ASSIGN_CASE(B, I)                                                                  \
     if (tp.block == B && tp.items == I) {                                                     \
@@ -2039,15 +2376,12 @@ cudaError_t launch_pass_dim(const EngineView& v, const TuneParams& tp, int assig
 #undef RD_ASSIGN_CASE
     }
     if (a1) cudaEventRecord(a1, st);
-    if (v.cull && v.n_chunks > 0)
-        k_keyhist<<<std::min(v.n_chunks, sms * 4), KH_BLOCK, hist_bytes, st>>>(v);
     // fixed grids; every kernel walks only the current work lists
     if (v.n_kblk > 0) k_chunkscan_cta<<<std::min(v.n_kblk, sms * 4), CS_W * 32, 0, st>>>(v);
     if (v.n_kblk_warp > 0)
         k_chunkscan_warp<<<std::min((v.n_kblk_warp + CSW_W - 1) / CSW_W, sms * 8), CSW_W * 32, 0, st>>>(v);
-    k_keybase<1024><<<std::min(v.n_clouds, sms * 2), 1024, 0, st>>>(v);
     if (v.n_chunks > 0)
-        k_scatter_cta<<<std::min(v.n_chunks, sms * 8), SCAT_W * 32, scatter_cta_smem_bytes(v), st>>>(v);
+        k_scatter_cta<DIM><<<std::min(v.n_chunks, sms * 8), SCAT_W * 32, scatter_cta_smem_bytes(v), st>>>(v);
     if (v.n_slots > 0) {
         // at most (points / SUM_BIG_MIN) keys can be big
         const int big_ctas = (int)std::min<int64_t>(
@@ -2056,7 +2390,8 @@ cudaError_t launch_pass_dim(const EngineView& v, const TuneParams& tp, int assig
     } else {
         k_control<<<std::min((v.n_clouds + 255) / 256, sms), 256, 0, st>>>(v);
     }
-    k_decimate<DIM, 512><<<std::min(v.n_groups, sms * 2), 512, dec_smem_bytes(v), st>>>(v);
+    k_decimate<DIM, 512><<<std::min(v.n_groups, sms * 2), 512, dec_smem_bytes(v), st>>>(
+        v, lc.h, 1, lc.use_handle);
     return cudaGetLastError();
 }
 
@@ -2138,10 +2473,10 @@ cudaError_t prepare_pass(int dim, const EngineView& v, const TuneParams& tp)
 }
 
 cudaError_t launch_pass(int dim, const EngineView& v, const TuneParams& tp, int assign_grid,
-                        cudaStream_t st, cudaEvent_t a0, cudaEvent_t a1)
+                        const LoopCond& lc, cudaStream_t st, cudaEvent_t a0, cudaEvent_t a1)
 {
     return with_dim(dim, [&](auto D) {
-        return launch_pass_dim<decltype(D)::value>(v, tp, assign_grid, st, a0, a1);
+        return launch_pass_dim<decltype(D)::value>(v, tp, assign_grid, lc, st, a0, a1);
     });
 }
 
@@ -2217,8 +2552,8 @@ cudaError_t prepare_tile_pass(int dim, const EngineView& v, int* cl_grid)
     });
 }
 
-cudaError_t launch_tile_pass(int dim, const EngineView& v, cudaStream_t st, cudaEvent_t a0,
-                             cudaEvent_t a1)
+cudaError_t launch_tile_pass(int dim, const EngineView& v, const LoopCond& lc, cudaStream_t st,
+                             cudaEvent_t a0, cudaEvent_t a1)
 {
     const int smem = tile_evolve_smem_bytes(dim);
     const int grid = std::max(1, std::min(v.n_clouds, v.n_sms * 3));
@@ -2238,7 +2573,7 @@ cudaError_t launch_tile_pass(int dim, const EngineView& v, cudaStream_t st, cuda
         }
         if (a1) cudaEventRecord(a1, st);
         launch_decbig<DIM>(v, st);
-        k_decimate<DIM, 512><<<dgrid, 512, dec_smem_bytes(v), st>>>(v);
+        k_decimate<DIM, 512><<<dgrid, 512, dec_smem_bytes(v), st>>>(v, lc.h, 1, lc.use_handle);
         return cudaGetLastError();
     });
 }
@@ -2302,7 +2637,7 @@ cudaError_t launch_decimate(int dim, const EngineView& v, cudaStream_t st)
         constexpr int DIM = decltype(D)::value;
         cudaError_t r = cudaFuncSetAttribute(k_decimate<DIM, 512>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (r == cudaSuccess) k_decimate<DIM, 512><<<grid, 512, smem, st>>>(v);
+        if (r == cudaSuccess) k_decimate<DIM, 512><<<grid, 512, smem, st>>>(v, 0, 0, 0);
         return r;
     });
     if (e != cudaSuccess) return e;
@@ -2324,9 +2659,8 @@ cudaError_t launch_evolve_step_dim(const EngineView& v, const TuneParams& tp, in
     if (v.n_kblk > 0) k_chunkscan_cta<<<std::min(v.n_kblk, sms * 4), CS_W * 32, 0, st>>>(v);
     if (v.n_kblk_warp > 0)
         k_chunkscan_warp<<<std::min((v.n_kblk_warp + CSW_W - 1) / CSW_W, sms * 8), CSW_W * 32, 0, st>>>(v);
-    k_keybase<1024><<<std::min(v.n_clouds, sms * 2), 1024, 0, st>>>(v);
     if (v.n_chunks > 0)
-        k_scatter_cta<<<std::min(v.n_chunks, sms * 8), SCAT_W * 32, scatter_cta_smem_bytes(v), st>>>(v);
+        k_scatter_cta<DIM><<<std::min(v.n_chunks, sms * 8), SCAT_W * 32, scatter_cta_smem_bytes(v), st>>>(v);
     if (v.n_slots > 0) {
         // at most (points / SUM_BIG_MIN) keys can be big
         const int big_ctas = (int)std::min<int64_t>(

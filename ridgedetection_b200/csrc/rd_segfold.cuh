@@ -38,6 +38,81 @@ namespace {
 
 constexpr int SEG_TR = 6;                 // trace entries per (segment, coordinate)
 
+// Where the members of a list live.  IdxSrc: member i is point mem[i] of P
+// (DIM floats per point), so a load is an index load and a dependent
+// coordinate load.  RowSrc: member i is row i of a grouped copy (PadDim<DIM>
+// floats per row, DIM 3 as float4), laid out by the stable scatter of the
+// lockstep passes, so a list is one contiguous stream.  Both give the same
+// values in the same order.
+template <int DIM>
+struct IdxSrc {
+    const int32_t* __restrict__ mem;
+    const float* __restrict__ P;
+    // members off + j, j < m, into x[.][j] (zeros beyond m)
+    template <int L>
+    __device__ __forceinline__ void load_run(int off, int m, float (&x)[DIM][L]) const
+    {
+        int ix[L];
+#pragma unroll
+        for (int j = 0; j < L; ++j) ix[j] = (j < m) ? mem[off + j] : -1;
+#pragma unroll
+        for (int j = 0; j < L; ++j)
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) x[d][j] = (ix[j] >= 0) ? P[(int64_t)ix[j] * DIM + d] : 0.0f;
+    }
+    template <int L>
+    __device__ __forceinline__ void load_run1(int off, int m, int d, float (&x)[L]) const
+    {
+        int ix[L];
+#pragma unroll
+        for (int j = 0; j < L; ++j) ix[j] = (j < m) ? mem[off + j] : -1;
+#pragma unroll
+        for (int j = 0; j < L; ++j) x[j] = (ix[j] >= 0) ? P[(int64_t)ix[j] * DIM + d] : 0.0f;
+    }
+};
+
+template <int DIM>
+struct RowSrc {
+    const float* __restrict__ rows;
+    __device__ __forceinline__ void load_row(int i, float (&x)[DIM]) const
+    {
+        if constexpr (PadDim<DIM>::v == 4) {
+            const float4 t = reinterpret_cast<const float4*>(rows)[i];
+            x[0] = t.x;
+            if constexpr (DIM > 1) x[1] = t.y;
+            if constexpr (DIM > 2) x[2] = t.z;
+            if constexpr (DIM > 3) x[3] = t.w;
+        } else if constexpr (DIM == 2) {
+            const float2 t = reinterpret_cast<const float2*>(rows)[i];
+            x[0] = t.x;
+            x[1] = t.y;
+        } else {
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) x[d] = rows[(int64_t)i * PadDim<DIM>::v + d];
+        }
+    }
+    template <int L>
+    __device__ __forceinline__ void load_run(int off, int m, float (&x)[DIM][L]) const
+    {
+#pragma unroll
+        for (int j = 0; j < L; ++j) {
+            float r[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) r[d] = 0.0f;
+            if (j < m) load_row(off + j, r);
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) x[d][j] = r[d];
+        }
+    }
+    template <int L>
+    __device__ __forceinline__ void load_run1(int off, int m, int d, float (&x)[L]) const
+    {
+#pragma unroll
+        for (int j = 0; j < L; ++j)
+            x[j] = (j < m) ? rows[(int64_t)(off + j) * PadDim<DIM>::v + d] : 0.0f;
+    }
+};
+
 enum : int { SK_RUN = 0, SK_EXACT = 1, SK_ABORT = 2 };
 
 struct SegEntry {
@@ -48,7 +123,7 @@ struct SegEntry {
     int pad[3];
 };
 
-struct SegTrace {
+struct alignas(16) SegTrace {
     float start;  // speculative start value
     float fin;    // speculative end value
     int n;        // entries
@@ -185,10 +260,9 @@ __device__ __forceinline__ float fold_chunk_traced(float s, const float (&x)[L],
 // point) from the start values s[d] (warp-uniform), recording the trace of
 // coordinate d in tr[d]; tr[d].start/fin/n are written by lane 0.  The next
 // chunk's indices and coordinates are loaded while a chunk is folded.
-template <int DIM>
-__device__ void warp_fold_traced(const int32_t* __restrict__ mem, const int b, const int e,
-                                 const float* __restrict__ P, float (&s)[DIM], SegTrace* tr,
-                                 const int lane)
+template <int DIM, class Src>
+__device__ void warp_fold_traced_src(const Src& src, const int b, const int e, float (&s)[DIM],
+                                     SegTrace* tr, const int lane)
 {
     constexpr int L = FOLD_L, C = FOLD_C;
     SegRec rec[DIM];
@@ -202,13 +276,7 @@ __device__ void warp_fold_traced(const int32_t* __restrict__ mem, const int b, c
     auto gather = [&](float (&x)[DIM][L], int& m, int off) {
         const int mtot = min(C, e - off);
         m = (off < e) ? max(0, min(L, mtot - lane * L)) : 0;
-        int ix[L];
-#pragma unroll
-        for (int j = 0; j < L; ++j) ix[j] = (j < m) ? mem[off + lane * L + j] : -1;
-#pragma unroll
-        for (int j = 0; j < L; ++j)
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) x[d][j] = (ix[j] >= 0) ? P[(int64_t)ix[j] * DIM + d] : 0.0f;
+        src.template load_run<L>(off + lane * L, m, x);
     };
     if (b < e) gather(xn, mn_, b);
     for (int off = b; off < e; off += C) {
@@ -234,31 +302,46 @@ __device__ void warp_fold_traced(const int32_t* __restrict__ mem, const int b, c
     }
 }
 
-// One warp folds members [from, to) of the list exactly (coordinate d) into
-// the warp-uniform s, a chunk of FOLD_C members at a time.
 template <int DIM>
-__device__ float fold_range_exact(const int32_t* __restrict__ mem, int from, const int to,
-                                  const float* __restrict__ P, const int d, float s, const int lane)
+__device__ __forceinline__ void warp_fold_traced(const int32_t* __restrict__ mem, const int b,
+                                                 const int e, const float* __restrict__ P,
+                                                 float (&s)[DIM], SegTrace* tr, const int lane)
+{
+    warp_fold_traced_src<DIM>(IdxSrc<DIM>{mem, P}, b, e, s, tr, lane);
+}
+
+// One warp folds members [from, to) of the list exactly (coordinate d) into
+// the warp-uniform s, a chunk of FOLD_C members at a time; the next chunk's
+// indices and coordinates are in flight while a chunk is folded.
+template <int DIM, class Src>
+__device__ float fold_range_exact(const Src& src, int from, const int to, const int d, float s,
+                                  const int lane)
 {
     constexpr int L = FOLD_L, C = FOLD_C;
+    auto gather = [&](float (&x)[L], int& m, int off) {
+        const int mtot = min(C, to - off);
+        m = max(0, min(L, mtot - lane * L));
+        src.template load_run1<L>(off + lane * L, m, d, x);
+    };
+    float xn[L];
+    int mn = 0;
+    if (from < to) gather(xn, mn, from);
     for (; from < to; from += C) {
-        const int mtot = min(C, to - from);
-        const int m = max(0, min(L, mtot - lane * L));
-        float x[L];
+        float xc[L];
 #pragma unroll
-        for (int j = 0; j < L; ++j)
-            x[j] = (j < m) ? P[(int64_t)mem[from + lane * L + j] * DIM + d] : 0.0f;
-        s = fold_chunk<L>(s, x, m, lane);
+        for (int j = 0; j < L; ++j) xc[j] = xn[j];
+        const int mc = mn;
+        if (from + C < to) gather(xn, mn, from + C);
+        s = fold_chunk<L>(s, xc, mc, lane);
     }
     return s;
 }
 
 // The exact value after segment [b, e) of the list for the exact start s,
 // from the segment's trace (which may live in another CTA's shared memory).
-template <int DIM>
-__device__ float replay_segment(const SegTrace& tr, const int32_t* __restrict__ mem, const int b,
-                                const int e, const float* __restrict__ P, const int d, float s,
-                                const int lane)
+template <int DIM, class Src>
+__device__ float replay_segment_src(const SegTrace& tr, const Src& src, const int b, const int e,
+                                    const int d, float s, const int lane)
 {
     if (__float_as_int(s) == __float_as_int(tr.start)) return tr.fin;
     const int n = tr.n;
@@ -273,34 +356,98 @@ __device__ float replay_segment(const SegTrace& tr, const int32_t* __restrict__ 
                 off += en.m;
                 continue;
             }
-            return fold_range_exact<DIM>(mem, off, e, P, d, s, lane);
+            return fold_range_exact<DIM>(src, off, e, d, s, lane);
         }
         if (kind == SK_EXACT) {
-            s = fold_range_exact<DIM>(mem, off, off + en.m, P, d, s, lane);
+            s = fold_range_exact<DIM>(src, off, off + en.m, d, s, lane);
             off += en.m;
             continue;
         }
-        return fold_range_exact<DIM>(mem, off, e, P, d, s, lane);   // ABORT
+        return fold_range_exact<DIM>(src, off, e, d, s, lane);   // ABORT
     }
     return s;
 }
 
-// FP64 sum of members [b, e) of the list, by one warp; lane 0 holds it.
 template <int DIM>
-__device__ void warp_sum64(const int32_t* __restrict__ mem, const int b, const int e,
-                           const float* __restrict__ P, double (&acc)[DIM], const int lane)
+__device__ __forceinline__ float replay_segment(const SegTrace& tr, const int32_t* __restrict__ mem,
+                                                const int b, const int e,
+                                                const float* __restrict__ P, const int d, float s,
+                                                const int lane)
+{
+    return replay_segment_src<DIM>(tr, IdxSrc<DIM>{mem, P}, b, e, d, s, lane);
+}
+
+// FP64 sum of members [b, e) of the list, by one warp; every lane holds it.
+// SUM64_U members per lane are gathered before any of them is added, so the
+// dependent index-then-coordinate loads of a step overlap instead of queueing
+// behind the add chain.
+constexpr int SUM64_U = 8;
+
+template <int DIM>
+__device__ void warp_sum64_add(const IdxSrc<DIM>& src, const int b, const int e,
+                               double (&acc)[DIM], const int lane)
+{
+    constexpr int U = SUM64_U;
+    for (int i0 = b; i0 < e; i0 += 32 * U) {
+        int ix[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int i = i0 + u * 32 + lane;
+            ix[u] = (i < e) ? src.mem[i] : -1;
+        }
+        float x[U][DIM];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int d = 0; d < DIM; ++d)
+                x[u][d] = (ix[u] >= 0) ? src.P[(int64_t)ix[u] * DIM + d] : 0.0f;
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) acc[d] += (double)x[u][d];
+    }
+}
+
+template <int DIM>
+__device__ void warp_sum64_add(const RowSrc<DIM>& src, const int b, const int e,
+                               double (&acc)[DIM], const int lane)
+{
+    constexpr int U = SUM64_U;
+    for (int i0 = b; i0 < e; i0 += 32 * U) {
+        float x[U][DIM];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int i = i0 + u * 32 + lane;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) x[u][d] = 0.0f;
+            if (i < e) src.load_row(i, x[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) acc[d] += (double)x[u][d];
+    }
+}
+
+template <int DIM, class Src>
+__device__ void warp_sum64_src(const Src& src, const int b, const int e, double (&acc)[DIM],
+                               const int lane)
 {
 #pragma unroll
     for (int d = 0; d < DIM; ++d) acc[d] = 0.0;
-    for (int i = b + lane; i < e; i += 32) {
-        const int64_t p = (int64_t)mem[i] * DIM;
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) acc[d] += (double)P[p + d];
-    }
+    warp_sum64_add<DIM>(src, b, e, acc, lane);
 #pragma unroll
     for (int d = 0; d < DIM; ++d)
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) acc[d] += __shfl_xor_sync(0xffffffffu, acc[d], o);
+}
+
+template <int DIM>
+__device__ __forceinline__ void warp_sum64(const int32_t* __restrict__ mem, const int b,
+                                           const int e, const float* __restrict__ P,
+                                           double (&acc)[DIM], const int lane)
+{
+    warp_sum64_src<DIM>(IdxSrc<DIM>{mem, P}, b, e, acc, lane);
 }
 
 // ---------------------------------------------------------------------------
@@ -315,14 +462,13 @@ struct SegFoldSmem {
     float out[DIM];
 };
 
-template <int W, int DIM>
-__device__ void fold_members_seg(const int32_t* __restrict__ mem, const int n,
-                                 const float* __restrict__ P, SegFoldSmem<W, DIM>& sm)
+template <int W, int DIM, class Src>
+__device__ void fold_members_seg_src(const Src& src, const int n, SegFoldSmem<W, DIM>& sm)
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int b = (int)(((int64_t)warp * n) / W), e = (int)(((int64_t)(warp + 1) * n) / W);
     double acc[DIM];
-    warp_sum64<DIM>(mem, b, e, P, acc, lane);
+    warp_sum64_src<DIM>(src, b, e, acc, lane);
     if (lane == 0)
 #pragma unroll
         for (int d = 0; d < DIM; ++d) sm.part[warp][d] = acc[d];
@@ -334,18 +480,26 @@ __device__ void fold_members_seg(const int32_t* __restrict__ mem, const int n,
         for (int w = 0; w < warp; ++w) est += sm.part[w][d];
         s[d] = (warp == 0) ? 0.0f : (float)est;
     }
-    warp_fold_traced<DIM>(mem, b, e, P, s, sm.tr[warp], lane);
+    warp_fold_traced_src<DIM>(src, b, e, s, sm.tr[warp], lane);
     __syncthreads();
     if (warp < DIM) {
         const int d = warp;
         float x = sm.tr[0][d].fin;   // segment 0 started exactly at 0
         for (int w = 1; w < W; ++w) {
             const int bw = (int)(((int64_t)w * n) / W), ew = (int)(((int64_t)(w + 1) * n) / W);
-            x = replay_segment<DIM>(sm.tr[w][d], mem, bw, ew, P, d, x, lane);
+            x = replay_segment_src<DIM>(sm.tr[w][d], src, bw, ew, d, x, lane);
         }
         if (lane == 0) sm.out[d] = x;
     }
     __syncthreads();
+}
+
+template <int W, int DIM>
+__device__ __forceinline__ void fold_members_seg(const int32_t* __restrict__ mem, const int n,
+                                                 const float* __restrict__ P,
+                                                 SegFoldSmem<W, DIM>& sm)
+{
+    fold_members_seg_src<W, DIM>(IdxSrc<DIM>{mem, P}, n, sm);
 }
 
 }  // namespace

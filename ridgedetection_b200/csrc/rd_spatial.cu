@@ -7,7 +7,8 @@
 // within r1 of the group's bounding box.  This file builds, once per run (the
 // evolve points never move), a copy of every cloud's points in a spatial
 // order -- cells of edge r1/4, Morton order of the cells, the packed slot
-// order inside a cell.
+// order inside a cell.  The copy pads DIM 3 to four floats per point, so that
+// a point is one 16-byte load.
 #include "rd_engine.cuh"
 
 #include <cub/cub.cuh>
@@ -88,11 +89,14 @@ template <int DIM>
 __global__ void __launch_bounds__(256) k_gather_spatial(EngineView v, int64_t n, const int32_t* val,
                                                         float* Ps, int32_t* sorder)
 {
+    constexpr int DP = PadDim<DIM>::v;
     for (int64_t pos = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; pos < n;
          pos += (int64_t)gridDim.x * blockDim.x) {
         const int32_t s = val[pos];
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) Ps[pos * DIM + d] = v.P[(int64_t)s * DIM + d];
+        for (int d = 0; d < DIM; ++d) Ps[pos * DP + d] = v.P[(int64_t)s * DIM + d];
+#pragma unroll
+        for (int d = DIM; d < DP; ++d) Ps[pos * DP + d] = 0.0f;
         sorder[pos] = s;
     }
 }

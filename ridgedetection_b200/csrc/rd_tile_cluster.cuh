@@ -14,7 +14,7 @@
 //   grouping     per-CTA key counts are exchanged through distributed shared
 //                memory; every CTA derives the key bases and the offset of its
 //                own members inside each key, so the stable placement into
-//                perm (index order inside every key) needs no further exchange;
+//                Pg (index order inside every key) needs no further exchange;
 //   folds        a key with tile_seg_min+ members is folded in TCL x W
 //                segments of its member list, one per warp of the cluster: each
 //                warp folds its segment from a speculative start (the FP64 sum
@@ -87,7 +87,6 @@ __device__ void tile_evolve_cluster(const EngineView& v, const int c, unsigned c
     int* hist = reinterpret_cast<int*>(sS + TILE_NS_MAX * DP);
     int* kbase = hist + W * (TILE_NS_MAX + 1);
     auto& s_buf = ts.buf;
-    auto& s_idx = ts.idx;
     auto& s_seg = ts.seg;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     static_assert(W == TCL_W, "the cluster smem holds TCL_W warp segments per CTA");
@@ -97,7 +96,7 @@ __device__ void tile_evolve_cluster(const EngineView& v, const int c, unsigned c
     const float* P = v.P + cd.p_off * DIM;
     float* gS = v.S + cd.s_off * DIM;
     int32_t* keys = v.keys + cd.p_off;
-    int32_t* perm = v.perm + cd.p_off;
+    float* Pg = v.Pg + cd.p_off * DP;   // coordinates grouped by key, shared by the cluster
     const float rsq = sqr_rn(cd.r1);
     const int nsp = (ns + KB - 1) / KB * KB;
     __syncthreads();
@@ -172,9 +171,9 @@ __device__ void tile_evolve_cluster(const EngineView& v, const int c, unsigned c
         }
         __syncthreads();
         // 3. stable placement of this CTA's members (as tile_evolve_one)
-        tile_place_range<DIM>(keys, r0, r1w, hist + warp * (TILE_NS_MAX + 1), ns, perm, lane);
+        tile_place_range<DIM>(P, keys, r0, r1w, hist + warp * (TILE_NS_MAX + 1), ns, Pg, lane);
         const int nseg = cs.nseg;
-        cl.sync();   // perm complete in the cluster
+        cl.sync();   // Pg complete in the cluster
         // FP64 sums of this CTA's warp segments of every segmented key; a key's
         // list is cut into TCL x W segments, segment g = rank * W + warp
         constexpr int NSEG = TCL * W;
@@ -183,7 +182,7 @@ __device__ void tile_evolve_cluster(const EngineView& v, const int c, unsigned c
             const int g = rank * W + warp;
             const int b = (int)(((int64_t)g * cnt) / NSEG), e = (int)(((int64_t)(g + 1) * cnt) / NSEG);
             double acc[DIM];
-            warp_sum64<DIM>(perm + kbase[k], b, e, P, acc, lane);
+            warp_sum64_src<DIM>(RowSrc<DIM>{Pg + (int64_t)kbase[k] * DP}, b, e, acc, lane);
             if (lane == 0)
 #pragma unroll
                 for (int d = 0; d < DIM; ++d) cs.part[j][warp][d] = acc[d];
@@ -210,7 +209,8 @@ __device__ void tile_evolve_cluster(const EngineView& v, const int c, unsigned c
                 for (int w = 0; w < warp; ++w) est += cs.part[j][w][d];
                 s0[d] = (g == 0) ? 0.0f : (float)est;
             }
-            warp_fold_traced<DIM>(perm + kbase[k], b, e, P, s0, cs.wtr[j][warp], lane);
+            warp_fold_traced_src<DIM>(RowSrc<DIM>{Pg + (int64_t)kbase[k] * DP}, b, e, s0, cs.wtr[j][warp],
+                                      lane);
         }
         // 4b. the other keys this CTA owns (key k belongs to CTA k % TCL)
         auto is_seg = [&](int k) {
@@ -221,7 +221,7 @@ __device__ void tile_evolve_cluster(const EngineView& v, const int c, unsigned c
         for (int k = rank; k < ns; k += TCL) {
             const int cnt = cs.kcnt[k];
             if (cnt < FOLD_CTA_MIN || is_seg(k)) continue;
-            fold_members_seg<W, DIM>(perm + kbase[k], cnt, P, s_seg);
+            fold_members_seg_src<W, DIM>(RowSrc<DIM>{Pg + (int64_t)kbase[k] * DP}, cnt, s_seg);
             if (warp == 0) {
                 int mv = 0;
                 if (lane < DIM) {
@@ -238,7 +238,7 @@ __device__ void tile_evolve_cluster(const EngineView& v, const int c, unsigned c
             const int k = rank + q * TCL;
             const int cnt = cs.kcnt[k];
             if (cnt == 0 || cnt >= FOLD_CTA_MIN || is_seg(k)) continue;
-            const float sum = fold_members<DIM>(perm + kbase[k], cnt, P, s_buf[warp], s_idx[warp], lane);
+            const float sum = fold_rows<DIM, SUM_BP>(Pg + (int64_t)kbase[k] * DP, cnt, s_buf[warp], lane);
             int moved = 0;
             float cval = 0.0f;
             if (lane < DIM) {
@@ -252,17 +252,37 @@ __device__ void tile_evolve_cluster(const EngineView& v, const int c, unsigned c
         cl.sync();   // traces and owned results visible
         // 4c. composition of the segmented keys: key j by CTA j % TCL, warp d,
         //     replaying the TCL x W segment traces in order from the exact start
+        //     The warp first copies the NSEG traces of its coordinate from the
+        //     cluster's shared memory into this CTA's histogram area (free
+        //     until the next pass), so the sequential replay reads local
+        //     shared memory instead of making one remote round trip per
+        //     segment; coordinates whose traces do not fit there read them
+        //     in place.
+        constexpr int TR16 = (int)(sizeof(SegTrace) / 16);   // 16-byte words per trace
+        constexpr bool STAGE = DIM * NSEG * (int)sizeof(SegTrace) <= W * (TILE_NS_MAX + 1) * 4;
         for (int j = rank; j < nseg; j += TCL) {
             if (warp >= DIM) break;
             const int d = warp;
             const int k = cs.segk[j], cnt = cs.kcnt[k];
-            const int32_t* mem = perm + kbase[k];
-            float x = cl.map_shared_rank(&cs, 0)->wtr[j][0][d].fin;   // segment 0 started at 0
+            const RowSrc<DIM> rows{Pg + (int64_t)kbase[k] * DP};
+            SegTrace* loc = reinterpret_cast<SegTrace*>(hist) + d * NSEG;
+            if constexpr (STAGE) {
+                for (int t = lane; t < NSEG * TR16; t += 32) {
+                    const int g = t / TR16, o = t - (t / TR16) * TR16;
+                    const int4* src = reinterpret_cast<const int4*>(
+                        &cl.map_shared_rank(&cs, g / W)->wtr[j][g % W][d]);
+                    reinterpret_cast<int4*>(loc + g)[o] = src[o];
+                }
+                __syncwarp();
+            }
+            auto trace = [&](int g) -> const SegTrace& {
+                if constexpr (STAGE) return loc[g];
+                else return cl.map_shared_rank(&cs, g / W)->wtr[j][g % W][d];
+            };
+            float x = trace(0).fin;   // segment 0 started at 0
             for (int g = 1; g < NSEG; ++g) {
-                const int q = g / W, w = g % W;
                 const int b = (int)(((int64_t)g * cnt) / NSEG), e = (int)(((int64_t)(g + 1) * cnt) / NSEG);
-                x = replay_segment<DIM>(cl.map_shared_rank(&cs, q)->wtr[j][w][d], mem, b, e, P, d, x,
-                                        lane);
+                x = replay_segment_src<DIM>(trace(g), rows, b, e, d, x, lane);
             }
             if (lane == 0) {
                 float cval = sS[k * DP + d];
