@@ -663,6 +663,10 @@ def run_b200_tiled(args, world, rank, local, embedded=False):
         "evolve_pairs_per_s": world * pairs_step / (ms_max * 1e-3),
         "pairs_per_step": pairs_step, "ns_final": ns_final,
         "timers_ms": timers,
+        # the global decimation: its passes are resolved in parallel rounds
+        # (per solve, from the profiling solve)
+        "decimation": {"passes": int(pst.dec_passes), "rounds": int(pst.dec_rounds),
+                       "rounds_per_pass": pst.dec_rounds / max(1, pst.dec_passes)},
         "roofline": {"bound": "hbm", "kernel": "k_tile_evolve", "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_src,

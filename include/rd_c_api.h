@@ -66,6 +66,8 @@ typedef struct rd_run_stats {
     int64_t assign_launches;/* profiling runs only: assign-kernel launches timed     */
     double  point_passes;   /* sum over clouds of (points x evolve passes): point   */
                             /* coordinates the assignment streams, in points        */
+    int64_t dec_passes;     /* decimation passes resolved in parallel rounds         */
+    int64_t dec_rounds;     /* rounds those passes took                              */
 } rd_run_stats;
 
 RD_API const char* rd_last_error(void);
@@ -107,8 +109,9 @@ RD_API rd_status rd_get_assign_cull(int* enable);
  * and changes no result).  In tiled runs, a tile with at least min_points
  * evolve points (own + halo) is evolved by a thread-block cluster of 8 CTAs
  * instead of one CTA, and each of its keys with at least seg_min members is
- * folded in 8 segments whose exact FP32 sums are composed in index order.
- * enable = 0: one CTA per tile.  0 for a threshold keeps its default (24,576
+ * folded in 64 warp segments (8 per CTA) whose exact FP32 sums are composed
+ * in index order.
+ * enable = 0: one CTA per tile.  0 for a threshold keeps its default (100,000
  * points, 8,192 members).  Process-wide, read when a run starts. */
 RD_API rd_status rd_set_tile_clusters(int enable, int64_t min_points, int64_t seg_min);
 RD_API rd_status rd_get_tile_clusters(int* enable, int64_t* min_points, int64_t* seg_min);
@@ -119,8 +122,9 @@ RD_API rd_status rd_get_tile_clusters(int* enable, int64_t* min_points, int64_t*
  * passes (the shape sets the assignment's launch and the chunking of the
  * grouping that follows it; the run's one-time setup is left out); five runs
  * per shape, interleaved over the shapes; the shape with the lowest median
- * time per pass wins -- unless the table already holds a shape for this (dim,
- * n, r1) bucket that is within 3% of it, which is kept.  Stores the pick for
+ * time per pass wins, shapes within 2% of it counting as tied (the first of
+ * them in the supported order is taken) -- unless the table already holds a
+ * shape for this (dim, n, r1) bucket that is within 3% of it, which is kept.  Stores the pick for
  * the bucket and returns it with its median time per pass in microseconds.
  * Runs on `stream` and waits for it; d_P is not modified. */
 RD_API rd_status rd_autotune(int dim, const float* d_P, int64_t n, int64_t ns, float r1, int reps,

@@ -40,7 +40,8 @@ class RunStats(ctypes.Structure):
                 ("max_passes", ctypes.c_int64), ("pairs", ctypes.c_double),
                 ("err_bits", ctypes.c_int32), ("pad", ctypes.c_int32),
                 ("assign_ms", ctypes.c_double), ("assign_launches", ctypes.c_int64),
-                ("point_passes", ctypes.c_double)]
+                ("point_passes", ctypes.c_double), ("dec_passes", ctypes.c_int64),
+                ("dec_rounds", ctypes.c_int64)]
 
 
 class CloudDesc(ctypes.Structure):

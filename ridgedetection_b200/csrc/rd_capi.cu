@@ -162,6 +162,8 @@ void fill_stats(const RunStats& s, rd_run_stats* o)
     o->assign_ms = s.assign_ms;
     o->assign_launches = s.assign_launches;
     o->point_passes = s.point_passes;
+    o->dec_passes = s.dec_passes;
+    o->dec_rounds = s.dec_rounds;
 }
 
 // independent FMA chains: 8 per thread, ITER rounds
@@ -220,7 +222,7 @@ extern "C" {
 
 const char* rd_last_error(void) { return g_err.c_str(); }
 
-int rd_abi_version(void) { return 2; }
+int rd_abi_version(void) { return 3; }
 
 int rd_supported_dims(void)
 {
@@ -385,6 +387,15 @@ rd_status rd_autotune(int dim, const float* d_P, int64_t n, int64_t ns, float r1
         med[ci] = median(ms[ci]);
         if (med[ci] < med[bi]) bi = ci;
     }
+    // shapes within 2% of the fastest count as tied: the first of them in the
+    // fixed candidate order is taken, so that runs that see the same timings
+    // up to noise pick the same shape
+    const float best = med[bi];
+    for (size_t ci = 0; ci < cand.size(); ++ci)
+        if (med[ci] <= 1.02f * best) {
+            bi = ci;
+            break;
+        }
     // keep the shape already in the table unless the new one is 3% faster
     TuneParams inc;
     if (tune_find_exact(dim, n, r1, &inc)) {

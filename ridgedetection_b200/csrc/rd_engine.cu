@@ -685,6 +685,8 @@ int Engine::collect(cudaStream_t st)
     RD_CK(cudaStreamSynchronize(st));
     stats_.loop_iters = ctr[CTR_ITERS];
     stats_.err_bits = ctr[CTR_ERR];
+    stats_.dec_passes = ctr[CTR_DEC_PASSES];
+    stats_.dec_rounds = ctr[CTR_DEC_ROUNDS];
     for (size_t c = 0; c < nc; ++c) {
         stats_.total_passes += tp[c];
         stats_.max_passes = std::max<int64_t>(stats_.max_passes, tp[c]);

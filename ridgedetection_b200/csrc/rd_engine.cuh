@@ -58,7 +58,9 @@ enum : int {
     CTR_TILE_HEAVY = 7,// heavy-tile ticket of the cluster tile kernel
     CTR_SUM_DONE = 8,  // CTAs of k_sum_shift finished (the last one runs the control step)
     CTR_DEC_DONE = 9,  // CTAs of k_decimate finished (the last one sets the loop condition)
-    CTR_COUNT = 10,
+    CTR_DEC_PASSES = 10,  // decimation passes resolved in parallel rounds (this run)
+    CTR_DEC_ROUNDS = 11,  // rounds they took
+    CTR_COUNT = 12,
 };
 
 struct EngineView {

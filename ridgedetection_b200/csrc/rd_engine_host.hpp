@@ -55,6 +55,8 @@ struct RunStats {
                                   // of the assign kernels (of whole iterations)
     int64_t assign_launches = 0;
     double point_passes = 0;      // sum over clouds of n_all * evolve passes
+    int64_t dec_passes = 0;       // decimation passes resolved in parallel rounds
+    int64_t dec_rounds = 0;       // rounds they took
 };
 
 // Process-wide tuning table: (dim, size bucket, r1 bucket) -> assignment

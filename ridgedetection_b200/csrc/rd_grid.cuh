@@ -255,10 +255,11 @@ __device__ __forceinline__ void dec_for_neighbours(const int i, const float* X,
 // State per point st[i]: 0 dead, 1 alive (undecided in a pass), 2 kept in
 // this pass, 3 removed in this pass; counts c1/c2 of alive points are exact
 // between passes.  Returns the alive count.  All threads of the block call it.
+// tally (optional): tally[0] += passes resolved, tally[1] += rounds they took.
 template <int BLOCK, class CT, class ST>
 __device__ int decimate_round_passes(const int total, int cnt, CT* c1, CT* c2, ST* st_,
                                      const int32_t* nb_off, const int32_t* nb, int* fallback,
-                                     int32_t* err)
+                                     int32_t* err, int32_t* tally = nullptr)
 {
     volatile ST* st = st_;
     const int tid = threadIdx.x;
@@ -292,6 +293,7 @@ __device__ int decimate_round_passes(const int total, int cnt, CT* c1, CT* c2, S
                 else if (a < 4 && b - und2 >= 3) st[i] = 2;
                 else und_left = 1;
             }
+            if (tally && tid == 0) atomicAdd(&tally[1], 1);
             if (!__syncthreads_or(und_left)) break;
             if (round > total) {   // cannot happen: every round decides a point
                 if (tid == 0) atomicOr(err, ERRB_DEC_CAP);
@@ -299,7 +301,10 @@ __device__ int decimate_round_passes(const int total, int cnt, CT* c1, CT* c2, S
             }
         }
         __shared__ int s_removed;
-        if (tid == 0) s_removed = 0;
+        if (tid == 0) {
+            s_removed = 0;
+            if (tally) atomicAdd(&tally[0], 1);
+        }
         __syncthreads();
         int mine = 0;
         for (int i = tid; i < total; i += BLOCK) mine += (st[i] == 3);
@@ -352,7 +357,7 @@ __device__ void decimate_scan_lists(const float* X, const int total, const float
                                     int32_t* c2g, int32_t* items, int32_t* bstart,
                                     const uint32_t hmask, int32_t* nb_off, int32_t* nb,
                                     const int64_t nb_cap, unsigned char* smem, const int smem_max,
-                                    int32_t* err, const int prepared = 0)
+                                    int32_t* err, const int prepared = 0, int32_t* tally = nullptr)
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const float rsq = sqr_rn(r2);
@@ -479,8 +484,8 @@ __device__ void decimate_scan_lists(const float* X, const int total, const float
     {
         int fb = 0;
         const int left = in_smem
-            ? decimate_round_passes<BLOCK>(total, total, c1s, c2s, as, nb_off, nb, &fb, err)
-            : decimate_round_passes<BLOCK>(total, total, c1g, c2g, alive, nb_off, nb, &fb, err);
+            ? decimate_round_passes<BLOCK>(total, total, c1s, c2s, as, nb_off, nb, &fb, err, tally)
+            : decimate_round_passes<BLOCK>(total, total, c1g, c2g, alive, nb_off, nb, &fb, err, tally);
         if (tid == 0) {
             s_alive = left;
             s_fallback = fb;

@@ -576,12 +576,16 @@ __global__ void __launch_bounds__(AC_BLOCK) k_assign_cull(EngineView v)
     __shared__ float s_box[2][AC_WARPS][2 * DIM];    // warp boxes
     __shared__ float s_cbox[2][2 * DIM];             // the CTA's box
     __shared__ int s_wcnt[2][AC_WARPS];              // survivors per warp range
-    __shared__ int s_item[2];
     __shared__ int s_staged;                         // cloud whose whole chosen set is in sS
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
     const ActiveList al(v, ACT_CHUNK);
+    // Each cloud is cut into blocks of SUBPTS consecutive positions of its
+    // spatial order, `subs` blocks per assignment chunk (a power of two: both
+    // sizes are); blocks past the cloud's end are empty.  The block bounds
+    // need no division.
     const int subs = (v.chunk_pts + SUBPTS - 1) / SUBPTS;
+    const int subs_log = 31 - __clz(subs);
     const int total = al.total * subs;
 
     // A work item's cloud, point range and this lane's points with their
@@ -602,39 +606,36 @@ __global__ void __launch_bounds__(AC_BLOCK) k_assign_cull(EngineView v)
         }
         if (item >= total) return;
         int lc;
-        al.locate(item / subs, t.c, lc);
-        const CloudDesc cd = v.cl[t.c];
-        const int start = (int)(((int64_t)lc * cd.n_all) / cd.n_chunks);
-        const int end = (int)(((int64_t)(lc + 1) * cd.n_all) / cd.n_chunks);
-        t.b0 = start + (item % subs) * SUBPTS;
-        t.b1 = min(end, t.b0 + SUBPTS);
-        const float* Ps = v.Ps + cd.p_off * DP;
+        al.locate(item >> subs_log, t.c, lc);
+        const int n_all = v.cl[t.c].n_all;
+        const int64_t p_off = v.cl[t.c].p_off;
+        t.b0 = min(n_all, ((lc << subs_log) + (item & (subs - 1))) * SUBPTS);
+        t.b1 = min(n_all, t.b0 + SUBPTS);
+        const float* Ps = v.Ps + p_off * DP;
 #pragma unroll
         for (int j = 0; j < AC_ITEMS; ++j) {
             const int i = t.b0 + warp * WPTS + j * 32 + lane;
             if (i < t.b1) {
                 load_chosen<DIM>(Ps, i, t.p[j]);
-                t.slot[j] = v.sorder[cd.p_off + i];
+                t.slot[j] = v.sorder[p_off + i];
             }
         }
     };
 
-    if (tid == 0) {
-        s_item[0] = atomicAdd(&v.ctr[CTR_WORK], 1);
-        s_staged = -1;
-    }
-    __syncthreads();
+    if (tid == 0) s_staged = -1;
+    // Items are dealt to the CTAs round robin (they are of equal size), so
+    // every CTA knows its next item at once: its points are loaded while the
+    // current one is evaluated.  Shared arrays indexed by `buf` alternate
+    // between items, so a warp still reading the previous item's list never
+    // races the next item's writes; sS is rewritten only after the barrier
+    // that every warp reaches once it is done with the previous item.
     Item cur;
-    load_item(s_item[0], cur);
-    // Shared arrays indexed by `buf` alternate between work items, so a warp
-    // still reading the previous item's list never races the next item's
-    // writes; sS is rewritten only after the barrier that every warp reaches
-    // once it is done with the previous item.
-    for (int it = 0;; ++it) {
+    load_item(blockIdx.x, cur);
+    int it = 0;
+    for (int item = blockIdx.x; item < total; item += gridDim.x, ++it) {
         const int buf = it & 1;
-        const int item = s_item[buf];
-        if (item >= total) break;
-        if (tid == 0) s_item[buf ^ 1] = atomicAdd(&v.ctr[CTR_WORK], 1);
+        Item nxt;
+        load_item(item + gridDim.x, nxt);
         const int c = cur.c;
         const CloudDesc cd = v.cl[c];
         const int ns = v.ns[c];
@@ -686,10 +687,7 @@ __global__ void __launch_bounds__(AC_BLOCK) k_assign_cull(EngineView v)
             best[j] = FLT_MAX;
             bi[j] = -1;
         }
-        __syncthreads();  // warp boxes and the next item visible; the previous item is done
-        // the next item's points are in flight while this one is evaluated
-        Item nxt;
-        load_item(s_item[buf ^ 1], nxt);
+        __syncthreads();  // warp boxes visible; the previous item is done
         if (warp == 0 && lane < 2 * DIM) {
             const bool hi = lane >= DIM;
             float x = s_box[buf][0][lane];
@@ -1855,7 +1853,7 @@ __device__ void decimate_group(const EngineView& v, const int g)
                                     hmask, v.dnb_off + gd.s_scratch + g,
                                     v.dnb + (int64_t)v.dec_nb_pp * gd.s_scratch,
                                     (int64_t)v.dec_nb_pp * gd.s_cap, dec_smem, v.dec_smem_max,
-                                    &v.err[gd.cloud_begin], prepared);
+                                    &v.err[gd.cloud_begin], prepared, v.ctr + CTR_DEC_PASSES);
     // compaction back into each cloud, in order
     int running = 0, total_after = 0;
     for (int ci = 0; ci < gd.n_clouds; ++ci) {
@@ -2317,7 +2315,7 @@ cudaError_t set_assign_attrs(int dyn)
 
 // persistent grid of k_assign_cull: every resident CTA, at most one per item
 template <int DIM, int ITEMS>
-void launch_assign_cull(const EngineView& v, cudaStream_t st)
+cudaError_t launch_assign_cull(const EngineView& v, cudaStream_t st)
 {
     static std::atomic<int> per_sm{0};
     int b = per_sm.load(std::memory_order_relaxed);
@@ -2328,9 +2326,11 @@ void launch_assign_cull(const EngineView& v, cudaStream_t st)
         per_sm.store(b, std::memory_order_relaxed);
     }
     const int subs = (v.chunk_pts + AC_BLOCK * ITEMS - 1) / (AC_BLOCK * ITEMS);
+    if (subs & (subs - 1)) return cudaErrorInvalidValue;  // the kernel's block bounds need 2^k
     const int64_t items = (int64_t)v.n_chunks * subs;
     const int g = (int)std::max<int64_t>(1, std::min<int64_t>(items, (int64_t)v.n_sms * b));
     k_assign_cull<DIM, ITEMS><<<g, AC_BLOCK, 0, st>>>(v);
+    return cudaGetLastError();
 }
 
 template <int DIM>
@@ -2359,9 +2359,11 @@ cudaError_t launch_pass_dim(const EngineView& v, const TuneParams& tp, int assig
     const int sms = v.n_sms;
     if (a0) cudaEventRecord(a0, st);
     if (v.cull) {
-        if (tp.cull_items == 2) launch_assign_cull<DIM, 2>(v, st);
-        else if (tp.cull_items == 8) launch_assign_cull<DIM, 8>(v, st);
-        else launch_assign_cull<DIM, 4>(v, st);
+        cudaError_t e;
+        if (tp.cull_items == 2) e = launch_assign_cull<DIM, 2>(v, st);
+        else if (tp.cull_items == 8) e = launch_assign_cull<DIM, 8>(v, st);
+        else e = launch_assign_cull<DIM, 4>(v, st);
+        if (e != cudaSuccess) return e;
     } else {
 #define RD_ASSIGN_CASE(B, I)                                                                  \
     if (tp.block == B && tp.items == I) {                                                     \

@@ -40,7 +40,7 @@ namespace {
 namespace cg = cooperative_groups;
 
 constexpr int TCL = 8;                  // CTAs per cluster (portable size)
-constexpr int TCL_MIN_POINTS = 24576;   // default: evolve points of a tile evolved by a cluster
+constexpr int TCL_MIN_POINTS = 100000;  // default: evolve points of a tile evolved by a cluster
 constexpr int TSEG_MIN = 8192;          // default: members of a key folded across the cluster
 constexpr int TSEG_KEYS = 4;            // such keys per pass (the first in key order)
 constexpr int TCL_W = 8;                // warps per CTA of the cluster kernel (256 threads)

@@ -51,7 +51,7 @@ def test_argument_errors_need_no_gpu():
     assert lib.rd_bf_create(ctypes.byref(h), 2, 0, 0, -5, 0.3, 0.6) == L.RD_ERR_ARG
     assert lib.rd_bf_run(None, None) == L.RD_ERR_ARG
     assert lib.rd_batch_run(None, None, 0, None, 0, 0, None) == L.RD_ERR_ARG
-    assert lib.rd_abi_version() == 2
+    assert lib.rd_abi_version() == 3
     assert lib.rd_supported_dims() & (1 << 2) and lib.rd_supported_dims() & (1 << 3)
 
 

@@ -70,4 +70,4 @@ def test_cluster_switch_changes_nothing(rdb):
         rdb.set_tile_clusters(True, 0, 0)
     S_on, st, _ = rdb.tiled_ridge_detection(P, *args)
     assert st.err_bits == 0 and bits_equal(S_on, S_off)
-    assert rdb.get_tile_clusters() == (True, 24576, 8192)
+    assert rdb.get_tile_clusters() == (True, 100000, 8192)

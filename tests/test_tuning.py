@@ -71,10 +71,10 @@ def test_assign_cull_switch_roundtrip():
 
 
 def test_tile_cluster_switch_roundtrip():
-    assert rdb.get_tile_clusters() == (True, 24576, 8192)
+    assert rdb.get_tile_clusters() == (True, 100000, 8192)
     try:
         rdb.set_tile_clusters(False, 1000, 64)
         assert rdb.get_tile_clusters() == (False, 1000, 64)
     finally:
         rdb.set_tile_clusters(True, 0, 0)
-    assert rdb.get_tile_clusters() == (True, 24576, 8192)
+    assert rdb.get_tile_clusters() == (True, 100000, 8192)
