@@ -253,7 +253,11 @@ __global__ void __launch_bounds__(256) k_choose_filter(EngineView v, int c, int 
 }
 
 // sel: the survivors of [a, b) in order, *nsel of them (nullptr in the first
-// round, where every point of the range is a candidate)
+// round, where every point of the range is a candidate).  The candidates are
+// taken in blocks of BLOCK as k_choose takes its points: all threads load
+// their candidates, compute their cells and drop those within r1 of a point
+// chosen so far (earlier rounds and earlier blocks of this one); warp 0 then
+// walks the block's survivors in order, from shared memory.
 template <int DIM, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_choose_resolve(EngineView v, int c, int a, int b,
                                                           const int32_t* __restrict__ sel,
@@ -263,10 +267,11 @@ __global__ void __launch_bounds__(BLOCK) k_choose_resolve(EngineView v, int c, i
     using CS = ChooseSmem<DIM>;
     constexpr int NB = Pow3<DIM>::v;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    int32_t* s_heads = reinterpret_cast<int32_t*>(smem_raw);  // HB
-    int32_t* s_next = s_heads + CS::HB;                        // SCAP
-    float* s_S = reinterpret_cast<float*>(s_next + CS::SCAP);  // SCAP*DIM
-    int32_t* s_list = reinterpret_cast<int32_t*>(s_S + CS::SCAP * DIM);  // BLOCK
+    int32_t* s_heads = reinterpret_cast<int32_t*>(smem_raw);          // HB
+    int32_t* s_next = s_heads + CS::HB;                                // SCAP
+    float* s_S = reinterpret_cast<float*>(s_next + CS::SCAP);          // SCAP*DIM
+    float* s_sp = s_S + CS::SCAP * DIM;                                // BLOCK*DIM
+    int32_t* s_scell = reinterpret_cast<int32_t*>(s_sp + BLOCK * DIM); // BLOCK*DIM
     __shared__ int s_ns;
     __shared__ int s_wsum[BLOCK / 32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -290,13 +295,39 @@ __global__ void __launch_bounds__(BLOCK) k_choose_resolve(EngineView v, int c, i
         return (q < CS::SCAP) ? s_S[q * DIM + d] : gS[(int64_t)q * DIM + d];
     };
     auto nxt = [&](int q) -> int { return (q < CS::SCAP) ? s_next[q] : gnext[q]; };
+    // any chosen point within r1 of p, over the given neighbour cells
+    auto query = [&](const float* p, const int* cc, int o) -> bool {
+        int nc[DIM];
+        neighbour_cell<DIM>(cc, o, nc);
+        int q = s_heads[cell_hash<DIM>(nc) & hmask];
+        while (q >= 0) {
+            float s[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) s[d] = coord(q, d);
+            if (sqdist_exact<DIM>(p, s) <= rsq) return true;
+            q = nxt(q);
+        }
+        return false;
+    };
     const int cnt = sel ? *nsel : (b - a);
     for (int base = 0; base < cnt; base += BLOCK) {
         const int j = base + tid;
-        const bool f = j < cnt;
-        const int i = f ? (sel ? sel[j] : a + j) : -1;
-        if (!__syncthreads_or(f)) continue;
-        const unsigned bal = __ballot_sync(FULL, f);
+        float p[DIM];
+        int cc[DIM];
+        bool surv = false;
+        if (j < cnt) {
+            const int i = sel ? sel[j] : a + j;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                p[d] = P[(int64_t)i * DIM + d];
+                cc[d] = cell_of(p[d], inv);
+            }
+            bool hit = false;
+            for (int t = 0; t < NB && !hit; ++t) hit = query(p, cc, (t + NB / 2) % NB);
+            surv = !hit;
+        }
+        // compact the block's survivors in visiting order
+        const unsigned bal = __ballot_sync(FULL, surv);
         if (lane == 0) s_wsum[warp] = __popc(bal);
         __syncthreads();
         int wbase = 0, tot = 0;
@@ -305,30 +336,27 @@ __global__ void __launch_bounds__(BLOCK) k_choose_resolve(EngineView v, int c, i
             wbase += (w < warp) ? x : 0;
             tot += x;
         }
-        if (f) s_list[wbase + __popc(bal & lanemask_lt())] = i;
+        if (surv) {
+            const int pos = wbase + __popc(bal & lanemask_lt());
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                s_sp[pos * DIM + d] = p[d];
+                s_scell[pos * DIM + d] = cc[d];
+            }
+        }
         __syncthreads();
         if (warp == 0) {
             int ns = s_ns;
             for (int sidx = 0; sidx < tot; ++sidx) {
-                const int pi = s_list[sidx];
                 float ps[DIM];
                 int cs[DIM];
 #pragma unroll
                 for (int d = 0; d < DIM; ++d) {
-                    ps[d] = P[(int64_t)pi * DIM + d];
-                    cs[d] = cell_of(ps[d], inv);
+                    ps[d] = s_sp[sidx * DIM + d];
+                    cs[d] = s_scell[sidx * DIM + d];
                 }
                 bool hit = false;
-                for (int o = lane; o < NB && !hit; o += 32) {
-                    int nc[DIM];
-                    neighbour_cell<DIM>(cs, o, nc);
-                    for (int q = s_heads[cell_hash<DIM>(nc) & hmask]; q >= 0 && !hit; q = nxt(q)) {
-                        float s[DIM];
-#pragma unroll
-                        for (int d = 0; d < DIM; ++d) s[d] = coord(q, d);
-                        hit = sqdist_exact<DIM>(ps, s) <= rsq;
-                    }
-                }
+                for (int o = lane; o < NB; o += 32) hit = hit || query(ps, cs, o);
                 hit = __any_sync(FULL, hit);
                 if (!hit) {
                     if (lane == 0) {
@@ -1022,6 +1050,9 @@ __device__ __forceinline__ void store_row(float* rows, int64_t r, const float (&
 // each in index order.  Ranges are in index order too, so the placement stays
 // stable while the dependent placement chain is SCAT_W times shorter.  Larger
 // chosen sets use scatter_chunk (one warp) in warp 0.
+// groups of more clouds than this are gathered and compacted one thread per
+// cloud (decimate_group)
+constexpr int DEC_CLOUDS_SERIAL = 32;
 constexpr int SCAT_W = 8;
 constexpr int SCAT_HMAX = 1024;
 constexpr int SCAT_KS = 8;   // chunk keys per thread loaded together (covers 2,048-point chunks)
@@ -1501,55 +1532,66 @@ __device__ __forceinline__ void tile_assign_range(const float* __restrict__ P, c
 #pragma unroll
             for (int d = 0; d < DIM; ++d) p[h][d] = (i < r1w) ? P[(int64_t)i * DIM + d] : 0.0f;
         }
+        if (ns <= KB) {
+            // first index of the minimum, directly: each chosen point is read
+            // once for the step's TILE_PPL points
+            float best[TILE_PPL];
+            int bk[TILE_PPL];
+#pragma unroll
+            for (int h = 0; h < TILE_PPL; ++h) {
+                best[h] = FLT_MAX;
+                bk[h] = -1;
+            }
+            for (int k = 0; k < ns; ++k) {
+                float s[DIM];
+                load_chosen<DIM>(sS, k, s);
+#pragma unroll
+                for (int h = 0; h < TILE_PPL; ++h) {
+                    const float dd = sqdist_exact<DIM>(s, p[h]);
+                    if (dd < best[h]) { best[h] = dd; bk[h] = k; }
+                }
+            }
+#pragma unroll
+            for (int h = 0; h < TILE_PPL; ++h) {
+                const int i = i0 + h * 32 + lane;
+                const int key = (i < r1w && best[h] <= rsq) ? bk[h] : -1;
+                if (i < r1w) keys[i] = key;
+#pragma unroll
+                for (int k = 0; k < KB; ++k)
+                    if (k < ns) kc[k] += __popc(__ballot_sync(FULL, key == k));
+            }
+            continue;
+        }
 #pragma unroll
         for (int h = 0; h < TILE_PPL; ++h) {
             const int i = i0 + h * 32 + lane;
             int key = -1;
             if (i < r1w) {
-                if (ns <= KB) {
-                    // first index of the minimum, directly
-                    float best = FLT_MAX;
-                    int bk = -1;
-                    for (int k = 0; k < ns; ++k) {
-                        float s[DIM];
-                        load_chosen<DIM>(sS, k, s);
-                        const float dd = sqdist_exact<DIM>(s, p[h]);
-                        if (dd < best) { best = dd; bk = k; }
-                    }
-                    key = (best <= rsq) ? bk : -1;
-                } else {
-                    float best = FLT_MAX;
-                    int blk = -1;
-                    for (int kb = 0; kb < nsp; kb += KB) {
-                        const float old = best;
+                float best = FLT_MAX;
+                int blk = -1;
+                for (int kb = 0; kb < nsp; kb += KB) {
+                    const float old = best;
 #pragma unroll
-                        for (int u = 0; u < KB; ++u) {
-                            float s[DIM];
-                            load_chosen<DIM>(sS, kb + u, s);
-                            best = fminf(best, sqdist_exact<DIM>(s, p[h]));
-                        }
-                        blk = (best < old) ? kb : blk;
+                    for (int u = 0; u < KB; ++u) {
+                        float s[DIM];
+                        load_chosen<DIM>(sS, kb + u, s);
+                        best = fminf(best, sqdist_exact<DIM>(s, p[h]));
                     }
-                    if (best <= rsq && blk >= 0) {
-                        for (int u = 0; u < KB && blk + u < ns; ++u) {
-                            float s[DIM];
-                            load_chosen<DIM>(sS, blk + u, s);
-                            if (sqdist_exact<DIM>(s, p[h]) == best) { key = blk + u; break; }
-                        }
+                    blk = (best < old) ? kb : blk;
+                }
+                if (best <= rsq && blk >= 0) {
+                    for (int u = 0; u < KB && blk + u < ns; ++u) {
+                        float s[DIM];
+                        load_chosen<DIM>(sS, blk + u, s);
+                        if (sqdist_exact<DIM>(s, p[h]) == best) { key = blk + u; break; }
                     }
                 }
                 keys[i] = key;
             }
-            if (ns <= KB) {
-#pragma unroll
-                for (int k = 0; k < KB; ++k)
-                    if (k < ns) kc[k] += __popc(__ballot_sync(FULL, key == k));
-            } else {
-                // a tile's warp step holds few distinct keys: the match
-                // instruction is cheap there (warp_runs suits many keys)
-                const unsigned mm = __match_any_sync(FULL, key);
-                if (key >= 0 && lane == __ffs(mm) - 1) atomicAdd(&whist[key], __popc(mm));
-            }
+            // a tile's warp step holds few distinct keys: the match
+            // instruction is cheap there (warp_runs suits many keys)
+            const unsigned mm = __match_any_sync(FULL, key);
+            if (key >= 0 && lane == __ffs(mm) - 1) atomicAdd(&whist[key], __popc(mm));
         }
     }
     if (ns <= KB && lane == 0)
@@ -1836,17 +1878,62 @@ __device__ void decimate_group(const EngineView& v, const int g)
     const uint32_t hmask = (1u << hbits) - 1;
     int32_t* bstart = v.dbstart + v.dec_hoff[g];
 
+    // Groups of many clouds (tiled runs) are walked one thread per cloud: the
+    // clouds' offsets in the group's list come from a block-wide scan of their
+    // chosen counts, or from the GPU-wide preparation (dcpre) when it ran.
+    const int prepared = (v.dbig[0] == 1 && v.dbig[1] == g) ? 1 : 0;
+    const bool per_thread = gd.n_clouds > DEC_CLOUDS_SERIAL;
+    // f(ci, c, ns, off) for every cloud of the group, one thread each; returns
+    // the group's total (the same in every thread)
+    auto for_clouds = [&](auto&& f) -> int {
+        __shared__ int s_w[BLOCK / 32];
+        __shared__ int s_carry;
+        if (tid == 0) s_carry = 0;
+        __syncthreads();
+        for (int c0 = 0; c0 < gd.n_clouds; c0 += BLOCK) {
+            const int ci = c0 + tid;
+            const int c = gd.cloud_begin + ci;
+            const int x = (ci < gd.n_clouds) ? v.ns[c] : 0;
+            int incl = x;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += y;
+            }
+            if (lane == 31) s_w[warp] = incl;
+            __syncthreads();
+            int pre = 0, tot = 0;
+            for (int w = 0; w < BLOCK / 32; ++w) {
+                pre += (w < warp) ? s_w[w] : 0;
+                tot += s_w[w];
+            }
+            const int carry = s_carry;
+            if (ci < gd.n_clouds) f(ci, c, x, prepared ? v.dcpre[ci] : carry + pre + incl - x);
+            __syncthreads();
+            if (tid == 0) s_carry = carry + tot;
+            __syncthreads();
+        }
+        return s_carry;
+    };
     // gather the group's chosen points (cloud order) into X, unless the
     // GPU-wide preparation kernels already did (large group)
-    const int prepared = (v.dbig[0] == 1 && v.dbig[1] == g) ? 1 : 0;
     int total = 0;
-    for (int i = 0; i < gd.n_clouds; ++i) {
-        const int c = gd.cloud_begin + i;
-        const CloudDesc cd = v.cl[c];
-        const int ns = v.ns[c];
-        if (!prepared)
+    if (prepared) {
+        total = v.dbig[2];
+    } else if (per_thread) {
+        total = for_clouds([&](int, int c, int ns, int off) {
+            const int64_t so = v.cl[c].s_off;
+            for (int e = 0; e < ns * DIM; ++e) X[(int64_t)off * DIM + e] = v.S[so * DIM + e];
+        });
+        __syncthreads();
+    } else {
+        for (int i = 0; i < gd.n_clouds; ++i) {
+            const int c = gd.cloud_begin + i;
+            const CloudDesc cd = v.cl[c];
+            const int ns = v.ns[c];
             for (int e = tid; e < ns * DIM; e += BLOCK) X[(int64_t)total * DIM + e] = v.S[cd.s_off * DIM + e];
-        total += ns;
+            total += ns;
+        }
     }
     extern __shared__ __align__(16) unsigned char dec_smem[];
     decimate_scan_lists<DIM, BLOCK>(X, total, c0.r2, gd.nocopy, cell, alive, c1, c2, items, bstart,
@@ -1856,7 +1943,28 @@ __device__ void decimate_group(const EngineView& v, const int g)
                                     &v.err[gd.cloud_begin], prepared, v.ctr + CTR_DEC_PASSES);
     // compaction back into each cloud, in order
     int running = 0, total_after = 0;
-    for (int ci = 0; ci < gd.n_clouds; ++ci) {
+    if (per_thread) {
+        __shared__ int s_after;
+        if (tid == 0) s_after = 0;
+        __syncthreads();
+        int mine = 0;
+        for_clouds([&](int, int c, int ns, int off) {
+            const int64_t so = v.cl[c].s_off;
+            int kept = 0;
+            for (int k = 0; k < ns; ++k) {
+                if (!alive[off + k]) continue;
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) v.S[(so + kept) * DIM + d] = X[(int64_t)(off + k) * DIM + d];
+                ++kept;
+            }
+            v.ns[c] = kept;
+            mine += kept;
+        });
+        if (mine) atomicAdd(&s_after, mine);
+        __syncthreads();
+        total_after = s_after;
+    }
+    for (int ci = 0; !per_thread && ci < gd.n_clouds; ++ci) {
         const int c = gd.cloud_begin + ci;
         const CloudDesc cd = v.cl[c];
         const int ns = v.ns[c];
@@ -2418,7 +2526,7 @@ cudaError_t launch_choose_rounds_dim(const EngineView& v, int c, int n, uint8_t*
 {
     using CS = ChooseSmem<DIM>;
     constexpr int B = 1024;
-    const int bytes = CS::HB * 4 + CS::SCAP * 4 + CS::SCAP * DIM * 4 + B * 4;
+    const int bytes = CS::HB * 4 + CS::SCAP * 4 + CS::SCAP * DIM * 4 + B * DIM * 8;
     cudaError_t e = cudaFuncSetAttribute(k_choose_resolve<DIM, B>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return e;
