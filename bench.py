@@ -291,11 +291,16 @@ def run_b200_bf(args, world, rank, local):
     stream = torch.cuda.current_stream()
     dP = torch.from_numpy(P).to(dev)
     l2_flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    # launch shape of the assignment kernel from the project's autotuner, on a
-    # synthetic cloud of this size with the chosen count of the first choose
-    # (setup, outside every timed region)
-    tb, ti, tci, tus = rdb.autotune(dim, n, max(1, rdb.choose_count(dP, r1)), reps=6, points=dP,
-                                    r1=r1)
+    # launch shape of the assignment from the project's autotuner: whole solves
+    # of this cloud, every supported shape (setup, outside every timed region);
+    # --shape fixes it instead
+    if args.shape:
+        tb, ti, tci = [int(x) for x in args.shape.split(",")] + ([4] if args.shape.count(",") == 1 else [])
+        rdb.tune_set(dim, n, tb, ti, tci, r1=r1)
+        tune_src, tune_ms = "--shape", None
+    else:
+        tb, ti, tci, tune_ms = rdb.autotune_solve(dim, dP, r1, r2, runs=3)
+        tune_src = "rd_autotune_solve (whole solves timed, median of 3 runs per shape)"
     rd = rdb.BruteForceRidgeDetection(n, r1, r2, dim)
     rd.set_points(dP)
 
@@ -444,8 +449,7 @@ def run_b200_bf(args, world, rank, local):
                    "loop": "CUDA graph WHILE node", "parallelism": f"replicas x{world}",
                    "assign": "culled (exact chunk-box culling)" if culled else "all pairs",
                    "assign_shape": {"block": tb, "items": ti, "cull_items": tci,
-                                    "source": "rd_autotune (whole evolve passes timed, median of 5 runs per shape)",
-                                    "tuned_us_per_pass": tus}},
+                                    "source": tune_src, "tuned_ms_per_solve": tune_ms}},
         "solves_per_s": world * 1e3 / ms_max,
         "pairs_per_step": pairs_step, "loop_iters_per_step": iters_step,
         "ns_final": ns_final,

@@ -130,6 +130,17 @@ RD_API rd_status rd_get_tile_clusters(int* enable, int64_t* min_points, int64_t*
 RD_API rd_status rd_autotune(int dim, const float* d_P, int64_t n, int64_t ns, float r1, int reps,
                              int* block, int* items, int* cull_items, double* us_per_pass,
                              void* stream);
+/* The same choice from whole solves: every supported shape solves the cloud
+ * d_P (device, n x dim ROW_MAJOR) with radii r1 and r2 from choose to
+ * convergence in the CUDA-graph loop, timed with CUDA events, `runs` times
+ * (interleaved over the shapes) after one untimed solve each.  The same
+ * decision rule as rd_autotune; stores the pick for the (dim, n, r1) bucket
+ * and returns it with its median time per solve in milliseconds.  Holds one
+ * engine per shape while it runs.  Runs on `stream` and waits for it; d_P is
+ * not modified. */
+RD_API rd_status rd_autotune_solve(int dim, const float* d_P, int64_t n, float r1, float r2, int runs,
+                                   int* block, int* items, int* cull_items, double* ms_per_solve,
+                                   void* stream);
 
 /* Orders a ridge into chains: rd::orderSamples (rd/cpu/brute_force/order.hpp:45)
  * with the condition of the brute-force class's order_ option

@@ -9,13 +9,13 @@ from ._lib import RDError, RunStats, lib  # noqa: F401
 from .api import (COL_MAJOR, LOOP_GRAPH, LOOP_HOST, ROW_MAJOR, TILED_LOCAL,  # noqa: F401
                   TILED_MIXED,
                   BatchedRidgeDetection, BruteForceRidgeDetection, TiledRidgeDetection,
-                  autotune, choose_count, load_binary_cloud, load_text_cloud, order_chains,
+                  autotune, autotune_solve, choose_count, load_binary_cloud, load_text_cloud, order_chains,
                   pack_clouds, save_binary_cloud, hausdorff, distance_stats, segment_hausdorff, ridge_detection,
                   tiled_ridge_detection, tune_get, tune_reset, tune_set, set_assign_cull,
                   get_assign_cull, set_tile_clusters, get_tile_clusters)
 
 __all__ = ["BruteForceRidgeDetection", "BatchedRidgeDetection", "TiledRidgeDetection",
            "ridge_detection", "tiled_ridge_detection",
-           "pack_clouds", "order_chains", "hausdorff", "distance_stats", "segment_hausdorff", "load_text_cloud", "load_binary_cloud", "save_binary_cloud", "autotune", "choose_count", "tune_get", "tune_set", "tune_reset", "set_assign_cull", "get_assign_cull", "set_tile_clusters", "get_tile_clusters",
+           "pack_clouds", "order_chains", "hausdorff", "distance_stats", "segment_hausdorff", "load_text_cloud", "load_binary_cloud", "save_binary_cloud", "autotune", "autotune_solve", "choose_count", "tune_get", "tune_set", "tune_reset", "set_assign_cull", "get_assign_cull", "set_tile_clusters", "get_tile_clusters",
            "ROW_MAJOR", "TILED_MIXED", "TILED_LOCAL", "COL_MAJOR", "LOOP_GRAPH", "LOOP_HOST", "RDError",
            "RunStats", "lib", "generators"]

@@ -83,6 +83,8 @@ SIGNATURES = {
     "rd_load_text_cloud": [ctypes.c_char_p, _vp, _i64, _i],
     "rd_load_binary_cloud": [ctypes.c_char_p, _i64, _i, _vp],
     "rd_save_binary_cloud": [ctypes.c_char_p, _vp, _i64, _i],
+    "rd_autotune_solve": [ctypes.c_int, _vp, ctypes.c_int64, ctypes.c_float, ctypes.c_float, ctypes.c_int,
+                          _vp, _vp, _vp, _vp, _vp],
     "rd_ordered_sum": [ctypes.c_int, _vp, _vp, ctypes.c_int64, _vp, ctypes.c_int, _vp],
     "rd_bf_create": [ctypes.POINTER(_vp), _i, _i, _i, _i64, _f, _f],
     "rd_bf_set_points": [_vp, _vp, _i64, _i, _vp],

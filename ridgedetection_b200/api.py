@@ -399,6 +399,23 @@ def autotune(dim: int, n: int, ns: int, reps: int = 5, points=None,
     return b.value, i.value, c.value, us.value
 
 
+def autotune_solve(dim: int, points, r1: float, r2: float,
+                   runs: int = 3) -> Tuple[int, int, int, float]:
+    """Time whole brute-force solves (choose to convergence, graph loop) of
+    ``points`` (a float32 CUDA tensor, n x dim) with every supported shape of
+    the assignment and keep the best for the (dim, size, r1) bucket, with the
+    same decision rule as :func:`autotune`; returns (block, items,
+    cull_items, milliseconds per solve)."""
+    if not _is_torch_cuda(points):
+        raise TypeError("points must be a CUDA tensor")
+    b, i, c, ms = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0), ctypes.c_double(0)
+    pts = points.contiguous()
+    L.check(L.lib().rd_autotune_solve(dim, ctypes.c_void_p(pts.data_ptr()), int(pts.shape[0]),
+                                      float(r1), float(r2), int(runs), ctypes.byref(b),
+                                      ctypes.byref(i), ctypes.byref(c), ctypes.byref(ms), None))
+    return b.value, i.value, c.value, ms.value
+
+
 def order_chains(S, r2: float):
     """Order a ridge into chains (rd::orderSamples, rd/cpu/brute_force/order.hpp:45,
     with the brute-force class's condition: squared distance <= r2*r2).

@@ -328,6 +328,45 @@ rd_status rd_get_assign_cull(int* enable)
     return RD_OK;
 }
 
+}  // extern "C"
+namespace {
+// The pick from per-candidate timings (NREP runs each): the lowest median;
+// shapes within 2% of it count as tied and the first of them in the fixed
+// candidate order is taken, so that runs that see the same timings up to
+// noise pick the same shape; an incumbent in the table for this bucket is
+// kept unless the pick beats it by more than 3%.
+size_t tune_pick(int dim, int64_t n, float r1, const std::vector<TuneParams>& cand,
+                 const std::vector<std::vector<float>>& ms, float* med_out)
+{
+    auto median = [](std::vector<float> v) {
+        std::sort(v.begin(), v.end());
+        return v[v.size() / 2];
+    };
+    size_t bi = 0;
+    std::vector<float> med(cand.size());
+    for (size_t ci = 0; ci < cand.size(); ++ci) {
+        med[ci] = median(ms[ci]);
+        if (med[ci] < med[bi]) bi = ci;
+    }
+    const float best = med[bi];
+    for (size_t ci = 0; ci < cand.size(); ++ci)
+        if (med[ci] <= 1.02f * best) {
+            bi = ci;
+            break;
+        }
+    TuneParams inc;
+    if (tune_find_exact(dim, n, r1, &inc)) {
+        for (size_t ci = 0; ci < cand.size(); ++ci)
+            if (cand[ci].block == inc.block && cand[ci].items == inc.items &&
+                cand[ci].cull_items == inc.cull_items && med[bi] > 0.97f * med[ci])
+                bi = ci;
+    }
+    *med_out = med[bi];
+    return bi;
+}
+}  // namespace
+extern "C" {
+
 rd_status rd_autotune(int dim, const float* d_P, int64_t n, int64_t ns, float r1, int reps,
                       int* block, int* items, int* cull_items, double* us_per_pass, void* stream)
 {
@@ -377,39 +416,69 @@ rd_status rd_autotune(int dim, const float* d_P, int64_t n, int64_t ns, float r1
                                                     : 0.0f);
         }
     }
-    auto median = [](std::vector<float> v) {
-        std::sort(v.begin(), v.end());
-        return v[v.size() / 2];
-    };
-    size_t bi = 0;
-    std::vector<float> med(cand.size());
-    for (size_t ci = 0; ci < cand.size(); ++ci) {
-        med[ci] = median(ms[ci]);
-        if (med[ci] < med[bi]) bi = ci;
-    }
-    // shapes within 2% of the fastest count as tied: the first of them in the
-    // fixed candidate order is taken, so that runs that see the same timings
-    // up to noise pick the same shape
-    const float best = med[bi];
-    for (size_t ci = 0; ci < cand.size(); ++ci)
-        if (med[ci] <= 1.02f * best) {
-            bi = ci;
-            break;
-        }
-    // keep the shape already in the table unless the new one is 3% faster
-    TuneParams inc;
-    if (tune_find_exact(dim, n, r1, &inc)) {
-        for (size_t ci = 0; ci < cand.size(); ++ci)
-            if (cand[ci].block == inc.block && cand[ci].items == inc.items &&
-                cand[ci].cull_items == inc.cull_items && med[bi] > 0.97f * med[ci])
-                bi = ci;
-    }
+    float med_best = 0.0f;
+    const size_t bi = tune_pick(dim, n, r1, cand, ms, &med_best);
     const TuneParams bt = cand[bi];
     tune_store(dim, n, r1, bt);
     *block = bt.block;
     *items = bt.items;
     *cull_items = bt.cull_items;
-    if (us_per_pass) *us_per_pass = 1e3 * med[bi];
+    if (us_per_pass) *us_per_pass = 1e3 * med_best;
+    return RD_OK;
+}
+
+
+rd_status rd_autotune_solve(int dim, const float* d_P, int64_t n, float r1, float r2, int runs,
+                            int* block, int* items, int* cull_items, double* ms_per_solve,
+                            void* stream)
+{
+    if (!dim_ok(dim)) return set_err(RD_ERR_UNSUPPORTED, "dim must be 1 to 4");
+    if (!d_P || !block || !items || !cull_items) return set_err(RD_ERR_ARG, "null argument");
+    if (n < 1 || n > INT32_MAX - 1024 || runs < 1 || runs > 100 || !(r1 > 0.0f) || !(r2 > 0.0f))
+        return set_err(RD_ERR_ARG, "need 1 <= n, 1 <= runs <= 100 and positive radii");
+    cudaStream_t st = (cudaStream_t)stream;
+    const std::vector<TuneParams>& cand = tune_candidates(assign_cull_enabled());
+    // Every candidate solves the cloud from choose to convergence in the
+    // CUDA-graph loop, timed whole with CUDA events; `runs` runs per shape,
+    // interleaved over the shapes; the same decision rule as rd_autotune.
+    std::vector<std::vector<float>> ms(cand.size());
+    cudaEvent_t e0, e1;
+    CK_CUDA(cudaEventCreate(&e0));
+    CK_CUDA(cudaEventCreate(&e1));
+    std::vector<std::unique_ptr<Engine>> eng(cand.size());
+    for (size_t ci = 0; ci < cand.size(); ++ci) {
+        eng[ci].reset(new Engine());
+        Engine& e = *eng[ci];
+        e.tune = cand[ci];
+        e.tune_locked = true;
+        if (rd_status s = one_cloud_engine(e, dim, n, n, r1, r2)) return s;
+        CK_CUDA(cudaMemcpyAsync(e.points(), d_P, sizeof(float) * n * dim, cudaMemcpyDeviceToDevice, st));
+        const int rc = e.run(st, true);   // untimed: graph build and first touch
+        if (rc && rc != RD_ERR_NOT_CONVERGED) return from_engine(rc, e);
+    }
+    for (int rep = 0; rep < runs; ++rep) {
+        for (size_t ci = 0; ci < cand.size(); ++ci) {
+            Engine& e = *eng[ci];
+            CK_CUDA(cudaEventRecord(e0, st));
+            const int rc = e.run(st, true);
+            CK_CUDA(cudaEventRecord(e1, st));
+            if (rc && rc != RD_ERR_NOT_CONVERGED) return from_engine(rc, e);
+            CK_CUDA(cudaEventSynchronize(e1));
+            float t = 0;
+            CK_CUDA(cudaEventElapsedTime(&t, e0, e1));
+            ms[ci].push_back(t);
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    float med_best = 0.0f;
+    const size_t bi = tune_pick(dim, n, r1, cand, ms, &med_best);
+    const TuneParams bt = cand[bi];
+    tune_store(dim, n, r1, bt);
+    *block = bt.block;
+    *items = bt.items;
+    *cull_items = bt.cull_items;
+    if (ms_per_solve) *ms_per_solve = med_best;
     return RD_OK;
 }
 

@@ -28,7 +28,7 @@ namespace {
 // chain -- while the pass has at most two such keys per big-key CTA; with more
 // (a batch of large clouds) every key is folded by a warp, which keeps all
 // SMs busy.
-constexpr int SUM_BIG_MIN = 2048;
+constexpr int SUM_BIG_MIN = 16384;
 constexpr int SUM_BIG_PER_CTA = 2;
 
 // Work lists over the clouds still evolving, rebuilt by k_loopcond after every
@@ -1266,6 +1266,10 @@ constexpr int TILE_PPL = 8;
 // (warp-segmented exact evaluation, rd_segfold.cuh) instead of one warp's add
 // chain
 constexpr int FOLD_CTA_MIN = 4096;
+// the same for the light tiles of the cluster kernel: the heavy tiles, whose
+// keys need the CTA-wide folds, went to clusters; the others fold faster with
+// every warp on its own keys
+constexpr int FOLD_CTA_MIN_LIGHT = 1 << 30;
 
 template <int DIM>
 __device__ void sum_shift_one(const EngineView& v, int c, int k, float* buf, int lane, bool cta_big);
@@ -1662,7 +1666,8 @@ struct TileCtaSmem {
 // One CTA evolves tile c to convergence (see above); dyn is the dynamic
 // shared memory laid out as tile_evolve_smem_bytes describes.
 template <int DIM, int BLOCK>
-__device__ void tile_evolve_one(const EngineView& v, const int c, unsigned char* dyn,
+__device__ void tile_evolve_one(const EngineView& v, const int c, const int fold_cta_min,
+                                unsigned char* dyn,
                                 TileCtaSmem<DIM, BLOCK>& ts)
 {
     constexpr int W = BLOCK / 32;
@@ -1741,7 +1746,7 @@ __device__ void tile_evolve_one(const EngineView& v, const int c, unsigned char*
             // 4a. very large keys, one at a time, folded by the whole CTA
             for (int k = 0; k < ns; ++k) {
                 const int cnt = kbase[k + 1] - kbase[k];
-                if (cnt < FOLD_CTA_MIN) continue;
+                if (cnt < fold_cta_min) continue;
                 fold_members_seg_src<W, DIM>(RowSrc<DIM>{Pg + (int64_t)kbase[k] * DP}, cnt, s_seg);
                 if (tid < DIM) {
                     float cval = sS[k * DP + tid];
@@ -1755,7 +1760,7 @@ __device__ void tile_evolve_one(const EngineView& v, const int c, unsigned char*
             // 4b. index-order fold and movement test, warp w takes keys w, w+W, ...
             for (int k = warp; k < ns; k += W) {
                 const int cnt = kbase[k + 1] - kbase[k];
-                if (cnt == 0 || cnt >= FOLD_CTA_MIN) continue;
+                if (cnt == 0 || cnt >= fold_cta_min) continue;
                 const float sum = fold_rows<DIM, SUM_BP>(Pg + (int64_t)kbase[k] * DP, cnt, s_buf[warp], lane);
                 int moved = 0;
                 if (lane < DIM) {
@@ -1798,7 +1803,8 @@ __global__ void __launch_bounds__(BLOCK) k_tile_evolve(EngineView v)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ TileCtaSmem<DIM, BLOCK> ts;
     const int nact = v.ctr[CTR_NACT];
-    for (int a = blockIdx.x; a < nact; a += gridDim.x) tile_evolve_one<DIM, BLOCK>(v, v.act_cloud[a], smem_raw, ts);
+    for (int a = blockIdx.x; a < nact; a += gridDim.x)
+        tile_evolve_one<DIM, BLOCK>(v, v.act_cloud[a], FOLD_CTA_MIN, smem_raw, ts);
 }
 
 __host__ __device__ constexpr int tile_evolve_smem_bytes(int dim)

@@ -366,7 +366,7 @@ __global__ void __launch_bounds__(BLOCK) k_tile_evolve_cl(EngineView v)
         const int c = s_t;
         __syncthreads();
         if (c < 0) break;
-        if (v.phase[c] == PH_EVOLVE) tile_evolve_one<DIM, BLOCK>(v, c, smem_raw, ts);
+        if (v.phase[c] == PH_EVOLVE) tile_evolve_one<DIM, BLOCK>(v, c, FOLD_CTA_MIN_LIGHT, smem_raw, ts);
     }
 }
 

@@ -108,3 +108,19 @@ def test_bf_full_size_helix_properties(rdb):
     S_after, _, _, _, cont = O.evolve_pass(P, S1, r1)
     assert cont == 0 and bits_equal(S_after, S1)
     assert decimation_is_stable(S1, r2)
+
+
+@pytest.mark.parametrize("centre", [0.0, -0.5])
+def test_bf_big_clusters_cta_fold(rdb, centre):
+    """Clusters of more than 16,384 members (folded by whole CTAs with the
+    warp-segmented exact fold in k_sum_shift), including coordinate sums that
+    wander around zero (centre -0.5: the cube straddles the origin)."""
+    P = (np.random.default_rng(77).uniform(0, 1, (300_000, 3)) + centre).astype(np.float32)
+    r1, r2 = 0.6, 1.2
+    S0 = O.choose(P, np.float32(r1))
+    _, _, cnt, _, _ = O.evolve_pass(P, S0, np.float32(r1))
+    assert cnt.max() >= 16384  # the CTA path is exercised
+    S_ref, _ = O.ridge_bf(P, np.float32(r1), np.float32(r2))
+    S, st = rdb.ridge_detection(P, r1, r2)
+    assert st.err_bits == 0
+    assert bits_equal(S, S_ref)

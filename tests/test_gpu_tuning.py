@@ -60,3 +60,20 @@ def test_every_shape_same_ridge(rdb, dim):
             else:
                 assert bits_equal(S, ref), (shape, ci)
     rdb.tune_reset()
+
+
+def test_autotune_solve_picks_and_stores_a_shape(rdb):
+    """Whole-solve tuning: a supported shape, stored for the bucket, and a
+    plausible time per solve; the ridge is the same with the pick."""
+    torch = require_cuda()
+    P = G.helix3d(60_000, seed=9)
+    dP = torch.from_numpy(P).cuda()
+    rdb.tune_reset()
+    S_before, _ = rdb.ridge_detection(P, 0.15, 0.3)
+    b, i, ci, ms = rdb.autotune_solve(3, dP, 0.15, 0.3, runs=1)
+    assert (b, i) in CHUNK_SHAPES and ci in (2, 4, 8)
+    assert 0.0 < ms < 10_000.0
+    assert rdb.tune_get(3, 60_000, 0.15) == (b, i, ci)
+    S_after, st = rdb.ridge_detection(P, 0.15, 0.3)
+    assert st.err_bits == 0 and bits_equal(S_after, S_before)
+    rdb.tune_reset()
