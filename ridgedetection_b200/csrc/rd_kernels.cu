@@ -1118,10 +1118,11 @@ __global__ void __launch_bounds__(SCAT_W * 32) k_scatter_cta(EngineView v)
         for (int e = SCAT_KS * SCAT_W * 32 + tid; e < len; e += SCAT_W * 32) s_keys[e] = keys[e];
         for (int e = tid; e < SCAT_W * ns; e += SCAT_W * 32) hw[e] = 0;
         __syncthreads();
-        for (int i0 = r0; i0 < r1; i0 += 32) {
-            const int i = i0 + lane;
-            const WarpRun r = warp_runs((i < r1) ? s_keys[i] : -1, lane);
-            if (r.key >= 0 && lane == r.head) atomicAdd(&hw[warp * ns + r.key], r.count);
+        // per-warp key counts (order-free: shared-memory adds into the
+        // warp's own row)
+        for (int i = r0 + lane; i < r1; i += 32) {
+            const int key = s_keys[i];
+            if (key >= 0) atomicAdd(&hw[warp * ns + key], 1);
         }
         __syncthreads();
 #pragma unroll
