@@ -324,6 +324,7 @@ EngineView Engine::view() const
     v.max_iters = max_iters;
     v.Ps = bPs_.as<float>();
     v.sorder = bSorder_.as<int32_t>();
+    v.srow = bSorder_.as<int32_t>() + total_points_;  // second half of the same buffer
     v.cull = cull_ ? 1 : 0;
     v.tile_order = bTileOrder_.as<int32_t>();
     v.n_heavy = n_heavy_;
@@ -532,7 +533,7 @@ int Engine::run(cudaStream_t st, bool use_graph, int mode)
     if (cull_) {
         const size_t scratch = spatial_prep_scratch_bytes(total_points_);
         RD_CK(bPs_.ensure(sizeof(float) * (size_t)(total_points_ * pad_dim(dim_) + 4)));
-        RD_CK(bSorder_.ensure(sizeof(int32_t) * (size_t)(total_points_ + 1)));
+        RD_CK(bSorder_.ensure(sizeof(int32_t) * (size_t)(2 * total_points_ + 1)));
         RD_CK(bSpatialTmp_.ensure(scratch));
         const EngineView vs = view();
         RD_CK(launch_spatial_prep(dim_, vs, total_points_, bSpatialTmp_.p, scratch, bPs_.as<float>(),
@@ -619,7 +620,7 @@ int Engine::plan_workspace(int mode)
         if (mode == RUN_EVOLVE_ONLY && cull_assign && assign_cull_enabled() && spatial_ok_ &&
             total_points_ > 0) {
             RD_CK(bPs_.ensure(sizeof(float) * (size_t)(total_points_ * pad_dim(dim_) + 4)));
-            RD_CK(bSorder_.ensure(sizeof(int32_t) * (size_t)(total_points_ + 1)));
+            RD_CK(bSorder_.ensure(sizeof(int32_t) * (size_t)(2 * total_points_ + 1)));
             RD_CK(bSpatialTmp_.ensure(spatial_prep_scratch_bytes(total_points_)));
         }
         return 0;

@@ -129,6 +129,7 @@ struct EngineView {
     // exact chunk-box culling of the assignment (see k_assign_cull)
     const float* Ps;             // evolve points in spatial order inside each cloud
     const int32_t* sorder;       // spatial position -> packed point slot
+    const int32_t* srow;         // spatial position -> its slot's chunk in the cloud (histogram row)
     int32_t cull;                // passes assign with k_assign_cull + k_keyhist
     // fused tiled runs: tiles by decreasing evolve points, the first n_heavy
     // evolved by whole thread-block clusters (rd_tile_cluster.cuh)

@@ -94,6 +94,18 @@ template <int DIM>
 struct PadDim { static constexpr int v = (DIM == 3) ? 4 : DIM; };
 inline int pad_dim(int dim) { return dim == 3 ? 4 : dim; }
 
+// slot-order chunk of position i of a cloud of n points in m chunks: the lc
+// with floor(lc n / m) <= i < floor((lc + 1) n / m), i.e. lc n < (i + 1) m <=
+// (lc + 1) n; a float estimate corrected with exact integer products
+__device__ __forceinline__ int slot_chunk(int i, int n, int m, float ratio)
+{
+    int lc = min(max(__float2int_rz(__fmul_rn((float)i, ratio)), 0), m - 1);
+    const int64_t t = (int64_t)(i + 1) * m;
+    while (lc > 0 && (int64_t)lc * n >= t) --lc;
+    while (lc < m - 1 && (int64_t)(lc + 1) * n < t) ++lc;
+    return lc;
+}
+
 constexpr int KBLK = 32;  // chosen points per histogram-scan block (one per lane)
 
 // ---------------------------------------------------------------------------

@@ -580,18 +580,6 @@ __device__ __forceinline__ float box_gap2(const float* s, const float* lo, const
     return g2;
 }
 
-// slot-order chunk of position i of a cloud of n points in m chunks: the lc
-// with floor(lc n / m) <= i < floor((lc + 1) n / m), i.e. lc n < (i + 1) m <=
-// (lc + 1) n; a float estimate corrected with exact integer products
-__device__ __forceinline__ int slot_chunk(int i, int n, int m, float ratio)
-{
-    int lc = min(max(__float2int_rz(__fmul_rn((float)i, ratio)), 0), m - 1);
-    const int64_t t = (int64_t)(i + 1) * m;
-    while (lc > 0 && (int64_t)lc * n >= t) --lc;
-    while (lc < m - 1 && (int64_t)(lc + 1) * n < t) ++lc;
-    return lc;
-}
-
 template <int DIM, int AC_ITEMS>
 __global__ void __launch_bounds__(AC_BLOCK) k_assign_cull(EngineView v)
 {
@@ -617,11 +605,12 @@ __global__ void __launch_bounds__(AC_BLOCK) k_assign_cull(EngineView v)
     const int total = al.total * subs;
 
     // A work item's cloud, point range and this lane's points with their
-    // slots; the next item's are loaded while the current one is evaluated.
+    // slots and histogram rows; the next item's are loaded while the current
+    // one is evaluated.
     struct Item {
         int c, b0, b1;
         float p[AC_ITEMS][DIM];
-        int slot[AC_ITEMS];
+        int slot[AC_ITEMS], row[AC_ITEMS];
     };
     auto load_item = [&](const int item, Item& t) {
         t.c = -1;
@@ -629,6 +618,7 @@ __global__ void __launch_bounds__(AC_BLOCK) k_assign_cull(EngineView v)
 #pragma unroll
         for (int j = 0; j < AC_ITEMS; ++j) {
             t.slot[j] = -1;
+            t.row[j] = 0;
 #pragma unroll
             for (int d = 0; d < DIM; ++d) t.p[j][d] = 0.0f;
         }
@@ -646,6 +636,7 @@ __global__ void __launch_bounds__(AC_BLOCK) k_assign_cull(EngineView v)
             if (i < t.b1) {
                 load_chosen<DIM>(Ps, i, t.p[j]);
                 t.slot[j] = v.sorder[p_off + i];
+                t.row[j] = v.srow[p_off + i];
             }
         }
     };
@@ -787,33 +778,39 @@ __global__ void __launch_bounds__(AC_BLOCK) k_assign_cull(EngineView v)
                     keep = !(may_skip && box_gap2<DIM>(s, blo, bhi) > thr);
                 }
                 unsigned bal = __ballot_sync(FULL, keep);
-                while (bal) {  // kept chosen points in index order, warp-uniform
-                    const int b = __ffs(bal) - 1;
+                // kept chosen points in index order, warp-uniform, two per
+                // step: both distances are in flight together, and the
+                // minimum is updated with the first one before the second
+                while (bal) {
+                    const int b1 = __ffs(bal) - 1;
                     bal &= bal - 1;
-                    const int eb = __shfl_sync(FULL, e, b);
-                    float s[DIM];
-                    load_chosen<DIM>(sS, eb, s);
-                    const int kk = t0 + eb;
+                    const bool two = bal != 0u;
+                    const int b2 = two ? __ffs(bal) - 1 : b1;
+                    bal &= bal - 1;
+                    const int e1 = __shfl_sync(FULL, e, b1), e2 = __shfl_sync(FULL, e, b2);
+                    float s1[DIM], s2[DIM];
+                    load_chosen<DIM>(sS, e1, s1);
+                    load_chosen<DIM>(sS, e2, s2);
+                    const int k1 = t0 + e1, k2 = t0 + e2;
 #pragma unroll
                     for (int jj = 0; jj < AC_ITEMS / 2; ++jj) {
-                        const float2 dd = sqdist2_exact<DIM>(s, np2[jj]);
-                        if (dd.x < best[2 * jj]) { best[2 * jj] = dd.x; bi[2 * jj] = kk; }
-                        if (dd.y < best[2 * jj + 1]) { best[2 * jj + 1] = dd.y; bi[2 * jj + 1] = kk; }
+                        const float2 d1 = sqdist2_exact<DIM>(s1, np2[jj]);
+                        const float2 d2 = sqdist2_exact<DIM>(s2, np2[jj]);
+                        if (d1.x < best[2 * jj]) { best[2 * jj] = d1.x; bi[2 * jj] = k1; }
+                        if (d1.y < best[2 * jj + 1]) { best[2 * jj + 1] = d1.y; bi[2 * jj + 1] = k1; }
+                        if (two && d2.x < best[2 * jj]) { best[2 * jj] = d2.x; bi[2 * jj] = k2; }
+                        if (two && d2.y < best[2 * jj + 1]) { best[2 * jj + 1] = d2.y; bi[2 * jj + 1] = k2; }
                     }
                 }
             }
         }
-        const float ratio = (float)cd.n_chunks / (float)cd.n_all;
         int32_t* hist = v.hist + cd.hist_off;
 #pragma unroll
         for (int j = 0; j < AC_ITEMS; ++j) {
             if (cur.slot[j] >= 0) {
                 const int key = (best[j] <= rsq) ? bi[j] : -1;
                 v.keys[cur.slot[j]] = key;
-                if (key >= 0) {
-                    const int r = slot_chunk((int)(cur.slot[j] - cd.p_off), cd.n_all, cd.n_chunks, ratio);
-                    atomicAdd(&hist[(int64_t)r * cd.ns_cap + key], 1);
-                }
+                if (key >= 0) atomicAdd(&hist[(int64_t)cur.row[j] * cd.ns_cap + key], 1);
             }
         }
         cur = nxt;

@@ -85,14 +85,20 @@ __global__ void __launch_bounds__(256) k_morton(EngineView v, uint64_t* key, int
     }
 }
 
+// Ps, sorder, and (second half of sorder) each position's histogram row: the
+// chunk of its slot inside its cloud, from the sorted keys' cloud field
 template <int DIM>
 __global__ void __launch_bounds__(256) k_gather_spatial(EngineView v, int64_t n, const int32_t* val,
-                                                        float* Ps, int32_t* sorder)
+                                                        const uint64_t* key, float* Ps,
+                                                        int32_t* sorder)
 {
     constexpr int DP = PadDim<DIM>::v;
     for (int64_t pos = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; pos < n;
          pos += (int64_t)gridDim.x * blockDim.x) {
         const int32_t s = val[pos];
+        const CloudDesc cd = v.cl[(int)(key[pos] >> 32)];
+        sorder[n + pos] = slot_chunk((int)(s - cd.p_off), cd.n_all, cd.n_chunks,
+                                     (float)cd.n_chunks / (float)cd.n_all);
 #pragma unroll
         for (int d = 0; d < DIM; ++d) Ps[pos * DP + d] = v.P[(int64_t)s * DIM + d];
 #pragma unroll
@@ -136,7 +142,7 @@ cudaError_t spatial_prep_dim(const EngineView& v, int64_t n, void* scratch, size
     cudaError_t e = cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, kb, vb, (int)n, 0, end_bit, st);
     if (e != cudaSuccess) return e;
     const int ggrid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sms * 16));
-    k_gather_spatial<DIM><<<ggrid, 256, 0, st>>>(v, n, vb.Current(), Ps, sorder);
+    k_gather_spatial<DIM><<<ggrid, 256, 0, st>>>(v, n, vb.Current(), kb.Current(), Ps, sorder);
     return cudaGetLastError();
 }
 
