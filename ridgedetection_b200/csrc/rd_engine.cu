@@ -279,7 +279,6 @@ EngineView Engine::view() const
     v.base = bBase_.as<int32_t>();
     v.big = bBig_.as<int32_t>();
     v.kbdone = bKbDone_.as<int32_t>();
-    v.kchg = bKchg_.as<int32_t>();
     v.next = bNext_.as<int32_t>();
     v.hash = bHash_.as<int32_t>();
     v.ns = bNs_.as<int32_t>();
@@ -401,9 +400,6 @@ int Engine::finish_setup_after_choose(cudaStream_t st)
     RD_CK(bCnt_.ensure(4 * (size_t)(key + 1)));
     RD_CK(bBase_.ensure(4 * (size_t)(key + 1)));
     RD_CK(bBig_.ensure(4 * (size_t)(key + 1)));
-    RD_CK(bKchg_.ensure(4 * (size_t)(key + 1)));
-    if (!(current_arena() && current_arena()->measuring()))
-        RD_CK(cudaMemsetAsync(bKchg_.p, 0, 4 * (size_t)(key + 1), st));
     RD_CK(bDx_.ensure(4 * (size_t)(sscr * dim_ + 1)));
     RD_CK(bDcell_.ensure(4 * (size_t)(sscr * dim_ + 1)));
     RD_CK(bDalive_.ensure(4 * (size_t)(sscr + 1)));

@@ -80,7 +80,6 @@ struct EngineView {
     int32_t* base;               // per chosen slot: first slot of its segment of perm
     int32_t* big;                // chosen slots with SUM_BIG_MIN+ members in this pass
     int32_t* kbdone;             // per cloud: key blocks of the chunk scan finished in this pass
-    int32_t* kchg;               // per chosen slot: 1 = some point joined or left the key in this pass
     int32_t* hash;               // choose hash heads
     int32_t* next;               // per chosen slot: choose hash chain
     int32_t* ns;                 // per cloud: current chosen count

@@ -172,7 +172,6 @@ private:
     DevBuf bCl_, bGr_, bChunkCloud_, bSlotCloud_;
     DevBuf bP_, bS_, bKeys_, bGrouped_, bPg_, bHist_, bCnt_, bBase_, bBig_, bNext_, bHash_, bSurv_;
     DevBuf bNs_, bPhase_, bCont_, bPasses_, bTotPasses_, bOuter_, bErr_, bPairs_, bCtr_, bKbDone_;
-    DevBuf bKchg_;
     DevBuf bActCloud_, bActPre_, bGroupConv_, bReady_, bDnbOff_, bDnb_, bDbig_, bDcpre_;
     int dec_smem_max_ = 0;
     int dec_nb_pp_ = DEC_NB_MIN_PER_POINT;

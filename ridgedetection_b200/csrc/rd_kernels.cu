@@ -409,20 +409,6 @@ __device__ __forceinline__ void load_chosen(const float* sS, int kk, float* s)
     }
 }
 
-// A point's key went from `old` (the previous pass's, or a stale value from an
-// earlier numbering) to `key`: both keys' member sets changed in this pass.
-// k_sum_shift folds only such keys (and every key of a cloud's first pass
-// after choose or a decimation): a key whose members are those of the
-// previous pass has the same sum, and the movement test has already given its
-// answer for that sum (no move).
-__device__ __forceinline__ void mark_key_change(const EngineView& v, const CloudDesc& cd, int old,
-                                                int key)
-{
-    if (old == key) return;
-    if (old >= 0 && old < cd.ns_cap) atomicOr(&v.kchg[cd.key_off + old], 1);
-    if (key >= 0) atomicOr(&v.kchg[cd.key_off + key], 1);
-}
-
 constexpr int ASSIGN_TS = 1024;  // chosen points per shared-memory tile
 
 template <int DIM, int BLOCK, int ITEMS>
@@ -523,10 +509,7 @@ __global__ void __launch_bounds__(BLOCK) k_assign(EngineView v)
                 }
             }
             key[j] = idx;
-            if (i < n) {
-                mark_key_change(v, cd, v.keys[cd.p_off + i], key[j]);
-                v.keys[cd.p_off + i] = key[j];
-            }
+            if (i < n) v.keys[cd.p_off + i] = key[j];
         }
         // chunk histogram row (row length ns_cap, first ns entries used)
         int32_t* row = v.hist + cd.hist_off + (int64_t)lc * cd.ns_cap;
@@ -627,7 +610,7 @@ __global__ void __launch_bounds__(AC_BLOCK) k_assign_cull(EngineView v)
     struct Item {
         int c, b0, b1;
         float p[AC_ITEMS][DIM];
-        int slot[AC_ITEMS], row[AC_ITEMS], old[AC_ITEMS];
+        int slot[AC_ITEMS], row[AC_ITEMS];
     };
     auto load_item = [&](const int item, Item& t) {
         t.c = -1;
@@ -636,7 +619,6 @@ __global__ void __launch_bounds__(AC_BLOCK) k_assign_cull(EngineView v)
         for (int j = 0; j < AC_ITEMS; ++j) {
             t.slot[j] = -1;
             t.row[j] = 0;
-            t.old[j] = -1;
 #pragma unroll
             for (int d = 0; d < DIM; ++d) t.p[j][d] = 0.0f;
         }
@@ -655,7 +637,6 @@ __global__ void __launch_bounds__(AC_BLOCK) k_assign_cull(EngineView v)
                 load_chosen<DIM>(Ps, i, t.p[j]);
                 t.slot[j] = v.sorder[p_off + i];
                 t.row[j] = v.srow[p_off + i];
-                t.old[j] = v.keys[t.slot[j]];  // the previous pass's key of the point
             }
         }
     };
@@ -830,7 +811,6 @@ __global__ void __launch_bounds__(AC_BLOCK) k_assign_cull(EngineView v)
                 const int key = (best[j] <= rsq) ? bi[j] : -1;
                 v.keys[cur.slot[j]] = key;
                 if (key >= 0) atomicAdd(&hist[(int64_t)cur.row[j] * cd.ns_cap + key], 1);
-                mark_key_change(v, cd, cur.old[j], key);
             }
         }
         cur = nxt;
@@ -1098,7 +1078,6 @@ __global__ void __launch_bounds__(SCAT_W * 32) k_scatter_cta(EngineView v)
         const int len = end - start;
         int* s_keys = s_dyn;                 // chunk_max
         int* hw = s_dyn + v.chunk_max;       // SCAT_W x ns: counts, then start slots
-        int* s_need = hw + SCAT_W * SCAT_HMAX;  // ns: the key's rows are read in this pass
         const int32_t* keys = v.keys + cd.p_off + start;
         int32_t* row = v.hist + cd.hist_off + (int64_t)lc * cd.ns_cap;
         const int32_t* bs = v.base + cd.key_off;
@@ -1114,16 +1093,12 @@ __global__ void __launch_bounds__(SCAT_W * 32) k_scatter_cta(EngineView v)
             const int e = u * SCAT_W * 32 + tid;
             kv[u] = (e < len) ? keys[e] : -1;
         }
-        int bsv[SCAT_HMAX / (SCAT_W * 32)], rwv[SCAT_HMAX / (SCAT_W * 32)], ndv[SCAT_HMAX / (SCAT_W * 32)];
-        // rows of keys whose members did not change are not folded in this
-        // pass (key_needs_fold), so they are not written either
-        const bool all_keys = v.passes[c] == 0 || (v.flags & ENG_ALWAYS_MOVE);
+        int bsv[SCAT_HMAX / (SCAT_W * 32)], rwv[SCAT_HMAX / (SCAT_W * 32)];
 #pragma unroll
         for (int u = 0; u < SCAT_HMAX / (SCAT_W * 32); ++u) {
             const int k = u * SCAT_W * 32 + tid;
             bsv[u] = (k < ns) ? bs[k] : 0;
             rwv[u] = (k < ns) ? row[k] : 0;
-            ndv[u] = (k < ns) ? (all_keys || v.kchg[cd.key_off + k] != 0) : 0;
         }
         float pc[SCAT_SP][DIM];
 #pragma unroll
@@ -1139,11 +1114,6 @@ __global__ void __launch_bounds__(SCAT_W * 32) k_scatter_cta(EngineView v)
         }
         for (int e = SCAT_KS * SCAT_W * 32 + tid; e < len; e += SCAT_W * 32) s_keys[e] = keys[e];
         for (int e = tid; e < SCAT_W * ns; e += SCAT_W * 32) hw[e] = 0;
-#pragma unroll
-        for (int u = 0; u < SCAT_HMAX / (SCAT_W * 32); ++u) {
-            const int k = u * SCAT_W * 32 + tid;
-            if (k < ns) s_need[k] = ndv[u];
-        }
         __syncthreads();
         // per-warp key counts (order-free: shared-memory adds into the
         // warp's own row)
@@ -1193,7 +1163,7 @@ __global__ void __launch_bounds__(SCAT_W * 32) k_scatter_cta(EngineView v)
                 float qv[DIM];
 #pragma unroll
                 for (int d = 0; d < DIM; ++d) qv[d] = __shfl_sync(FULL, pc[q][d], r.src);
-                if (r.key >= 0 && s_need[r.key]) store_row<DIM>(Pg, b + r.rank, qv);
+                if (r.key >= 0) store_row<DIM>(Pg, b + r.rank, qv);
             }
         }
     }
@@ -1202,7 +1172,7 @@ __global__ void __launch_bounds__(SCAT_W * 32) k_scatter_cta(EngineView v)
 // dynamic shared memory of k_scatter_cta
 inline int scatter_cta_smem_bytes(const EngineView& v)
 {
-    const int block_path = v.chunk_max + SCAT_W * SCAT_HMAX + SCAT_HMAX;
+    const int block_path = v.chunk_max + SCAT_W * SCAT_HMAX;
     const int warp_path = v.chunk_max + v.scat_smem;
     return 4 * (block_path > warp_path ? block_path : warp_path);
 }
@@ -1488,24 +1458,15 @@ __device__ float fold_rows(const float* __restrict__ rows, const int n, float* b
     return sum;
 }
 
-// whether the key's sum must be formed in this pass (mark_key_change)
-__device__ __forceinline__ bool key_needs_fold(const EngineView& v, int c, int64_t slot)
-{
-    if (v.passes[c] == 0 || (v.flags & ENG_ALWAYS_MOVE)) return true;  // first pass: no answer yet
-    return v.kchg[slot] != 0;
-}
-
 template <int DIM>
 __device__ void sum_shift_one(const EngineView& v, int c, int k, float* buf, int lane, bool cta_big)
 {
     const CloudDesc cd = v.cl[c];
     const int n = v.cnt[cd.key_off + k];
     if (n == 0 || (cta_big && n >= SUM_BIG_MIN)) return;  // big keys: the CTA path
-    if (!key_needs_fold(v, c, cd.key_off + k)) return;
     const float* rows = v.Pg + (cd.p_off + v.base[cd.key_off + k]) * PadDim<DIM>::v;
     const float sum = fold_rows<DIM, SUM_BP_WIDE>(rows, n, buf, lane);
     apply_shift<DIM>(v, c, cd, k, n, sum, lane);
-    if (lane == 0) v.kchg[cd.key_off + k] = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -1526,11 +1487,9 @@ __device__ void sum_shift_big_one(const EngineView& v, int slot, SegFoldSmem<8, 
     const CloudDesc cd = v.cl[c];
     const int k = (int)(slot - cd.key_off);
     const int n = v.cnt[slot];
-    if (!key_needs_fold(v, c, slot)) return;
     const float* rows = v.Pg + (cd.p_off + v.base[slot]) * PadDim<DIM>::v;
     __syncthreads();  // the previous key's scratch is no longer read
     fold_members_seg_src<8, DIM>(RowSrc<DIM>{rows}, n, sm);
-    if (threadIdx.x == 0) v.kchg[slot] = 0;
     if (warp == 0) apply_shift<DIM>(v, c, cd, k, n, (lane < DIM) ? sm.out[lane] : 0.0f, lane);
 }
 
@@ -1546,7 +1505,7 @@ __device__ void sum_shift_big_one(const EngineView& v, int slot, SegFoldSmem<8, 
 //     index order (match_any ranks inside 32-point steps), i.e. in index order;
 //   * warp w folds keys w, w+W, ... (fold_members) and applies the shift.
 // Shared memory: chosen points (TILE_NS_MAX, padded to float4 for DIM 3),
-// W x (ns+1) counters, key bases, per-key change flags.
+// W x (ns+1) counters, key bases.
 // ---------------------------------------------------------------------------
 // Assignment of the points [r0, r1w) of a tile by one warp (steps of 32 x
 // TILE_PPL points, loads first): keys[i] = nearest chosen point within r1
@@ -1556,22 +1515,12 @@ __device__ void sum_shift_big_one(const EngineView& v, int slot, SegFoldSmem<8, 
 // otherwise one shared-memory add per distinct key of a step.
 constexpr int TILE_KB = 8;
 
-// chg (optional, shared memory): chg[k] = 1 for every key that a point joined
-// or left in this pass (the point's key before the pass is keys[i]).
-__device__ __forceinline__ void tile_mark_change(unsigned char* chg, const int ns, const int old,
-                                                 const int key)
-{
-    if (old == key) return;
-    if (old >= 0 && old < ns) chg[old] = 1;
-    if (key >= 0) chg[key] = 1;
-}
-
 template <int DIM>
 __device__ __forceinline__ void tile_assign_range(const float* __restrict__ P, const int r0,
                                                   const int r1w, const float* sS, const int ns,
                                                   const int nsp, const float rsq,
                                                   int32_t* __restrict__ keys, int* whist,
-                                                  const int lane, unsigned char* chg = nullptr)
+                                                  const int lane)
 {
     constexpr int KB = TILE_KB;
     int kc[KB];
@@ -1579,13 +1528,11 @@ __device__ __forceinline__ void tile_assign_range(const float* __restrict__ P, c
     for (int k = 0; k < KB; ++k) kc[k] = 0;
     for (int i0 = r0; i0 < r1w; i0 += 32 * TILE_PPL) {
         float p[TILE_PPL][DIM];
-        int oldk[TILE_PPL];
 #pragma unroll
         for (int h = 0; h < TILE_PPL; ++h) {
             const int i = i0 + h * 32 + lane;
 #pragma unroll
             for (int d = 0; d < DIM; ++d) p[h][d] = (i < r1w) ? P[(int64_t)i * DIM + d] : 0.0f;
-            oldk[h] = (chg && i < r1w) ? keys[i] : -1;
         }
         if (ns <= KB) {
             // first index of the minimum, directly: each chosen point is read
@@ -1610,10 +1557,7 @@ __device__ __forceinline__ void tile_assign_range(const float* __restrict__ P, c
             for (int h = 0; h < TILE_PPL; ++h) {
                 const int i = i0 + h * 32 + lane;
                 const int key = (i < r1w && best[h] <= rsq) ? bk[h] : -1;
-                if (i < r1w) {
-                    if (chg) tile_mark_change(chg, ns, oldk[h], key);
-                    keys[i] = key;
-                }
+                if (i < r1w) keys[i] = key;
 #pragma unroll
                 for (int k = 0; k < KB; ++k)
                     if (k < ns) kc[k] += __popc(__ballot_sync(FULL, key == k));
@@ -1644,7 +1588,6 @@ __device__ __forceinline__ void tile_assign_range(const float* __restrict__ P, c
                         if (sqdist_exact<DIM>(s, p[h]) == best) { key = blk + u; break; }
                     }
                 }
-                if (chg) tile_mark_change(chg, ns, oldk[h], key);
                 keys[i] = key;
             }
             // a tile's warp step holds few distinct keys: the match
@@ -1732,7 +1675,6 @@ __device__ void tile_evolve_one(const EngineView& v, const int c, const int fold
     float* sS = reinterpret_cast<float*>(dyn);                              // TILE_NS_MAX*DP
     int* hist = reinterpret_cast<int*>(sS + TILE_NS_MAX * DP);             // W*(TILE_NS_MAX+1)
     int* kbase = hist + W * (TILE_NS_MAX + 1);                              // TILE_NS_MAX+1
-    unsigned char* chg = reinterpret_cast<unsigned char*>(kbase + TILE_NS_MAX + 1);  // TILE_NS_MAX
     auto& s_buf = ts.buf;
     int& s_moved = ts.moved;
     auto& s_seg = ts.seg;
@@ -1757,13 +1699,9 @@ __device__ void tile_evolve_one(const EngineView& v, const int c, const int fold
             // 1. assignment of the warp's range + per-warp key counts
             //    (counts added once per distinct key of a warp step)
             for (int k = lane; k <= ns; k += 32) hist[warp * (TILE_NS_MAX + 1) + k] = 0;
-            for (int k = tid; k < ns; k += BLOCK) chg[k] = 0;
             __syncthreads();
             int* whist = hist + warp * (TILE_NS_MAX + 1);
-            // Keys whose members are those of the previous pass keep their sum,
-            // and the movement test has already answered for it (no move), so
-            // after the first pass only the keys marked in chg are folded.
-            tile_assign_range<DIM>(P, r0, r1w, sS, ns, nsp, rsq, keys, whist, lane, chg);
+            tile_assign_range<DIM>(P, r0, r1w, sS, ns, nsp, rsq, keys, whist, lane);
             __syncthreads();
             // 2. key bases and per-warp starts (thread per key)
             for (int k = tid; k < ns; k += BLOCK) {
@@ -1806,7 +1744,7 @@ __device__ void tile_evolve_one(const EngineView& v, const int c, const int fold
             // 4a. very large keys, one at a time, folded by the whole CTA
             for (int k = 0; k < ns; ++k) {
                 const int cnt = kbase[k + 1] - kbase[k];
-                if (cnt < fold_cta_min || (pass > 0 && !chg[k])) continue;
+                if (cnt < fold_cta_min) continue;
                 fold_members_seg_src<W, DIM>(RowSrc<DIM>{Pg + (int64_t)kbase[k] * DP}, cnt, s_seg);
                 if (tid < DIM) {
                     float cval = sS[k * DP + tid];
@@ -1820,7 +1758,7 @@ __device__ void tile_evolve_one(const EngineView& v, const int c, const int fold
             // 4b. index-order fold and movement test, warp w takes keys w, w+W, ...
             for (int k = warp; k < ns; k += W) {
                 const int cnt = kbase[k + 1] - kbase[k];
-                if (cnt == 0 || cnt >= fold_cta_min || (pass > 0 && !chg[k])) continue;
+                if (cnt == 0 || cnt >= fold_cta_min) continue;
                 const float sum = fold_rows<DIM, SUM_BP>(Pg + (int64_t)kbase[k] * DP, cnt, s_buf[warp], lane);
                 int moved = 0;
                 if (lane < DIM) {
@@ -1871,7 +1809,7 @@ __host__ __device__ constexpr int tile_evolve_smem_bytes(int dim)
 {
     const int dp = (dim == 3) ? 4 : dim;
     const int w = 8;
-    return TILE_NS_MAX * dp * 4 + w * (TILE_NS_MAX + 1) * 4 + (TILE_NS_MAX + 1) * 4 + TILE_NS_MAX;
+    return TILE_NS_MAX * dp * 4 + w * (TILE_NS_MAX + 1) * 4 + (TILE_NS_MAX + 1) * 4;
 }
 
 }  // namespace
